@@ -1,0 +1,15 @@
+"""B200-native BlackTracer hot path: Kerr geodesic grid integration and the
+per-pixel map, behind the reference's own Grid / Camera / BlackHole /
+StarProcessor / makeImage interfaces.
+
+Compute runs in hand-written sm_100a CUDA (libblacktracer_b200.so, C ABI in
+include/blacktracer.h).  This package is the Python host mirror of the
+reference interfaces; device buffers are torch CUDA tensors.
+"""
+from ._lib import (BtError, PRECISION_MIXED, PRECISION_PLAIN, RAY_CAPTURED,  # noqa: F401
+                   RAY_ESCAPED, RAY_MAXSTEP, RAY_NONCONVERGED, lib)
+from .host import (BlackHole, Camera, Grid, IntegOpts, grid_dims,  # noqa: F401
+                   integrate_rays, integrate_rays_host)
+
+__all__ = ["BlackHole", "Camera", "Grid", "IntegOpts", "grid_dims", "integrate_rays",
+           "integrate_rays_host", "BtError", "lib"]

@@ -1,0 +1,96 @@
+"""ctypes bindings of libblacktracer_b200.so (the C ABI in include/blacktracer.h).
+
+The library is the only compute path: if it is missing or fails to load,
+every entry point raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libblacktracer_b200.so")
+
+BT_OK, BT_ERR_ARG, BT_ERR_CUDA, BT_ERR_NOMEM, BT_ERR_NUMERIC, BT_ERR_STATE = range(6)
+RAY_ESCAPED, RAY_CAPTURED, RAY_MAXSTEP, RAY_NONCONVERGED = range(4)
+PRECISION_PLAIN, PRECISION_MIXED = 0, 1
+
+
+class BtError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"blacktracer error {code}: {msg}")
+        self.code = code
+
+
+class bt_camera(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "theta", "phi", "r", "speed", "br", "btheta", "bphi",
+        "alpha", "w", "wbar", "Delta", "ro")]
+
+
+class bt_integ_opts(C.Structure):
+    _fields_ = [("eps", C.c_double), ("h1", C.c_double), ("z_end", C.c_double),
+                ("maxstp", C.c_int32), ("precision", C.c_int32),
+                ("fp64_band", C.c_double)]
+
+
+class bt_grid_info(C.Structure):
+    _fields_ = [("N", C.c_int32), ("M", C.c_int32), ("maxlevel", C.c_int32),
+                ("startlevel", C.c_int32), ("angle", C.c_int32),
+                ("traced", C.c_int64), ("n_leaf_blocks", C.c_int64),
+                ("flags", C.c_uint32),
+                ("thphi", C.c_void_p), ("steps", C.c_void_p), ("exists", C.c_void_p),
+                ("blevel", C.c_void_p), ("status", C.c_void_p)]
+
+
+_vp = C.c_void_p
+_SIGS = {
+    "bt_camera_static": (C.c_int, [C.c_double] * 5 + [C.POINTER(bt_camera)]),
+    "bt_camera_orbit": (C.c_int, [C.c_double] * 7 + [C.POINTER(bt_camera)]),
+    "bt_camera_params": (C.c_int, [C.POINTER(bt_camera), C.POINTER(C.c_float)]),
+    "bt_integ_opts_default": (None, [C.POINTER(bt_integ_opts)]),
+    "bt_integrate_rays": (C.c_int, [C.POINTER(bt_camera), C.c_double, _vp, _vp, C.c_size_t,
+                                    _vp, _vp, _vp, _vp, C.POINTER(bt_integ_opts), _vp]),
+    "bt_integrate_rays_host": (C.c_int, [C.POINTER(bt_camera), C.c_double, _vp, _vp,
+                                         C.c_size_t, _vp, _vp, _vp, _vp,
+                                         C.POINTER(bt_integ_opts), _vp]),
+    "bt_grid_dims": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "bt_grid_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(_vp)]),
+    "bt_grid_destroy": (None, [_vp]),
+    "bt_grid_build": (C.c_int, [_vp, C.POINTER(bt_camera), C.c_double, C.c_int,
+                                C.POINTER(bt_integ_opts), _vp]),
+    "bt_grid_query": (C.c_int, [_vp, C.POINTER(bt_grid_info), _vp]),
+    "bt_grid_export_dense": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "bt_grid_map_export": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_int32), _vp]),
+    "bt_last_error": (C.c_char_p, []),
+    "bt_version": (C.c_char_p, []),
+}
+
+_lib = None
+
+
+def lib():
+    """Loads the CUDA library (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m blacktracer_b200.build` "
+                "(there is no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGS)
+
+
+def check(rc: int) -> None:
+    if rc != BT_OK:
+        raise BtError(rc, lib().bt_last_error().decode(errors="replace"))

@@ -1,0 +1,314 @@
+// integrate.cu -- camera set-up and the ray-integration entry points.
+//
+// Compiled with --fmad=false: the plain FP64 integrator must round exactly
+// as the reference's host build (see kerr_plain.cuh).
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "bt_internal.h"
+#include "kerr_plain.cuh"
+#include "trace_kernel.cuh"
+
+namespace bt {
+
+static thread_local char g_err[512] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+void clear_error() { g_err[0] = 0; }
+
+// ---- host Kerr scalars (BT/Metric.h:64-108), evaluated with glibc ----
+namespace host {
+static inline double sq(double x) { return x * x; }
+static double delta(double a2, double r) { return sq(r) - 2. * r + a2; }
+static double sigma(double a2, double r, double th) {
+  return std::sqrt(sq(sq(r) + a2) - a2 * delta(a2, r) * sq(std::sin(th)));
+}
+static double w(double a, double a2, double r, double th) {
+  return 2. * a * r / sq(sigma(a2, r, th));
+}
+static double ro(double a2, double r, double th) {
+  return std::sqrt(sq(r) + a2 * sq(std::cos(th)));
+}
+static double wbar(double a2, double r, double th) {
+  return sigma(a2, r, th) * std::sin(th) / ro(a2, r, th);
+}
+static double alpha(double a2, double r, double th) {
+  return ro(a2, r, th) * std::sqrt(delta(a2, r)) / sigma(a2, r, th);
+}
+static double b0(double a, double a2, double r0) {
+  return -(r0 * r0 * r0 - 3. * sq(r0) + a2 * r0 + a2) / (a * (r0 - 1.));
+}
+static void initforms(double a, bt_camera* c) {
+  const double a2 = a * a;
+  c->alpha = alpha(a2, c->r, c->theta);
+  c->w = w(a, a2, c->r, c->theta);
+  c->wbar = wbar(a2, c->r, c->theta);
+  c->Delta = delta(a2, c->r);
+  c->ro = ro(a2, c->r, c->theta);
+}
+}  // namespace host
+
+int make_ray_params(const bt_camera* c, double a, const bt_integ_opts* o,
+                    RayParams* p) {
+  bt_integ_opts d;
+  if (!o) {
+    bt_integ_opts_default(&d);
+    o = &d;
+  }
+  if (!c || !p) return BT_ERR_ARG;
+  if (!(o->eps > 0) || o->maxstp < 0 || !(c->r > 0)) return BT_ERR_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->thetaS = c->theta; p->phiS = c->phi; p->rS = c->r; p->sp = c->speed;
+  p->br = c->br; p->btheta = c->btheta; p->bphi = c->bphi;
+  p->alpha = c->alpha; p->w = c->w; p->wbar = c->wbar; p->Delta = c->Delta;
+  p->ro = c->ro;
+  // Single-precision square roots exactly as the reference (BT/Grid.h:529,542)
+  p->sqrt_1msp2 = (double)sqrtf((float)(1 - c->speed * c->speed));
+  p->sqrtf_delta = (double)sqrtf((float)c->Delta);
+  p->kb = std::sqrt(1 - c->btheta * c->btheta);
+  p->cosS2 = std::cos(c->theta) * std::cos(c->theta);
+  p->sinS2 = std::sin(c->theta) * std::sin(c->theta);
+  p->a = a;
+  p->asq = a * a;
+  // checkB_Q thresholds, BT/Metric.h:146-147,164-165
+  const double r1 = 2. * (1. + std::cos(2. * std::acos(-a) / 3.));
+  const double r2 = 2. * (1. + std::cos(2. * std::acos(a) / 3.));
+  p->b_lo = host::b0(a, p->asq, r2);
+  p->b_hi = host::b0(a, p->asq, r1);
+  p->eps = o->eps;
+  p->h1 = o->h1;
+  p->z_end = o->z_end;
+  p->maxstp = o->maxstp;
+  p->precision = o->precision;
+  p->fp64_band = o->fp64_band;
+  // equatorial photon-orbit radii: prograde r1 and retrograde r2 bracket
+  // every spherical photon orbit radius
+  p->r_ph_lo = r1;
+  p->r_ph_hi = r2;
+  return BT_OK;
+}
+
+// ---------------------------------------------------------------- kernels
+// One ray per thread, grid-stride.  256 threads, the FP64 register file
+// limits residency to ~2 blocks/SM.
+__global__ void __launch_bounds__(128)
+k_integrate_plain(const RayParams p, const double* __restrict__ th,
+                  const double* __restrict__ ph, size_t n,
+                  double* __restrict__ tho, double* __restrict__ pho,
+                  int32_t* __restrict__ steps, uint8_t* __restrict__ status) {
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n;
+       r += (size_t)gridDim.x * blockDim.x) {
+    double to, po;
+    int32_t st;
+    uint8_t s;
+    plain::integrate_ray(p, th[r], ph[r], to, po, st, s);
+    tho[r] = to;
+    pho[r] = po;
+    steps[r] = st;
+    if (status) status[r] = s;
+  }
+}
+
+struct PlainPolicy {
+  using State = plain::RayState;
+  static __device__ __forceinline__ bool begin(const RayParams& p, double th,
+                                               double ph, State& s, double& to,
+                                               double& po, int32_t& st,
+                                               uint8_t& ss) {
+    return plain::begin_ray(p, th, ph, s, to, po, st, ss);
+  }
+  static __device__ __forceinline__ bool attempt(const RayParams& p, State& s) {
+    return plain::attempt(p, s);
+  }
+  static __device__ __forceinline__ void finish(const RayParams& p,
+                                                const State& s, double& to,
+                                                double& po, int32_t& st,
+                                                uint8_t& ss) {
+    plain::finish_ray(p, s, to, po, st, ss);
+  }
+};
+
+int launch_trace_plain(const RayParams& p, const LatticeView& L,
+                       const uint32_t* keys, GridCounters* ctr,
+                       cudaStream_t s) {
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, k_trace_lattice<PlainPolicy>, 128, 0);
+    if (per_sm < 1) per_sm = 1;
+  }
+  k_trace_lattice<PlainPolicy><<<sm_count() * per_sm, 128, 0, s>>>(p, L, keys, ctr);
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+int launch_integrate(const RayParams& p, const double* th, const double* ph,
+                     size_t n, double* tho, double* pho, int32_t* steps,
+                     uint8_t* status, cudaStream_t s) {
+  if (n == 0) return BT_OK;
+  const int threads = 128;
+  size_t blocks = (n + threads - 1) / threads;
+  const size_t cap = (size_t)sm_count() * 16;
+  if (blocks > cap) blocks = cap;
+  if (p.precision == BT_PRECISION_MIXED)
+    return launch_integrate_mixed(p, th, ph, n, tho, pho, steps, status, s);
+  k_integrate_plain<<<(unsigned)blocks, threads, 0, s>>>(p, th, ph, n, tho,
+                                                         pho, steps, status);
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
+}  // namespace bt
+
+using namespace bt;
+
+extern "C" {
+
+const char* bt_last_error(void) { return bt::g_err; }
+
+const char* bt_version(void) {
+  return "blacktracer_b200 abi " "1" " sm_100a";
+}
+
+void bt_integ_opts_default(bt_integ_opts* o) {
+  if (!o) return;
+  o->eps = 1e-5;
+  o->h1 = 0.01;
+  o->z_end = -10000000;
+  o->maxstp = 1000;
+  o->precision = BT_PRECISION_PLAIN;
+  o->fp64_band = 0.05;
+}
+
+int bt_camera_static(double a, double theta, double phi, double r,
+                     double speed, bt_camera* out) {
+  BT_ARG_CHECK(out != nullptr, "out is NULL");
+  BT_ARG_CHECK(r > 0, "r must be positive");
+  std::memset(out, 0, sizeof(*out));
+  out->theta = theta; out->phi = phi; out->r = r; out->speed = speed;
+  out->bphi = 1; out->btheta = 0; out->br = 0;
+  host::initforms(a, out);
+  return BT_OK;
+}
+
+int bt_camera_orbit(double a, double theta, double phi, double r, double br,
+                    double btheta, double bphi, bt_camera* out) {
+  BT_ARG_CHECK(out != nullptr, "out is NULL");
+  BT_ARG_CHECK(r > 0, "r must be positive");
+  std::memset(out, 0, sizeof(*out));
+  out->theta = theta; out->phi = phi; out->r = r;
+  out->bphi = bphi; out->btheta = btheta; out->br = br;
+  const double a2 = a * a;
+  // metric::calcSpeed, BT/Metric.h:104-108
+  const double omega = 1. / (a + std::pow(r, 1.5));
+  out->speed = host::wbar(a2, r, theta) / host::alpha(a2, r, theta) *
+               (omega - host::w(a, a2, r, theta));
+  host::initforms(a, out);
+  return BT_OK;
+}
+
+int bt_camera_params(const bt_camera* c, float out7[7]) {
+  BT_ARG_CHECK(c && out7, "NULL pointer");
+  out7[0] = (float)c->speed; out7[1] = (float)c->alpha; out7[2] = (float)c->w;
+  out7[3] = (float)c->wbar; out7[4] = (float)c->br; out7[5] = (float)c->btheta;
+  out7[6] = (float)c->bphi;
+  return BT_OK;
+}
+
+int bt_integrate_rays(const bt_camera* cam, double a, const double* theta,
+                      const double* phi, size_t n, double* theta_out,
+                      double* phi_out, int32_t* steps, uint8_t* status,
+                      const bt_integ_opts* o, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(cam != nullptr, "cam is NULL");
+  if (n == 0) return BT_OK;
+  BT_ARG_CHECK(theta && phi && theta_out && phi_out && steps,
+               "NULL array pointer");
+  RayParams p;
+  int rc = make_ray_params(cam, a, o, &p);
+  if (rc) {
+    set_error("invalid camera or integrator options");
+    return rc;
+  }
+  return launch_integrate(p, theta, phi, n, theta_out, phi_out, steps, status,
+                          (cudaStream_t)stream);
+}
+
+// Per-thread staging buffer for the host-pointer variant.
+namespace {
+struct Staging {
+  void* dev = nullptr;
+  size_t bytes = 0;
+  ~Staging() {
+    if (dev) cudaFree(dev);
+  }
+};
+thread_local Staging g_stage;
+}  // namespace
+
+int bt_integrate_rays_host(const bt_camera* cam, double a, const double* theta,
+                           const double* phi, size_t n, double* theta_out,
+                           double* phi_out, int32_t* steps, uint8_t* status,
+                           const bt_integ_opts* o, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(cam != nullptr, "cam is NULL");
+  if (n == 0) return BT_OK;
+  BT_ARG_CHECK(theta && phi && theta_out && phi_out && steps,
+               "NULL array pointer");
+  const size_t need = n * (4 * sizeof(double) + sizeof(int32_t) + 1) + 256;
+  if (g_stage.bytes < need) {
+    if (g_stage.dev) cudaFree(g_stage.dev);
+    g_stage.dev = nullptr;
+    g_stage.bytes = 0;
+    cudaError_t e = cudaMalloc(&g_stage.dev, need);
+    if (e != cudaSuccess) {
+      set_error("staging allocation of %zu bytes failed: %s", need,
+                cudaGetErrorString(e));
+      return BT_ERR_NOMEM;
+    }
+    g_stage.bytes = need;
+  }
+  char* base = (char*)g_stage.dev;
+  double* dth = (double*)base;
+  double* dph = dth + n;
+  double* dto = dph + n;
+  double* dpo = dto + n;
+  int32_t* dst = (int32_t*)(dpo + n);
+  uint8_t* dss = (uint8_t*)(dst + n);
+  cudaStream_t s = (cudaStream_t)stream;
+  BT_CUDA_TRY(cudaMemcpyAsync(dth, theta, n * sizeof(double),
+                              cudaMemcpyHostToDevice, s));
+  BT_CUDA_TRY(cudaMemcpyAsync(dph, phi, n * sizeof(double),
+                              cudaMemcpyHostToDevice, s));
+  int rc = bt_integrate_rays(cam, a, dth, dph, n, dto, dpo, dst, dss, o, stream);
+  if (rc) return rc;
+  BT_CUDA_TRY(cudaMemcpyAsync(theta_out, dto, n * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  BT_CUDA_TRY(cudaMemcpyAsync(phi_out, dpo, n * sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+  BT_CUDA_TRY(cudaMemcpyAsync(steps, dst, n * sizeof(int32_t),
+                              cudaMemcpyDeviceToHost, s));
+  if (status)
+    BT_CUDA_TRY(cudaMemcpyAsync(status, dss, n, cudaMemcpyDeviceToHost, s));
+  BT_CUDA_TRY(cudaStreamSynchronize(s));
+  return BT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,175 @@
+/*
+ * blacktracer.h -- C ABI of the B200-native BlackTracer hot path.
+ *
+ * Plain C types only (pointers, sizes, PODs).  CUDA streams are passed as
+ * void* (a cudaStream_t; NULL = the legacy default stream).  Unless stated
+ * otherwise, array arguments of the *_dev functions are DEVICE pointers owned
+ * by the caller; *_host functions take HOST pointers and do the copies.
+ *
+ * Every entry point returns 0 (BT_OK) or a BT_ERR_* code; bt_last_error()
+ * gives a message for the last failure on the calling thread.
+ *
+ * Each declaration names the reference interface it replaces
+ * (annemiekie/BlackTracer; "BT/" = BlackTracer2/BlackTracer/).
+ */
+#ifndef BLACKTRACER_H
+#define BLACKTRACER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BT_ABI_VERSION 1
+
+enum {
+  BT_OK = 0,
+  BT_ERR_ARG = 1,      /* invalid argument (size, level, NULL pointer)      */
+  BT_ERR_CUDA = 2,     /* a CUDA runtime call failed                        */
+  BT_ERR_NOMEM = 3,    /* device allocation failed / budget exceeded        */
+  BT_ERR_NUMERIC = 4,  /* a bounded iteration did not converge              */
+  BT_ERR_STATE = 5     /* handle used in the wrong state                    */
+};
+
+/* Per-ray status written by the integrators. */
+enum {
+  BT_RAY_ESCAPED = 0,     /* integrated to the end of the affine range     */
+  BT_RAY_CAPTURED = 1,    /* capture test said "falls in": (-1, -1, 0)     */
+  BT_RAY_MAXSTEP = 2,     /* MAXSTP attempts without reaching the end: the
+                             reference then returns the camera's own angles */
+  BT_RAY_NONCONVERGED = 3 /* capture-test Newton loop hit its cap (the
+                             reference loop is unbounded, BT/Metric.h:152)  */
+};
+
+/* Arithmetic of the geodesic integrator. */
+enum {
+  BT_PRECISION_PLAIN = 0, /* FP64, reference operation order, no FMA      */
+  BT_PRECISION_MIXED = 1  /* FP32 bulk, FP64 near the photon sphere, at
+                             turning points, for capture and for phi       */
+};
+
+/* Field-for-field the reference Camera (BT/Camera.h:8-11). */
+typedef struct bt_camera {
+  double theta, phi, r;
+  double speed, br, btheta, bphi;
+  double alpha, w, wbar, Delta, ro;
+} bt_camera;
+
+/* Camera(theta, phi, r, speed): static / user-speed camera.
+ * Replaces BT/Camera.h:27-38 (+ initforms :54-61).  Spin a replaces the
+ * process-global metric::a set by BlackHole::setA (BT/BlackHole.h:12-15). */
+int bt_camera_static(double a, double theta, double phi, double r,
+                     double speed, bt_camera* out);
+
+/* Camera(theta, phi, r, br, btheta, bphi): Keplerian circular-orbit camera
+ * boosted along (br, btheta, bphi).  Replaces BT/Camera.h:40-52 with
+ * metric::calcSpeed (BT/Metric.h:104-108). */
+int bt_camera_orbit(double a, double theta, double phi, double r, double br,
+                    double btheta, double bphi, bt_camera* out);
+
+/* Camera::getParamArray (BT/Camera.h:67-78): the 7 floats the map uses. */
+int bt_camera_params(const bt_camera* cam, float out7[7]);
+
+/* Integrator options.  Defaults (bt_integ_opts_default) are the reference's
+ * rkckIntegrate1 constants, BT/Metric.h:311-314 and MAXSTP :31. */
+typedef struct bt_integ_opts {
+  double eps;        /* relative tolerance            (1e-5)   */
+  double h1;         /* initial step magnitude        (0.01)   */
+  double z_end;      /* affine end point, negative    (-1e7)   */
+  int32_t maxstp;    /* attempt cap                   (1000)   */
+  int32_t precision; /* BT_PRECISION_*                (PLAIN)  */
+  double fp64_band;  /* MIXED: |r - r_ph| band kept in FP64, in M (0.05) */
+} bt_integ_opts;
+
+void bt_integ_opts_default(bt_integ_opts* o);
+
+/* Backward null-geodesic integration of n camera-sky directions.
+ * Replaces Grid::integration_wrapper (BT/Grid.h:514-556; called from
+ * Grid::callKernel :382-401), which works in place on vector<double>& theta,
+ * phi and vector<int>& step with the camera and spin taken from globals.
+ * Here inputs and outputs are separate DEVICE arrays of n elements; outputs
+ * follow the reference: captured rays give (-1, -1, 0); a ray that reaches
+ * MAXSTP keeps the camera's angles (wrapped) with steps = maxstp-1.
+ * status (may be NULL) receives BT_RAY_* per ray.  o may be NULL (defaults). */
+int bt_integrate_rays(const bt_camera* cam, double a, const double* theta,
+                      const double* phi, size_t n, double* theta_out,
+                      double* phi_out, int32_t* steps, uint8_t* status,
+                      const bt_integ_opts* o, void* stream);
+
+/* The same with HOST arrays: copies in, integrates, copies out, synchronises
+ * the stream.  Uses a per-thread device staging area grown on demand. */
+int bt_integrate_rays_host(const bt_camera* cam, double a, const double* theta,
+                           const double* phi, size_t n, double* theta_out,
+                           double* phi_out, int32_t* steps, uint8_t* status,
+                           const bt_integ_opts* o, void* stream);
+
+/* ------------------------------------------------------------------ grid */
+
+/* Lattice size of a grid with max level L: N = 2^L/(2-eq)+1 rows,
+ * M = (2-eq)*2*(N-1) columns, eq = angle ? 1 : 0.  BT/Grid.h:612-615. */
+int bt_grid_dims(int maxlevel, int angle, int32_t* N, int32_t* M);
+
+/* A device-resident adaptive grid: the reference's Grid object
+ * (BT/Grid.h:27-660) with CamToCel / steps / blockLevels held as a dense
+ * N x M lattice in HBM instead of hash maps.  Created once per (maxlevel,
+ * angle) and rebuilt in place for any camera / spin. */
+typedef struct bt_grid bt_grid;
+
+int bt_grid_create(int maxlevel, int angle, bt_grid** out);
+void bt_grid_destroy(bt_grid* g);
+
+/* Builds the grid: Grid::Grid(maxLevelPrec, startLevel, angle, camera, bh)
+ * (BT/Grid.h:605-624) -- start-level trace, level-synchronous refinement
+ * (refineCheck, PRECCELEST = 0.015), T-vertex fix.  Asynchronous on
+ * `stream`; no host synchronisation inside (graph-capturable).  The
+ * T-vertex fix runs in the canonical order (level, then key i<<32|j) --
+ * the reference iterates an unordered_map there, whose order is
+ * implementation-defined.  o may be NULL (reference defaults); o->precision
+ * selects the plain or mixed integrator. */
+int bt_grid_build(bt_grid* g, const bt_camera* cam, double a, int startlevel,
+                  const bt_integ_opts* o, void* stream);
+
+typedef struct bt_grid_info {
+  int32_t N, M, maxlevel, startlevel, angle;
+  int64_t traced;         /* rays integrated by the build            */
+  int64_t n_leaf_blocks;  /* leaf blocks below the max level          */
+  uint32_t flags;         /* nonzero: a bounded iteration gave up    */
+  /* device pointers into the lattice (valid until the next build) */
+  const double* thphi;    /* N*M (theta, phi) pairs                  */
+  const int32_t* steps;   /* N*M                                     */
+  const uint8_t* exists;  /* N*M, 1 where CamToCel holds the key     */
+  const int8_t* blevel;   /* N*M, blockLevels at the block origin    */
+  const uint8_t* status;  /* N*M, BT_RAY_* of traced vertices        */
+} bt_grid_info;
+
+/* Synchronises `stream` and reports the build.  Returns BT_ERR_NUMERIC when
+ * a bounded loop (T-vertex fixed point) gave up. */
+int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream);
+
+/* Dense export into caller DEVICE arrays of N*M elements (any may be NULL):
+ * theta/phi (-2 where no vertex exists), exists, steps, blevel (-1 = none),
+ * status. */
+int bt_grid_export_dense(const bt_grid* g, double* theta, double* phi,
+                         uint8_t* exists, int32_t* steps, int8_t* blevel,
+                         uint8_t* status, void* stream);
+
+/* The float2 grid the per-pixel map reads: replaces saveAsGpuHash
+ * (BT/Grid.h:642-654) + the PSH tables + makeGrid
+ * (BT/MakeImageKernel.cu:369-384).  (-2,-2) = no vertex, (-1,-1) =
+ * captured; for half grids (GM/GN > 3) the lower hemisphere is mirrored
+ * (rows = 2N-1).  Returns a device pointer owned by the grid. */
+int bt_grid_map_export(bt_grid* g, const float** grid_out, int32_t* rows,
+                       int32_t* cols, int32_t* sym, void* stream);
+
+/* Message for the last error on this thread ("" when none). */
+const char* bt_last_error(void);
+
+/* Library build/version string. */
+const char* bt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BLACKTRACER_H */

@@ -1,0 +1,191 @@
+"""CPU oracle for the BlackTracer hot path -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this package, and only as the checker.  The product
+library never loads it.
+
+Two back ends:
+
+* ``_build/libbt_oracle.so`` -- the plain-C restatement (bt_oracle.c) of the
+  reference algorithm (annemiekie/BlackTracer, BT/Metric.h, BT/Grid.h).
+* ``_ref/libbtref.so`` -- the reference's own code compiled in place from the
+  reference tree by ``make -C oracle ref`` (ref_harness.cpp).  It exists only
+  where the reference tree was present at build time; everything here that
+  needs it checks ``have_ref()``.
+
+Arrays are numpy; camera parameters are 12 doubles in the field order of the
+reference Camera (BT/Camera.h:8-11).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ORC = os.path.join(_HERE, "_build", "libbt_oracle.so")
+_REF = os.path.join(_HERE, "_ref", "libbtref.so")
+
+CAM_FIELDS = ("theta", "phi", "r", "speed", "br", "btheta", "bphi",
+              "alpha", "w", "wbar", "Delta", "ro")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+_i8p = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
+
+
+def build(with_ref: bool | None = None) -> None:
+    """Compile the restatement (and the reference harness when the reference
+    tree is present)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    if with_ref is None:
+        with_ref = os.path.isdir("/root/reference/BlackTracer2")
+    if with_ref:
+        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+
+
+_orc = None
+_ref = None
+
+
+def _lib():
+    global _orc
+    if _orc is None:
+        if not os.path.exists(_ORC):
+            build(with_ref=False)
+        lib = C.CDLL(_ORC)
+        lib.orc_camera_static.argtypes = [C.c_double] * 5 + [_dp]
+        lib.orc_camera_orbit.argtypes = [C.c_double] * 7 + [_dp]
+        lib.orc_integrate_rays.argtypes = [_dp, C.c_double, _dp, _dp, C.c_size_t,
+                                           _dp, _dp, _i32p, _u8p, C.c_int]
+        lib.orc_integrate_rays_opts.argtypes = [
+            _dp, C.c_double, _dp, _dp, C.c_size_t, _dp, _dp, _i32p, _u8p,
+            C.c_double, C.c_double, C.c_double, C.c_int32, C.c_int]
+        lib.orc_grid_build.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_double,
+                                       C.c_int, _dp, _dp, _u8p, _i32p, _i8p, C.c_int]
+        lib.orc_grid_build.restype = C.c_long
+        lib.orc_grid_dims.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int)]
+        _orc = lib
+    return _orc
+
+
+def have_ref() -> bool:
+    return os.path.exists(_REF)
+
+
+def _reflib():
+    global _ref
+    if _ref is None:
+        if not have_ref():
+            raise RuntimeError("reference harness not built (make -C oracle ref)")
+        lib = C.CDLL(_REF)
+        lib.btref_camera.argtypes = [C.c_int] + [C.c_double] * 7 + [_dp]
+        lib.btref_integrate_rays.argtypes = [_dp, C.c_double, _dp, _dp, C.c_long,
+                                             _dp, _dp, _i32p, C.c_int]
+        lib.btref_grid_build.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_double,
+                                         C.c_int, _dp, _dp, _u8p, _i32p, _i8p]
+        lib.btref_grid_build.restype = C.c_long
+        lib.btref_grid_time.argtypes = [C.c_int, C.c_int, C.c_int, _dp, C.c_double,
+                                        C.POINTER(C.c_long)]
+        lib.btref_grid_time.restype = C.c_double
+        _ref = lib
+    return _ref
+
+
+# ---------------------------------------------------------------- cameras
+def camera_static(a, theta, phi, r, speed, ref=False):
+    """Camera(theta, phi, r, speed) -- BT/Camera.h:27-38."""
+    out = np.zeros(12)
+    if ref:
+        _reflib().btref_camera(0, a, theta, phi, r, speed, 0.0, 0.0, out)
+    else:
+        _lib().orc_camera_static(a, theta, phi, r, speed, out)
+    return out
+
+
+def camera_orbit(a, theta, phi, r, br, btheta, bphi, ref=False):
+    """Camera(theta, phi, r, br, btheta, bphi), Keplerian -- BT/Camera.h:40-52."""
+    out = np.zeros(12)
+    if ref:
+        _reflib().btref_camera(1, a, theta, phi, r, br, btheta, bphi, out)
+    else:
+        _lib().orc_camera_orbit(a, theta, phi, r, br, btheta, bphi, out)
+    return out
+
+
+# ---------------------------------------------------------------- rays
+def integrate_rays(cam, a, theta, phi, nthreads=0, ref=False, opts=None):
+    """Grid::integration_wrapper (BT/Grid.h:514-556) on n rays.
+
+    Returns (theta_out, phi_out, steps, status); status is None for ref=True.
+    opts = (eps, h1, z_end, maxstp) selects a non-default tolerance
+    (restatement only).
+    """
+    cam = np.ascontiguousarray(cam, dtype=np.float64)
+    theta = np.ascontiguousarray(theta, dtype=np.float64)
+    phi = np.ascontiguousarray(phi, dtype=np.float64)
+    n = theta.size
+    to = np.empty(n)
+    po = np.empty(n)
+    st = np.empty(n, dtype=np.int32)
+    if ref:
+        _reflib().btref_integrate_rays(cam, a, theta, phi, n, to, po, st,
+                                       max(1, nthreads or os.cpu_count() or 1))
+        return to, po, st, None
+    status = np.empty(n, dtype=np.uint8)
+    if opts is None:
+        _lib().orc_integrate_rays(cam, a, theta, phi, n, to, po, st, status, nthreads)
+    else:
+        eps, h1, z_end, maxstp = opts
+        _lib().orc_integrate_rays_opts(cam, a, theta, phi, n, to, po, st, status,
+                                       eps, h1, z_end, int(maxstp), nthreads)
+    return to, po, st, status
+
+
+# ---------------------------------------------------------------- grid
+def grid_dims(maxlevel, angle=True):
+    N, M = C.c_int(), C.c_int()
+    _lib().orc_grid_dims(maxlevel, 1 if angle else 0, C.byref(N), C.byref(M))
+    return N.value, M.value
+
+
+def grid_build(maxlevel, startlevel, angle, cam, a, tfix=1, ref=False, nthreads=0):
+    """Adaptive grid (BT/Grid.h:605-624) on a dense lattice.
+
+    tfix: 0 = raw traced values, 1 = canonical-order T-vertex fix,
+          2 = (ref only) the reference's own unordered_map order.
+    Returns dict(theta, phi, exists, steps, blevel, N, M, count).
+    """
+    N, M = grid_dims(maxlevel, angle)
+    cam = np.ascontiguousarray(cam, dtype=np.float64)
+    th = np.empty(N * M)
+    ph = np.empty(N * M)
+    ex = np.empty(N * M, dtype=np.uint8)
+    st = np.empty(N * M, dtype=np.int32)
+    bl = np.empty(N * M, dtype=np.int8)
+    if ref:
+        cnt = _reflib().btref_grid_build(maxlevel, startlevel, 1 if angle else 0, cam,
+                                         a, tfix, th, ph, ex, st, bl)
+    else:
+        if tfix == 2:
+            raise ValueError("tfix=2 (native unordered_map order) exists only in the reference")
+        cnt = _lib().orc_grid_build(maxlevel, startlevel, 1 if angle else 0, cam, a,
+                                    tfix, th, ph, ex, st, bl, nthreads)
+    if cnt < 0:
+        raise ValueError("bad grid arguments")
+    shp = (N, M)
+    return dict(theta=th.reshape(shp), phi=ph.reshape(shp), exists=ex.reshape(shp),
+                steps=st.reshape(shp), blevel=bl.reshape(shp), N=N, M=M, count=int(cnt))
+
+
+def ref_grid_time(maxlevel, startlevel, angle, cam, a):
+    """Wall time of the reference Grid constructor (one thread, incl. hash)."""
+    n = C.c_long()
+    cam = np.ascontiguousarray(cam, dtype=np.float64)
+    t = _reflib().btref_grid_time(maxlevel, startlevel, 1 if angle else 0, cam, a,
+                                  C.byref(n))
+    return t, n.value

@@ -1,0 +1,197 @@
+// ref_harness.cpp -- drives the REFERENCE's own code, compiled in place.
+//
+// TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file against the
+// reference headers where they lie (BlackTracer2/BlackTracer/ of the reference
+// tree) into oracle/_ref/libbtref.so.  No reference source is copied into this
+// repository; this file only calls the reference's classes:
+//   Camera (BT/Camera.h:27,40), BlackHole (BT/BlackHole.h:7),
+//   Grid::integration_wrapper (BT/Grid.h:514), Grid::raytrace (BT/Grid.h:291),
+//   Grid::fixTvertices (BT/Grid.h:103), Grid::Grid (BT/Grid.h:605-624).
+// It exposes them through a small extern "C" surface that oracle/__init__.py
+// loads with ctypes, so the plain-C restatement (oracle/bt_oracle.c) and the
+// GPU library can be pinned to the reference's own outputs.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <fstream>
+#include <functional>
+#include <iomanip>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <set>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+#include "opencv2/imgcodecs/imgcodecs.hpp"
+#include "opencv2/highgui/highgui.hpp"
+#include "opencv2/imgproc/imgproc.hpp"
+#include <cereal/archives/binary.hpp>
+#include <cereal/types/vector.hpp>
+#include <cereal/types/memory.hpp>
+#include <cereal/types/unordered_map.hpp>
+#include "cuda_runtime.h"
+// The grid's work routines are private; the harness needs to call them one by
+// one (raytrace, then fixTvertices in a chosen order).
+#define private public
+#include "Grid.h"
+#undef private
+
+namespace {
+
+struct NullBuf : std::streambuf {
+  int overflow(int c) override { return c; }
+};
+
+// Silences the reference's progress printing on std::cout during a call.
+struct Quiet {
+  NullBuf nb;
+  std::streambuf* old;
+  Quiet() : old(std::cout.rdbuf(&nb)) {}
+  ~Quiet() { std::cout.rdbuf(old); }
+};
+
+// Packs/unpacks Camera's public fields (BT/Camera.h:8-11) as 12 doubles.
+void cam_to_array(const Camera& c, double* o) {
+  double v[12] = {c.theta, c.phi, c.r, c.speed, c.br, c.btheta, c.bphi,
+                  c.alpha, c.w, c.wbar, c.Delta, c.ro};
+  std::copy(v, v + 12, o);
+}
+Camera cam_from_array(const double* v) {
+  Camera c;
+  c.theta = v[0]; c.phi = v[1]; c.r = v[2]; c.speed = v[3]; c.br = v[4];
+  c.btheta = v[5]; c.bphi = v[6]; c.alpha = v[7]; c.w = v[8]; c.wbar = v[9];
+  c.Delta = v[10]; c.ro = v[11];
+  return c;
+}
+
+void export_grid(Grid& g, double* theta, double* phi, uint8_t* exists,
+                 int32_t* steps, int8_t* blevel) {
+  const size_t NM = (size_t)g.N * g.M;
+  for (size_t q = 0; q < NM; q++) { theta[q] = -2; phi[q] = -2; }
+  std::fill(exists, exists + NM, 0);
+  std::fill(blevel, blevel + NM, (int8_t)-1);
+  for (auto& e : g.CamToCel) {
+    uint32_t i = (uint32_t)(e.first >> 32), j = (uint32_t)e.first;
+    size_t id = (size_t)i * g.M + j;
+    theta[id] = e.second.x;
+    phi[id] = e.second.y;
+    exists[id] = 1;
+  }
+  for (size_t q = 0; q < NM; q++) steps[q] = g.steps[q];
+  for (auto& e : g.blockLevels) {
+    uint32_t i = (uint32_t)(e.first >> 32), j = (uint32_t)e.first;
+    blevel[(size_t)i * g.M + j] = (int8_t)e.second;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// kind 0: Camera(theta, phi, r, speed)            BT/Camera.h:27
+// kind 1: Camera(theta, phi, r, br, btheta, bphi)  BT/Camera.h:40
+void btref_camera(int kind, double a, double theta, double phi, double r,
+                  double p0, double p1, double p2, double* out12) {
+  BlackHole bh(a);
+  Camera c = kind == 0 ? Camera(theta, phi, r, p0)
+                       : Camera(theta, phi, r, p0, p1, p2);
+  cam_to_array(c, out12);
+}
+
+// Grid::integration_wrapper over n rays, split into nthreads disjoint slices
+// (each slice on its own Grid object; the wrapper only reads the camera and
+// the spin globals).
+void btref_integrate_rays(const double* cam12, double a, const double* theta,
+                          const double* phi, long n, double* theta_out,
+                          double* phi_out, int32_t* steps, int nthreads) {
+  Quiet q;
+  BlackHole bh(a);
+  Camera cam = cam_from_array(cam12);
+  if (nthreads < 1) nthreads = 1;
+  if (n < nthreads * 4) nthreads = 1;
+  auto work = [&](long lo, long hi) {
+    Grid g;
+    g.cam = &cam;
+    g.black = &bh;
+    int m = (int)(hi - lo);
+    std::vector<double> th(theta + lo, theta + hi), ph(phi + lo, phi + hi);
+    std::vector<int> st(m);
+    g.integration_wrapper(th, ph, m, st);
+    for (int k = 0; k < m; k++) {
+      theta_out[lo + k] = th[k];
+      phi_out[lo + k] = ph[k];
+      steps[lo + k] = st[k];
+    }
+  };
+  if (nthreads == 1) { work(0, n); return; }
+  std::vector<std::thread> ts;
+  for (int t = 0; t < nthreads; t++) {
+    long lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
+    ts.emplace_back(work, lo, hi);
+  }
+  for (auto& t : ts) t.join();
+}
+
+// Adaptive grid.
+//   order 0: raytrace only (no T-vertex fix)
+//   order 1: raytrace, then fixTvertices over blockLevels sorted by
+//            (level ascending, key ascending)
+//   order 2: raytrace, then fixTvertices in the unordered_map's own
+//            iteration order, exactly as the constructor does (BT/Grid.h:620)
+// Returns the number of CamToCel entries; the hash table of :623 is skipped.
+long btref_grid_build(int maxlevel, int startlevel, int angle,
+                      const double* cam12, double a, int order, double* theta,
+                      double* phi, uint8_t* exists, int32_t* steps,
+                      int8_t* blevel) {
+  Quiet q;
+  BlackHole bh(a);
+  Camera cam = cam_from_array(cam12);
+  Grid g;
+  // Field set-up of Grid::Grid, BT/Grid.h:606-616
+  g.MAXLEVEL = maxlevel;
+  g.STARTLVL = startlevel;
+  g.cam = &cam;
+  g.black = &bh;
+  g.equafactor = angle ? 1 : 0;
+  g.N = (uint32_t)round(pow(2, g.MAXLEVEL) / (2 - g.equafactor) + 1);
+  g.STARTN = (uint32_t)round(pow(2, startlevel) / (2 - g.equafactor) + 1);
+  g.M = (2 - g.equafactor) * 2 * (g.N - 1);
+  g.STARTM = (2 - g.equafactor) * 2 * (g.STARTN - 1);
+  g.steps = std::vector<int>(g.M * g.N);
+  g.raytrace();
+  if (order == 1) {
+    std::vector<std::pair<uint64_t, int>> bl(g.blockLevels.begin(),
+                                             g.blockLevels.end());
+    std::sort(bl.begin(), bl.end(), [](const std::pair<uint64_t, int>& x,
+                                       const std::pair<uint64_t, int>& y) {
+      return x.second != y.second ? x.second < y.second : x.first < y.first;
+    });
+    for (auto& b : bl) g.fixTvertices(b);
+  } else if (order == 2) {
+    for (auto block : g.blockLevels) g.fixTvertices(block);
+  }
+  export_grid(g, theta, phi, exists, steps, blevel);
+  return (long)g.CamToCel.size();
+}
+
+// The full reference constructor (incl. the perfect hash), timed: the
+// faithful single-thread CPU baseline.  Returns wall seconds; *nrays = number
+// of CamToCel entries.
+double btref_grid_time(int maxlevel, int startlevel, int angle,
+                       const double* cam12, double a, long* nentries) {
+  Quiet q;
+  BlackHole bh(a);
+  Camera cam = cam_from_array(cam12);
+  auto t0 = std::chrono::steady_clock::now();
+  Grid g(maxlevel, startlevel, angle != 0, &cam, &bh);
+  auto t1 = std::chrono::steady_clock::now();
+  if (nentries) *nentries = (long)g.CamToCel.size();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+}  // extern "C"
