@@ -11,5 +11,7 @@ from ._lib import (BtError, PRECISION_MIXED, PRECISION_PLAIN, RAY_CAPTURED,  # n
 from .host import (BlackHole, Camera, Grid, IntegOpts, grid_dims,  # noqa: F401
                    integrate_rays, integrate_rays_host)
 
-__all__ = ["BlackHole", "Camera", "Grid", "IntegOpts", "grid_dims", "integrate_rays",
+from .render import Environment, Renderer, StarProcessor, Viewer  # noqa: F401
+
+__all__ = ["Environment", "Renderer", "StarProcessor", "Viewer", "BlackHole", "Camera", "Grid", "IntegOpts", "grid_dims", "integrate_rays",
            "integrate_rays_host", "BtError", "lib"]

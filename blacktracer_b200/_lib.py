@@ -43,7 +43,23 @@ class bt_grid_info(C.Structure):
                 ("blevel", C.c_void_p), ("status", C.c_void_p)]
 
 
+class bt_frame(C.Structure):
+    _fields_ = [("grid", C.c_void_p), ("grid_rows", C.c_int32), ("grid_cols", C.c_int32),
+                ("grid_level", C.c_int32), ("view", C.c_void_p), ("hor", C.c_float),
+                ("ver", C.c_float), ("cam", C.c_float * 7), ("env", C.c_void_p),
+                ("stars", C.c_void_p), ("map", C.c_int32), ("star", C.c_int32),
+                ("lr", C.c_int32), ("step", C.c_int32), ("diffraction", C.c_int32),
+                ("out", C.c_void_p)]
+
+
+class bt_map_buffers(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("thphi", "gap", "bh", "area", "light",
+                                          "stars_img", "env_img")]
+
+
 _vp = C.c_void_p
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
 _SIGS = {
     "bt_camera_static": (C.c_int, [C.c_double] * 5 + [C.POINTER(bt_camera)]),
     "bt_camera_orbit": (C.c_int, [C.c_double] * 7 + [C.POINTER(bt_camera)]),
@@ -63,6 +79,20 @@ _SIGS = {
     "bt_grid_export_dense": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_grid_map_export": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), _vp]),
+    "bt_view_sphere": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
+    "bt_env_create": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp), _vp]),
+    "bt_env_destroy": (None, [_vp]),
+    "bt_env_sat": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "bt_stars_tree_size": (C.c_int, [C.c_int]),
+    "bt_stars_build_tree": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_float,
+                                      _vp, _vp, _vp, C.POINTER(C.c_int)]),
+    "bt_stars_create": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int,
+                                  C.POINTER(_vp), _vp]),
+    "bt_stars_destroy": (None, [_vp]),
+    "bt_map_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(_vp)]),
+    "bt_map_destroy": (None, [_vp]),
+    "bt_map_render": (C.c_int, [_vp, C.POINTER(bt_frame), _vp]),
+    "bt_map_scratch": (C.c_int, [_vp, C.POINTER(bt_map_buffers)]),
     "bt_last_error": (C.c_char_p, []),
     "bt_version": (C.c_char_p, []),
 }

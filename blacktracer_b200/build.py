@@ -29,6 +29,9 @@ UNITS = {
     "integrate.cu": ["--fmad=false"],
     "grid.cu": ["--fmad=false"],
     "mixed.cu": [],
+    "map.cu": ["--fmad=false"],
+    "stars.cu": ["--fmad=false"],
+    "map_api.cu": [],
 }
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
            if f.endswith((".h", ".cuh"))] + [os.path.join(ROOT, "include", "blacktracer.h")]

@@ -1,0 +1,284 @@
+// map.cu -- the per-pixel map on the device: grid interpolation, black-hole
+// mask, solid angles and their smoothing, the environment map's summed-area
+// table and its integration over each projected pixel, with lensing and
+// redshift (annemiekie/BlackTracer BT/MakeImageKernel.cu:458-751 and the
+// summed-area table of cudaPrep :1312-1330).
+//
+// Thread mapping: x -> column j, y -> row i, so consecutive lanes touch
+// consecutive pixels (the reference maps x to rows, which strides every
+// access by a full row).  Compiled with --fmad=false so the FP32 arithmetic
+// rounds like the reference's (see map_math.cuh).
+#include <cstring>
+#include <new>
+
+#include "bt_internal.h"
+#include "map_math.cuh"
+#include "map_internal.h"
+
+namespace bt {
+
+using namespace mapm;
+
+constexpr int TX = 32, TY = 8;
+
+static dim3 grid2(int w, int h) {
+  return dim3((unsigned)((w + TX - 1) / TX), (unsigned)((h + TY - 1) / TY));
+}
+
+// Camera-sky corners of an equirectangular output, Viewer::makeSphereView
+// (BT/Viewer.h:82-88): {i*PI/H, j*PI2/W} evaluated in double, stored float.
+__global__ void k_view_sphere(float2* view, int W, int H) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  if (i > H || j > W) return;
+  view[(size_t)i * (W + 1) + j] =
+      make_float2((float)(1.f * i * kPi / H), (float)(1.f * j * kPi2 / W));
+}
+
+// pixInterpolation, G = 1 (BT/MakeImageKernel.cu:458-515): celestial
+// (theta, phi) and block size at every pixel corner.
+__global__ void k_pixinterp(const float2* __restrict__ view, int M, int N,
+                            GridRef G, int gridlvl, float hor, float ver,
+                            float2* __restrict__ thphi, int* __restrict__ gap) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  const int M1 = M + 1;
+  if (i > N || j > M) return;
+  const float2 v = view[(size_t)i * M1 + j];
+  const float theta = v.x + ver;
+  const float phi = fmodf(v.y + hor + PI2, PI2);
+  int g = 0;
+  thphi[(size_t)i * M1 + j] = interpolate_pix(G, theta, phi, gridlvl, g);
+  gap[(size_t)i * M1 + j] = g;
+}
+
+// findBlackPixels + findArea (BT/MakeImageKernel.cu:539-568), fused.
+__global__ void k_bh_area(const float2* __restrict__ thphi, int M, int N,
+                          uint8_t* __restrict__ bh, float* __restrict__ area) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  if (i >= N || j >= M) return;
+  float t[4], p[4];
+  bool picheck = false;
+  const bool ok = pixel_corners(thphi, i * (M + 1) + j, M, t, p, picheck, 0.f);
+  bh[(size_t)i * M + j] = ok ? 0 : 1;
+  // the reference computes the area for captured pixels too, from the
+  // partially wrapped corners; those values are never read
+  area[(size_t)i * M + j] = ok ? pixel_solid_angle(t, p) : 0.f;
+}
+
+__device__ __forceinline__ int corner_gap(const int* gap, int i, int j, int M) {
+  const int M1 = M + 1;
+  return max(max(gap[i * M1 + j], gap[i * M1 + M1 + j]),
+             max(gap[i * M1 + j + 1], gap[i * M1 + M1 + j + 1]));
+}
+
+// smoothAreaH (BT/MakeImageKernel.cu:570-591): box filter along the row,
+// width max(corner gaps)/2, over non-black pixels; the column wraps.
+__global__ void k_smooth_h(float* __restrict__ out, const float* __restrict__ area,
+                           const uint8_t* __restrict__ bh, const int* __restrict__ gap,
+                           int M, int N) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  if (i >= N || j >= M) return;
+  if (bh[(size_t)i * M + j] == 1) return;
+  const int fs = corner_gap(gap, i, j, M) / 2;
+  float sum = 0.f;
+  int count = 0;
+  const size_t row = (size_t)i * M;
+  for (int h = -fs; h <= fs; h++) {
+    int jj = (j + h) % M;
+    if (jj < 0) jj += M;
+    if (bh[row + jj] == 0) {
+      sum += area[row + jj];
+      count++;
+    }
+  }
+  out[row + j] = sum / (1.f * count);
+}
+
+// smoothAreaV (BT/MakeImageKernel.cu:593-616): the same along the column,
+// clamped at the image edges; writes back into `area`.
+__global__ void k_smooth_v(const float* __restrict__ in, float* __restrict__ area,
+                           const uint8_t* __restrict__ bh, const int* __restrict__ gap,
+                           int M, int N) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  if (i >= N || j >= M) return;
+  if (bh[(size_t)i * M + j] == 1) return;
+  const int fs = corner_gap(gap, i, j, M) / 2;
+  float sum = 0.f;
+  const int minv = max(0, i - fs);
+  const int maxv = min(N - 1, i + fs);
+  int count = 0;
+  for (int h = minv; h <= maxv; h++) {
+    if (bh[(size_t)h * M + j] == 0) {
+      sum += in[(size_t)h * M + j];
+      count++;
+    }
+  }
+  area[(size_t)i * M + j] = sum / (1.f * count);
+}
+
+// Summed-area table of the environment map, one thread per column, rows in
+// order: the reference's sequential float accumulation (cudaPrep,
+// BT/MakeImageKernel.cu:1312-1330).  Channels: B^2.2*A, G^2.2*A, R^2.2*A, A.
+__global__ void k_sat(const uint8_t* __restrict__ bgr, int rows, int cols,
+                      float4* __restrict__ sat) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= cols) return;
+  const float pxsz = PI2 / (1.f * cols);
+  float4 prev = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float phi[4] = {pxsz * q, pxsz * q, pxsz * (q + 1), pxsz * (q + 1)};
+  for (int p = 0; p < rows; p++) {
+    const float theta[4] = {pxsz * (p + 1), pxsz * p, pxsz * p, pxsz * (p + 1)};
+    const float area = calc_area(theta, phi);
+    const uint8_t* px = bgr + ((size_t)p * cols + q) * 3;
+    prev.x += powf((float)px[0], 2.2f) * area;
+    prev.y += powf((float)px[1], 2.2f) * area;
+    prev.z += powf((float)px[2], 2.2f) * area;
+    prev.w += area;
+    sat[(size_t)p * cols + q] = prev;
+  }
+}
+
+// Summed-area table read at the reference's linear index.  The reference
+// can index a row before the table (int(thMin/pixSize)-1 = -1, :664) and up
+// to a row past it (theta = pi, or a phi that rounds to `cols`); such reads
+// return zero here.
+__device__ __forceinline__ float4 sat_lin(const float4* sat, long idx, long total) {
+  if (idx < 0 || idx >= total) return make_float4(0.f, 0.f, 0.f, 0.f);
+  return sat[idx];
+}
+
+// distortEnvironmentMap (BT/MakeImageKernel.cu:631-751): integrate the
+// environment over the projected pixel column by column with two
+// summed-area reads per column, gamma, HSP, lensing and redshift; BGRA8.
+__global__ void k_env(const float2* __restrict__ thphi, uchar4* __restrict__ out,
+                      const uint8_t* __restrict__ bh, int rows, int cols, int M,
+                      int N, const float4* __restrict__ sat, Cam7 cam,
+                      const float* __restrict__ solidangle,
+                      const float2* __restrict__ view, int lr) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  if (i >= N || j >= M) return;
+  const size_t ij = (size_t)i * M + j;
+  const long total = (long)rows * cols;
+  float4 color = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (bh[ij] == 0) {
+    float t[4], p[4];
+    bool picheck = false;
+    const int ind = i * (M + 1) + j;
+    const bool ok = pixel_corners(thphi, ind, M, t, p, picheck, 0.f);
+    if (ok && ind > 0) {  // pixel (0,0) is never coloured by the reference
+      const float pixSize = PI / float(rows);
+      const float phMax = fmaxf(fmaxf(p[0], p[1]), fmaxf(p[2], p[3]));
+      const float phMin = fminf(fminf(p[0], p[1]), fminf(p[2], p[3]));
+      const int pixMax = int(phMax / pixSize);
+      const int pixMin = int(phMin / pixSize);
+      int pixNum = pixMax - pixMin + 1;
+      if (pixNum > 1 && pixMax * pixSize > phMax) pixNum -= 1;
+      if (pixNum == 1) {
+        const float thMax = fmaxf(fmaxf(t[0], t[1]), fmaxf(t[2], t[3]));
+        const float thMin = fminf(fminf(t[0], t[1]), fminf(t[2], t[3]));
+        const float4 mx = sat_lin(sat, (long)int(thMax / pixSize) * cols + pixMin, total);
+        const float4 mn = sat_lin(sat, (long)(int(thMin / pixSize) - 1) * cols + pixMin, total);
+        color.x += mx.x - mn.x;
+        color.y += mx.y - mn.y;
+        color.z += mx.z - mn.z;
+        color.w += mx.w - mn.w;
+      } else if (pixNum < cols) {
+        float max1 = -100, min1 = cols + 1, max2 = -100, min2 = cols + 1;
+        for (int s = 0; s <= pixNum; s++) {
+          const float cp = (pixMin + s) * pixSize;
+          for (int q = 0; q < 4; q++) {
+            const float ap = p[q], bp = p[(q + 1) % 4];
+            const float at = t[q], bt = t[(q + 1) % 4];
+            if ((cp - ap) * (cp - bp) <= 0) {
+              const float ct = at + (bt - at) / (bp - ap) * (cp - ap);
+              min2 = ct < min2 ? ct : min2;
+              max2 = ct > max2 ? ct : max2;
+            }
+          }
+          if (s > 0) {
+            const float max_ = fmaxf(max1, max2);
+            const float min_ = fminf(min1, min2);
+            const int col = (pixMin + s) % cols;
+            const long index1 = (long)int(max_ / pixSize) * cols + col;
+            const long index2 = (long)(int(min_ / pixSize) - 1) * cols + col;
+            const float4 mx = sat_lin(sat, index1, total);
+            const float4 mn = index2 > 0 ? sat_lin(sat, index2, total)
+                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+            color.x += mx.x - mn.x;
+            color.y += mx.y - mn.y;
+            color.z += mx.z - mn.z;
+            color.w += mx.w - mn.w;
+          }
+          max1 = max2;
+          min1 = min2;
+        }
+      } else {
+        const float thMax = fmaxf(fmaxf(t[0], t[1]), fmaxf(t[2], t[3]));
+        const float thMin = fminf(fminf(t[0], t[1]), fminf(t[2], t[3]));
+        const long thMaxPix = (long)int(thMax / pixSize) * cols;
+        const long thMinPix = (long)int(thMin / pixSize) * cols;
+        for (int q = 0; q < pixNum; q++) {
+          const int col = (pixMin + q) % cols;
+          const float4 mx = sat_lin(sat, thMaxPix + col, total);
+          const float4 mn = sat_lin(sat, thMinPix + col, total);
+          color.x += mx.x - mn.x;
+          color.y += mx.y - mn.y;
+          color.z += mx.z - mn.z;
+          color.w += mx.w - mn.w;
+        }
+      }
+      color.x = fminf(255.f, powf(color.x / color.w, 1.f / 2.2f));
+      color.y = fminf(255.f, powf(color.y / color.w, 1.f / 2.2f));
+      color.z = fminf(255.f, powf(color.z / color.w, 1.f / 2.2f));
+      float H, S, P;
+      rgb_to_hsp(color.z / 255.f, color.y / 255.f, color.x / 255.f, H, S, P);
+      if (lr) {
+        float redshft, frac;
+        lensing_redshift(t, p, M, ind, cam.v, view, frac, redshft, solidangle[ij]);
+        P *= frac;
+        P = powf(P, redshft);
+      }
+      hsp_to_rgb(H, S, fminf(1.f, P), color.z, color.y, color.x);
+    }
+  }
+  out[ij] = make_uchar4((unsigned char)min(255, int(color.x * 255)),
+                        (unsigned char)min(255, int(color.y * 255)),
+                        (unsigned char)min(255, int(color.z * 255)), 255);
+}
+
+int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s) {
+  const int M = S.M, N = S.N;
+  GridRef G{F.grid, F.GM, F.GN};
+  k_pixinterp<<<grid2(M + 1, N + 1), dim3(TX, TY), 0, s>>>(
+      F.view, M, N, G, F.gridlvl, F.hor, F.ver, S.thphi, S.gap);
+  k_bh_area<<<grid2(M, N), dim3(TX, TY), 0, s>>>(S.thphi, M, N, S.bh, S.area);
+  k_smooth_h<<<grid2(M, N), dim3(TX, TY), 0, s>>>(S.area_tmp, S.area, S.bh, S.gap, M, N);
+  k_smooth_v<<<grid2(M, N), dim3(TX, TY), 0, s>>>(S.area_tmp, S.area, S.bh, S.gap, M, N);
+  BT_CUDA_TRY(cudaGetLastError());
+  if (F.map && F.env) {
+    k_env<<<grid2(M, N), dim3(TX, TY), 0, s>>>(
+        S.thphi, (uchar4*)F.out_bg, S.bh, F.env->rows, F.env->cols, M, N,
+        F.env->sat, F.cam, S.area, F.view, F.lr);
+    BT_CUDA_TRY(cudaGetLastError());
+  }
+  return BT_OK;
+}
+
+int launch_view_sphere(float2* view, int W, int H, cudaStream_t s) {
+  k_view_sphere<<<grid2(W + 1, H + 1), dim3(TX, TY), 0, s>>>(view, W, H);
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
+int launch_sat(const uint8_t* bgr, int rows, int cols, float4* sat, cudaStream_t s) {
+  k_sat<<<(cols + 127) / 128, 128, 0, s>>>(bgr, rows, cols, sat);
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
+}  // namespace bt

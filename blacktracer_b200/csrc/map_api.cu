@@ -1,0 +1,205 @@
+// map_api.cu -- C ABI of the per-pixel map: resident environment maps,
+// renderers (per-resolution scratch) and the frame call that replaces
+// makeImage / cudaPrep (annemiekie/BlackTracer BT/MakeImageKernel.cu:1206-1559).
+#include <cstring>
+#include <new>
+
+#include "bt_internal.h"
+#include "map_internal.h"
+
+struct bt_env {
+  bt::EnvMap e;
+};
+
+struct bt_map {
+  bt::MapScratch S;
+  uint8_t* tmp_img;  // env image when stars are composited on top
+};
+
+using namespace bt;
+
+namespace {
+
+void map_free(bt_map* m) {
+  void* ptrs[] = {m->S.thphi, m->S.gap,   m->S.bh,        m->S.area,
+                  m->S.area_tmp, m->S.light, m->S.light2, m->S.stars_img,
+                  m->S.flag, m->S.cells, m->S.diff_list, m->S.diff_count,
+                  m->S.heavy_list, m->S.heavy_count, m->tmp_img};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+}
+
+}  // namespace
+
+extern "C" {
+
+int bt_env_create(const uint8_t* bgr, int rows, int cols, int bgr_on_device,
+                  bt_env** out, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(out && bgr, "NULL pointer");
+  BT_ARG_CHECK(rows > 0 && cols > 0 && (size_t)rows * cols <= ((size_t)1 << 31),
+               "environment size out of range");
+  *out = nullptr;
+  cudaStream_t s = (cudaStream_t)stream;
+  bt_env* e = new (std::nothrow) bt_env;
+  if (!e) return BT_ERR_NOMEM;
+  e->e.rows = rows;
+  e->e.cols = cols;
+  e->e.sat = nullptr;
+  const size_t n = (size_t)rows * cols;
+  cudaError_t err = cudaMalloc((void**)&e->e.sat, n * sizeof(float4));
+  if (err != cudaSuccess) {
+    delete e;
+    set_error("summed-area table allocation failed: %s", cudaGetErrorString(err));
+    return BT_ERR_NOMEM;
+  }
+  const uint8_t* src = bgr;
+  uint8_t* staged = nullptr;
+  if (!bgr_on_device) {
+    err = cudaMalloc((void**)&staged, n * 3);
+    if (err == cudaSuccess)
+      err = cudaMemcpyAsync(staged, bgr, n * 3, cudaMemcpyHostToDevice, s);
+    if (err != cudaSuccess) {
+      if (staged) cudaFree(staged);
+      cudaFree(e->e.sat);
+      delete e;
+      set_error("environment upload failed: %s", cudaGetErrorString(err));
+      return BT_ERR_CUDA;
+    }
+    src = staged;
+  }
+  int rc = launch_sat(src, rows, cols, e->e.sat, s);
+  if (staged) {
+    cudaStreamSynchronize(s);
+    cudaFree(staged);
+  }
+  if (rc) {
+    cudaFree(e->e.sat);
+    delete e;
+    return rc;
+  }
+  *out = e;
+  return BT_OK;
+}
+
+void bt_env_destroy(bt_env* e) {
+  if (!e) return;
+  if (e->e.sat) cudaFree(e->e.sat);
+  delete e;
+}
+
+int bt_env_sat(const bt_env* e, const float** sat, int32_t* rows, int32_t* cols) {
+  BT_ARG_CHECK(e && sat, "NULL pointer");
+  *sat = (const float*)e->e.sat;
+  if (rows) *rows = e->e.rows;
+  if (cols) *cols = e->e.cols;
+  return BT_OK;
+}
+
+int bt_map_create(int width, int height, bt_map** out) {
+  clear_error();
+  BT_ARG_CHECK(out != nullptr, "NULL pointer");
+  BT_ARG_CHECK(width > 0 && height > 0 && (size_t)width * height <= ((size_t)1 << 28),
+               "image size out of range");
+  *out = nullptr;
+  bt_map* m = new (std::nothrow) bt_map;
+  if (!m) return BT_ERR_NOMEM;
+  std::memset(m, 0, sizeof(*m));
+  MapScratch& S = m->S;
+  S.M = width;
+  S.N = height;
+  const size_t np = (size_t)width * height;
+  const size_t nc = (size_t)(width + 1) * (height + 1);
+  cudaError_t e = cudaSuccess;
+#define MALLOC(p, bytes) \
+  if (e == cudaSuccess) e = cudaMalloc((void**)&(p), (bytes));
+  MALLOC(S.thphi, nc * sizeof(float2));
+  MALLOC(S.gap, nc * sizeof(int));
+  MALLOC(S.bh, np);
+  MALLOC(S.area, np * sizeof(float));
+  MALLOC(S.area_tmp, np * sizeof(float));
+  MALLOC(S.light, np * 3 * sizeof(float));
+  MALLOC(S.light2, np * 3 * sizeof(float));
+  MALLOC(S.stars_img, np * 4);
+  MALLOC(S.flag, np);
+  MALLOC(S.diff_list, np * sizeof(uint32_t));
+  MALLOC(S.diff_count, sizeof(uint32_t));
+  MALLOC(S.heavy_list, np * sizeof(uint32_t));
+  MALLOC(S.heavy_count, sizeof(uint32_t));
+  MALLOC(m->tmp_img, np * 4);
+#undef MALLOC
+  if (e != cudaSuccess) {
+    map_free(m);
+    delete m;
+    set_error("renderer allocation (%dx%d) failed: %s", width, height,
+              cudaGetErrorString(e));
+    return BT_ERR_NOMEM;
+  }
+  *out = m;
+  return BT_OK;
+}
+
+void bt_map_destroy(bt_map* m) {
+  if (!m) return;
+  map_free(m);
+  delete m;
+}
+
+int bt_view_sphere(float* view, int width, int height, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(view && width > 0 && height > 0, "invalid view arguments");
+  return launch_view_sphere((float2*)view, width, height, (cudaStream_t)stream);
+}
+
+int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(m && f, "NULL pointer");
+  BT_ARG_CHECK(f->grid && f->view && f->out, "grid, view and out are required");
+  BT_ARG_CHECK(f->grid_rows > 1 && f->grid_cols > 1 && f->grid_level >= 1,
+               "invalid grid description");
+  BT_ARG_CHECK(!f->map || f->env, "map requested without an environment");
+  BT_ARG_CHECK(!f->star || f->stars, "stars requested without a star set");
+  BT_ARG_CHECK(f->step >= 0 && f->step <= 2, "step out of [0, 2]");
+  cudaStream_t s = (cudaStream_t)stream;
+  MapFrame F;
+  F.grid = (const float2*)f->grid;
+  F.GN = f->grid_rows;
+  F.GM = f->grid_cols;
+  F.gridlvl = f->grid_level;
+  F.view = (const float2*)f->view;
+  F.hor = f->hor;
+  F.ver = f->ver;
+  for (int q = 0; q < 7; q++) F.cam.v[q] = f->cam[q];
+  F.env = f->env ? &f->env->e : nullptr;
+  F.stars = f->stars ? stars_internal(f->stars) : nullptr;
+  F.map = f->map;
+  F.star = f->star;
+  F.lr = f->lr;
+  F.step = f->step;
+  F.diffraction = f->diffraction;
+  F.out = f->out;
+  // environment into the output directly, or into a temporary when stars
+  // are composited on top (addStarsAndBackground)
+  F.out_bg = (f->star && f->map) ? m->tmp_img : f->out;
+  int rc = map_run_env(m->S, F, s);
+  if (rc) return rc;
+  if (f->star) {
+    rc = map_run_stars(m->S, F, s);
+    if (rc) return rc;
+  }
+  return BT_OK;
+}
+
+int bt_map_scratch(const bt_map* m, bt_map_buffers* b) {
+  BT_ARG_CHECK(m && b, "NULL pointer");
+  b->thphi = (const float*)m->S.thphi;
+  b->gap = m->S.gap;
+  b->bh = m->S.bh;
+  b->area = m->S.area;
+  b->light = m->S.light;
+  b->stars_img = m->S.stars_img;
+  b->env_img = m->tmp_img;
+  return BT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,61 @@
+// map_internal.h -- shared declarations of the per-pixel map.
+#pragma once
+
+#include "bt_internal.h"
+
+namespace bt {
+
+struct Cam7 {
+  float v[7];  // Camera::getParamArray, BT/Camera.h:67-78
+};
+
+// Resident environment map: its summed-area table in HBM.
+struct EnvMap {
+  int rows, cols;
+  float4* sat;  // rows*cols
+};
+
+// Per-resolution scratch of the renderer (the reference's dev_in, dev_gap,
+// dev_bh, dev_area, dev_areaSmooth, star buffers).
+struct MapScratch {
+  int M, N;             // output width, height
+  float2* thphi;        // (N+1)(M+1) celestial corners
+  int* gap;             // (N+1)(M+1) block size at each corner
+  uint8_t* bh;          // N*M black-hole mask
+  float* area;          // N*M solid angle (smoothed in place)
+  float* area_tmp;      // N*M
+  float* light;         // N*M*3 summed star light
+  float* light2;        // N*M*3 star light after diffraction
+  uint8_t* stars_img;   // N*M*4 star image (BGRA8)
+  uint8_t* flag;        // N*M: pixel holds at least one star
+  float3* cells;        // N*M*(2s+1)^2 splat cells (lazy)
+  int cells_fw;         // 2s+1 the cells were sized for
+  uint32_t* diff_list;  // bright pixels (diffraction)
+  uint32_t* diff_count;
+  uint32_t* heavy_list; // pixels deferred to the warp-cooperative star path
+  uint32_t* heavy_count;
+};
+
+struct StarSet;
+const StarSet* stars_internal(const bt_stars* s);
+
+// One frame's inputs.
+struct MapFrame {
+  const float2* grid;   // map grid GN x GM (rows = GN1 for half grids)
+  int GN, GM, gridlvl;
+  const float2* view;   // (N+1)(M+1)
+  float hor, ver;
+  Cam7 cam;
+  const EnvMap* env;
+  const StarSet* stars;
+  int map, star, lr, step, diffraction;
+  uint8_t* out_bg;      // N*M*4 environment (or final) image
+  uint8_t* out;         // N*M*4 final image
+};
+
+int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s);
+int map_run_stars(MapScratch& S, const MapFrame& F, cudaStream_t s);
+int launch_view_sphere(float2* view, int W, int H, cudaStream_t s);
+int launch_sat(const uint8_t* bgr, int rows, int cols, float4* sat, cudaStream_t s);
+
+}  // namespace bt

@@ -1,0 +1,206 @@
+"""Host mirror of the reference's map-side interfaces.
+
+  Viewer(viewangle, offUp, offRight, pixw, pixh, sphere)   BT/Viewer.h:20-33
+  StarProcessor (star list -> kd tree)                    BT/StarProcessor.h:34-64
+  Distorter(grids, viewer, stars, cams) -> makeImage      BT/Distorter.h:166-176
+plus the resident pieces the B200 design keeps in HBM: Environment (the
+summed-area table of an environment map) and Renderer (per-resolution
+scratch).  Device buffers are torch CUDA tensors; compute is the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .host import Camera, Grid, _stream_ptr, _torch
+
+
+class Viewer:
+    """Camera-sky corner directions of the output pixels (BT/Viewer.h).
+
+    Only the equirectangular sphere view (makeSphereView) is implemented on
+    the device; viewMatrix is a ((pixh+1)*(pixw+1), 2) float32 CUDA tensor."""
+
+    def __init__(self, viewangle, offUp, offRight, pixw, pixh, sphere=True, stream=None):
+        if not sphere:
+            raise NotImplementedError("perspective camera view: not built")
+        torch = _torch()
+        self.pixelwidth, self.pixelheight = int(pixw), int(pixh)
+        self.viewAngleWide = float(viewangle)
+        self.viewMatrix = torch.empty(((pixh + 1) * (pixw + 1), 2), dtype=torch.float32,
+                                      device="cuda")
+        L.check(L.lib().bt_view_sphere(self.viewMatrix.data_ptr(), self.pixelwidth,
+                                       self.pixelheight, _stream_ptr(stream)))
+
+
+class Environment:
+    """A resident environment map (BGR8, rows x cols, rows = cols/2)."""
+
+    def __init__(self, bgr, stream=None):
+        torch = _torch()
+        if isinstance(bgr, np.ndarray):
+            bgr = np.ascontiguousarray(bgr, dtype=np.uint8)
+            rows, cols = bgr.shape[:2]
+            ptr, on_dev = bgr.ctypes.data, 0
+            self._keep = bgr
+        else:
+            bgr = bgr.contiguous()
+            rows, cols = bgr.shape[:2]
+            ptr, on_dev = bgr.data_ptr(), 1
+            self._keep = bgr
+        self.rows, self.cols = int(rows), int(cols)
+        h = C.c_void_p()
+        L.check(L.lib().bt_env_create(ptr, self.rows, self.cols, on_dev, C.byref(h),
+                                      _stream_ptr(stream)))
+        self._h = h
+
+    def sat(self):
+        """The summed-area table as a (rows, cols, 4) float32 CUDA tensor view."""
+        torch = _torch()
+        p = C.c_void_p()
+        L.check(L.lib().bt_env_sat(self._h, C.byref(p), None, None))
+        return _device_view(p.value, (self.rows, self.cols, 4), torch.float32)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None:
+            try:
+                L.lib().bt_env_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+def _device_view(ptr, shape, dtype):
+    """A torch tensor aliasing library-owned device memory (copy it if it must
+    outlive the owner)."""
+    torch = _torch()
+
+    class _Arr:
+        __cuda_array_interface__ = {
+            "shape": tuple(shape), "typestr": {torch.float32: "<f4", torch.int32: "<i4",
+                                               torch.uint8: "|u1"}[dtype],
+            "data": (ptr, False), "version": 2, "strides": None}
+    return torch.as_tensor(_Arr(), device="cuda")
+
+
+class StarProcessor:
+    """BT/StarProcessor.h: a star list arranged in the reference's binary
+    tree (starPos, starMag, binaryStarTree) and uploaded to the device."""
+
+    def __init__(self, theta, phi, mag, bv, treeLevel=8, magnitudeCut=1000.0,
+                 psf=None, stream=None):
+        lib = L.lib()
+        theta = np.ascontiguousarray(theta, dtype=np.float32)
+        phi = np.ascontiguousarray(phi, dtype=np.float32)
+        mag = np.ascontiguousarray(mag, dtype=np.float32)
+        bv = np.ascontiguousarray(bv, dtype=np.float32)
+        n = theta.size
+        self.treeLevel = int(treeLevel)
+        tsize = lib.bt_stars_tree_size(self.treeLevel)
+        self.starPos = np.empty(2 * n, dtype=np.float32)
+        self.starMag = np.empty(2 * n, dtype=np.float32)
+        self.binaryStarTree = np.empty(tsize, dtype=np.int32)
+        kept = C.c_int()
+        L.check(lib.bt_stars_build_tree(theta.ctypes.data, phi.ctypes.data, mag.ctypes.data,
+                                        bv.ctypes.data, n, self.treeLevel,
+                                        float(magnitudeCut), self.starPos.ctypes.data,
+                                        self.starMag.ctypes.data,
+                                        self.binaryStarTree.ctypes.data, C.byref(kept)))
+        self.starSize = kept.value
+        self.starPos = self.starPos[: 2 * self.starSize].copy()
+        self.starMag = self.starMag[: 2 * self.starSize].copy()
+        self.psf = None if psf is None else np.ascontiguousarray(psf, dtype=np.uint8)
+        h = C.c_void_p()
+        L.check(lib.bt_stars_create(self.starPos.ctypes.data, self.starMag.ctypes.data,
+                                    self.starSize, self.binaryStarTree.ctypes.data,
+                                    self.treeLevel,
+                                    None if self.psf is None else self.psf.ctypes.data,
+                                    0 if self.psf is None else self.psf.shape[0],
+                                    C.byref(h), _stream_ptr(stream)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None:
+            try:
+                L.lib().bt_stars_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+class Renderer:
+    """Per-resolution device scratch + the frame call (makeImage, G = 1)."""
+
+    def __init__(self, width, height):
+        self.width, self.height = int(width), int(height)
+        h = C.c_void_p()
+        L.check(L.lib().bt_map_create(self.width, self.height, C.byref(h)))
+        self._h = h
+
+    def render(self, grid: Grid, viewer: Viewer, cam: Camera, env: Environment | None = None,
+               stars: StarProcessor | None = None, lr=True, step=1, diffraction=False,
+               hor=0.0, ver=0.0, out=None, stream=None):
+        """Returns (or fills) an (H, W, 4) uint8 BGRA CUDA tensor."""
+        torch = _torch()
+        gp, rows, cols, _ = grid.map_grid()
+        if out is None:
+            out = torch.empty((self.height, self.width, 4), dtype=torch.uint8, device="cuda")
+        f = L.bt_frame()
+        f.grid, f.grid_rows, f.grid_cols, f.grid_level = gp, rows, cols, grid.MAXLEVEL
+        f.view = viewer.viewMatrix.data_ptr()
+        f.hor, f.ver = hor, ver
+        f.cam[:] = [float(x) for x in cam.getParamArray()]
+        f.env = env._h if env is not None else None
+        f.stars = stars._h if stars is not None else None
+        f.map, f.star, f.lr = int(env is not None), int(stars is not None), int(bool(lr))
+        f.step, f.diffraction = int(step), int(bool(diffraction))
+        f.out = out.data_ptr()
+        L.check(L.lib().bt_map_render(self._h, C.byref(f), _stream_ptr(stream)))
+        return out
+
+    def render_raw(self, grid_ptr, grid_rows, grid_cols, grid_level, view, cam7, env=None,
+                   stars=None, lr=True, step=1, diffraction=False, hor=0.0, ver=0.0,
+                   out=None, stream=None):
+        """The same from a raw float2 grid (device pointer) and 7 camera floats."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty((self.height, self.width, 4), dtype=torch.uint8, device="cuda")
+        f = L.bt_frame()
+        f.grid, f.grid_rows, f.grid_cols, f.grid_level = grid_ptr, grid_rows, grid_cols, grid_level
+        f.view = view.data_ptr()
+        f.hor, f.ver = hor, ver
+        f.cam[:] = [float(x) for x in cam7]
+        f.env = env._h if env is not None else None
+        f.stars = stars._h if stars is not None else None
+        f.map, f.star, f.lr = int(env is not None), int(stars is not None), int(bool(lr))
+        f.step, f.diffraction = int(step), int(bool(diffraction))
+        f.out = out.data_ptr()
+        L.check(L.lib().bt_map_render(self._h, C.byref(f), _stream_ptr(stream)))
+        return out
+
+    def scratch(self):
+        """Device views of the frame's intermediates (thphi, gap, bh, area, light)."""
+        torch = _torch()
+        b = L.bt_map_buffers()
+        L.check(L.lib().bt_map_scratch(self._h, C.byref(b)))
+        W, H = self.width, self.height
+        return dict(
+            thphi=_device_view(b.thphi, ((H + 1) * (W + 1), 2), torch.float32),
+            gap=_device_view(b.gap, ((H + 1) * (W + 1),), torch.int32),
+            bh=_device_view(b.bh, (H * W,), torch.uint8),
+            area=_device_view(b.area, (H * W,), torch.float32),
+            light=_device_view(b.light, (H * W * 3,), torch.float32),
+            env_img=_device_view(b.env_img, (H * W * 4,), torch.uint8))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None:
+            try:
+                L.lib().bt_map_destroy(h)
+            except Exception:
+                pass
+            self._h = None

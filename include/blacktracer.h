@@ -163,6 +163,82 @@ int bt_grid_export_dense(const bt_grid* g, double* theta, double* phi,
 int bt_grid_map_export(bt_grid* g, const float** grid_out, int32_t* rows,
                        int32_t* cols, int32_t* sym, void* stream);
 
+/* ------------------------------------------------------- per-pixel map */
+
+/* Camera-sky corner directions of an equirectangular W x H output:
+ * Viewer::makeSphereView (BT/Viewer.h:82-88).  view: DEVICE float2 array of
+ * (H+1)*(W+1) (theta, phi) pairs. */
+int bt_view_sphere(float* view, int width, int height, void* stream);
+
+/* A resident environment map: its summed-area table (float4 per pixel,
+ * channels B^2.2*A, G^2.2*A, R^2.2*A, A), built on the device from a BGR8
+ * image of rows x cols (cv::imread order).  Replaces the host OpenMP table
+ * of cudaPrep (BT/MakeImageKernel.cu:1312-1330) and its per-call upload. */
+typedef struct bt_env bt_env;
+int bt_env_create(const uint8_t* bgr, int rows, int cols, int bgr_on_device,
+                  bt_env** out, void* stream);
+void bt_env_destroy(bt_env* e);
+int bt_env_sat(const bt_env* e, const float** sat, int32_t* rows, int32_t* cols);
+
+/* A resident star set in the reference's StarProcessor layout
+ * (BT/StarProcessor.h:25-31): star_pos = 2n (theta, phi), star_mag = 2n
+ * (magnitude, B-V), tree = 2^(treeLevel+1)-1 cumulative counts (binaryStarTree).
+ * psf_rgb (optional) is the diffraction sprite, psf_size^2 RGB8. */
+typedef struct bt_stars bt_stars;
+int bt_stars_tree_size(int treeLevel);
+/* StarProcessor's tree (makeTree, BT/StarProcessor.h:172-212) from a star
+ * list: HOST arrays; stars with mag > magnitude_cut are left out
+ * (BT/StarProcessor.h:37-46).  Outputs sized 2n, 2n, tree_size. */
+int bt_stars_build_tree(const float* theta, const float* phi, const float* mag,
+                        const float* bv, int n, int treeLevel,
+                        float magnitude_cut, float* star_pos, float* star_mag,
+                        int* tree, int* n_kept);
+int bt_stars_create(const float* star_pos, const float* star_mag, int n,
+                    const int* tree, int treeLevel, const uint8_t* psf_rgb,
+                    int psf_size, bt_stars** out, void* stream);
+void bt_stars_destroy(bt_stars* s);
+
+/* A renderer: per-resolution device scratch (the reference's dev_in,
+ * dev_gap, dev_bh, dev_area, star buffers), created once per output size. */
+typedef struct bt_map bt_map;
+int bt_map_create(int width, int height, bt_map** out);
+void bt_map_destroy(bt_map* m);
+
+/* One frame.  Replaces makeImage / cudaPrep (BT/MakeImageKernel.cu:1206-1559,
+ * called from Distorter::cudaCall, BT/Distorter.h:103-148) for one grid
+ * (G = 1): pixInterpolation, findBlackPixels, findArea, smoothAreaH/V,
+ * distortEnvironmentMap (map), distortStarMap + sumStarLight
+ * (+ addDiffraction) + makePix (star), addStarsAndBackground (both).
+ * All pointers are DEVICE pointers; nothing is copied to the host. */
+typedef struct bt_frame {
+  const float* grid;      /* bt_grid_map_export: grid_rows x grid_cols float2 */
+  int32_t grid_rows, grid_cols, grid_level;  /* GN1, GM, MAXLEVEL            */
+  const float* view;      /* (H+1)*(W+1) float2 camera-sky corners          */
+  float hor, ver;         /* look-around offsets (pixInterpolation)         */
+  float cam[7];           /* Camera::getParamArray                          */
+  const bt_env* env;      /* required when map != 0                         */
+  const bt_stars* stars;  /* required when star != 0                        */
+  int32_t map, star, lr;  /* the reference's map / star / dev_lr toggles    */
+  int32_t step;           /* splat half-width, 0..2 (the reference uses 1)  */
+  int32_t diffraction;    /* scatter the sprite around saturated stars      */
+  uint8_t* out;           /* H*W BGRA8                                      */
+} bt_frame;
+int bt_map_render(bt_map* m, const bt_frame* f, void* stream);
+
+/* Device pointers into a renderer's scratch after a frame (for tests and
+ * tools): corner (theta, phi), block gaps, black-hole mask, smoothed area,
+ * summed star light (3 floats), star image and environment image. */
+typedef struct bt_map_buffers {
+  const float* thphi;
+  const int32_t* gap;
+  const uint8_t* bh;
+  const float* area;
+  const float* light;
+  const uint8_t* stars_img;
+  const uint8_t* env_img;
+} bt_map_buffers;
+int bt_map_scratch(const bt_map* m, bt_map_buffers* b);
+
 /* Message for the last error on this thread ("" when none). */
 const char* bt_last_error(void);
 

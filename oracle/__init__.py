@@ -27,6 +27,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ORC = os.path.join(_HERE, "_build", "libbt_oracle.so")
 _REF = os.path.join(_HERE, "_ref", "libbtref.so")
+_REF_MAP = os.path.join(_HERE, "_ref", "libbtref_map.so")
 
 CAM_FIELDS = ("theta", "phi", "r", "speed", "br", "btheta", "bphi",
               "alpha", "w", "wbar", "Delta", "ro")
@@ -189,3 +190,122 @@ def ref_grid_time(maxlevel, startlevel, angle, cam, a):
     t = _reflib().btref_grid_time(maxlevel, startlevel, 1 if angle else 0, cam, a,
                                   C.byref(n))
     return t, n.value
+
+
+# ---------------------------------------------------------------- map (reference kernels)
+_refmap = None
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_i32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def have_ref_map() -> bool:
+    return os.path.exists(_REF_MAP)
+
+
+def _refmaplib():
+    global _refmap
+    if _refmap is None:
+        if not have_ref_map():
+            raise RuntimeError("reference map harness not built (make -C oracle ref)")
+        lib = C.CDLL(_REF_MAP)
+        lib.btref_map_pixinterp.argtypes = [_f32p, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                            C.c_int, C.c_int, C.c_float, C.c_float, _f32p,
+                                            _i32]
+        lib.btref_map_bh_area.argtypes = [_f32p, C.c_int, C.c_int, _u8p, _f32p]
+        lib.btref_map_smooth.argtypes = [_f32p, _f32p, _u8p, _i32, C.c_int, C.c_int]
+        lib.btref_map_sat.argtypes = [_u8p, C.c_int, C.c_int, _f32p]
+        lib.btref_map_env.argtypes = [_f32p, _u8p, _u8p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      _f32p, _f32p, _f32p, _f32p, C.c_int]
+        lib.btref_map_stars.argtypes = [_f32p, _u8p, _f32p, _i32, C.c_int, _f32p, _f32p,
+                                        C.c_int, C.c_int, C.c_int, C.c_int, _f32p, C.c_int,
+                                        _f32p, _f32p, _u8p, C.c_void_p]
+        lib.btref_map_compose.argtypes = [_u8p, _u8p, _u8p, C.c_int, C.c_int]
+        _refmap = lib
+    return _refmap
+
+
+def ref_star_tree(theta, phi, mag, bv, tree_level):
+    """StarProcessor::makeTree of the reference (BT/StarProcessor.h:172-212)."""
+    lib = _reflib()
+    lib.btref_star_tree.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int,
+                                    _f32p, _f32p, _i32]
+    f = lambda x: np.ascontiguousarray(x, dtype=np.float32)  # noqa: E731
+    n = len(theta)
+    pos = np.empty(2 * n, np.float32)
+    mg = np.empty(2 * n, np.float32)
+    tree = np.empty((1 << (tree_level + 1)) - 1, np.int32)
+    lib.btref_star_tree(f(theta), f(phi), f(mag), f(bv), n, tree_level, pos, mg, tree)
+    return pos, mg, tree
+
+
+def ref_map_frame(grid_f2, grid_rows, grid_cols, gridlvl, view, width, height, cam7,
+                  bgr=None, stars=None, lr=True, step=1, hor=0.0, ver=0.0, want_cells=False):
+    """One frame through the reference's own map kernels (host-compiled).
+
+    grid_f2: (grid_rows*grid_cols, 2) float32 map grid; view: ((H+1)*(W+1), 2)
+    float32; bgr: (rows, cols, 3) uint8 or None; stars: (pos, mag, tree,
+    tree_level) or None.  Rows of the grid are padded with absent vertices
+    above and below, which is what this build reads where the reference
+    indexes outside the grid.  Returns a dict of the intermediates and the
+    BGRA image."""
+    lib = _refmaplib()
+    M, N = width, height
+    pad = 2 * grid_rows + 8
+    g = np.full(((grid_rows + 2 * pad) * grid_cols, 2), -2.0, np.float32)
+    g[pad * grid_cols:(pad + grid_rows) * grid_cols] = grid_f2
+    gview = g[pad * grid_cols:]
+    view = np.ascontiguousarray(view, dtype=np.float32)
+    thphi = np.zeros(((N + 1) * (M + 1), 2), np.float32)
+    gap = np.zeros((N + 1) * (M + 1), np.int32)
+    # pass a pointer into the padded array: the harness indexes rows around it
+    lib.btref_map_pixinterp(view, M, N, C.c_void_p(gview.ctypes.data), grid_cols, grid_rows,
+                            gridlvl, hor, ver, thphi, gap)
+    bh = np.zeros(N * M, np.uint8)
+    area = np.zeros(N * M, np.float32)
+    lib.btref_map_bh_area(thphi, M, N, bh, area)
+    area_raw = area.copy()
+    tmp = np.zeros(N * M, np.float32)
+    lib.btref_map_smooth(area, tmp, bh, gap, M, N)
+    cam7 = np.ascontiguousarray(cam7, dtype=np.float32)
+    out = dict(thphi=thphi, gap=gap, bh=bh, area_raw=area_raw, area=area)
+    img = None
+    if bgr is not None:
+        bgr = np.ascontiguousarray(bgr, dtype=np.uint8)
+        rows, cols = bgr.shape[:2]
+        sat = np.zeros(rows * cols * 4, np.float32)
+        lib.btref_map_sat(bgr, rows, cols, sat)
+        # zero rows around the table: what this build reads where the
+        # reference indexes a row before or past it
+        padded = np.zeros((rows + 4) * cols * 4, np.float32)
+        padded[2 * cols * 4:(rows + 2) * cols * 4] = sat
+        img = np.zeros(N * M * 4, np.uint8)
+        lib.btref_map_env.argtypes = list(lib.btref_map_env.argtypes[:7]) + [C.c_void_p] + \
+            list(lib.btref_map_env.argtypes[8:])
+        lib.btref_map_env(thphi, img, bh, rows, cols, M, N,
+                          C.c_void_p(padded.ctypes.data + 2 * cols * 16), cam7, area, view,
+                          int(lr))
+        out["sat"] = sat
+        out["env"] = img.copy()
+    if stars is not None:
+        pos, mg, tree, tl = stars
+        light = np.zeros(N * M * 3, np.float32)
+        simg = np.zeros(N * M * 4, np.uint8)
+        fw = 2 * step + 1
+        cells = np.zeros(N * M * fw * fw * 3, np.float32) if want_cells else None
+        lib.btref_map_stars(thphi, bh, np.ascontiguousarray(pos, np.float32),
+                            np.ascontiguousarray(tree, np.int32), len(pos) // 2, cam7,
+                            np.ascontiguousarray(mg, np.float32), tl, M, N, step, view,
+                            int(lr), area, light, simg,
+                            None if cells is None else C.c_void_p(cells.ctypes.data))
+        if cells is not None:
+            out["cells"] = cells
+        out["light"] = light
+        out["stars"] = simg.copy()
+        if img is not None:
+            comp = np.zeros(N * M * 4, np.uint8)
+            lib.btref_map_compose(simg, img, comp, M, N)
+            img = comp
+        else:
+            img = simg
+    out["image"] = img
+    return out

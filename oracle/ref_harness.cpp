@@ -11,6 +11,7 @@
 // loads with ctypes, so the plain-C restatement (oracle/bt_oracle.c) and the
 // GPU library can be pinned to the reference's own outputs.
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <cstdio>
 #include <fstream>
@@ -39,7 +40,17 @@
 // one (raytrace, then fixTvertices in a chosen order).
 #define private public
 #include "Grid.h"
+#include "StarProcessor.h"
 #undef private
+
+// StarProcessor holds an (always empty) cv::Mat; its inline destructor
+// references two OpenCV library functions that an empty Mat never calls.  No
+// OpenCV library is linked, so the harness supplies stand-ins that stop the
+// process if they are ever reached.
+namespace cv {
+void fastFree(void*) { std::abort(); }
+void Mat::deallocate() { std::abort(); }
+}  // namespace cv
 
 namespace {
 
@@ -192,6 +203,28 @@ double btref_grid_time(int maxlevel, int startlevel, int angle,
   auto t1 = std::chrono::steady_clock::now();
   if (nentries) *nentries = (long)g.CamToCel.size();
   return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// StarProcessor::makeTree (BT/StarProcessor.h:172-212) on a star list
+// {theta, phi, mag, bv}, with the set-up of the constructor (:263-271).
+void btref_star_tree(const float* theta, const float* phi, const float* mag,
+                     const float* bv, int n, int treeLevel, float* star_pos,
+                     float* star_mag, int* tree) {
+  std::vector<std::vector<float>> stars(n);
+  for (int k = 0; k < n; k++) stars[k] = {theta[k], phi[k], mag[k], bv[k]};
+  StarProcessor sp;
+  sp.starSize = n;
+  sp.starMag.resize(n * 2);
+  sp.starPos.resize(n * 2);
+  sp.treeLevel = treeLevel;
+  sp.treeSize = (1 << (treeLevel + 1)) - 1;
+  sp.binaryStarTree.resize(sp.treeSize);
+  float thphi[2] = {0, 0};
+  float size[2] = {PI, PI2};
+  sp.makeTree(stars, 0, thphi, size, 0);
+  std::copy(sp.starPos.begin(), sp.starPos.end(), star_pos);
+  std::copy(sp.starMag.begin(), sp.starMag.end(), star_mag);
+  std::copy(sp.binaryStarTree.begin(), sp.binaryStarTree.end(), tree);
 }
 
 }  // extern "C"

@@ -1,0 +1,236 @@
+// ref_map_harness.cpp -- runs the REFERENCE's per-pixel map kernels on the
+// host.  TEST INFRASTRUCTURE ONLY.
+//
+// oracle/Makefile extracts the kernel bodies of the reference
+// (BT/MakeImageKernel.cu lines 27-853: the kernels only, no GL, no host
+// driver) into oracle/_ref/mik_body.inc at build time and compiles them here
+// for the host together with the reference's device helpers (BT/kernel.cuh),
+// with CUDA's qualifiers and builtins defined away.  Nothing of the reference
+// is copied into this repository.
+//
+// Each kernel is run once per valid pixel / corner (blockDim = 1, blockIdx =
+// (i, j)), which is the reference's per-thread computation without the
+// out-of-range threads its launch shapes create (distortEnvironmentMap,
+// distortStarMap, sumStarLight, makePix and addStarsAndBackground have no
+// bounds check and index past the image when N or M is not a multiple of
+// their block shape).  The summed-area table of cudaPrep
+// (BT/MakeImageKernel.cu:1312-1330) lives in the host driver outside that
+// range, so it is restated below (btref_map_sat), calling the reference's
+// calcArea.
+#define _GNU_SOURCE 1
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <strings.h>
+#include <vector>
+
+#include "opencv2/core/core.hpp"
+// threadIdx & co become per-thread host variables the driver sets.
+#define __STORAGE__ thread_local
+#include "cuda_runtime.h"
+#include "device_launch_parameters.h"
+
+#undef __device__
+#undef __global__
+#undef __host__
+#undef __constant__
+#undef __forceinline__
+#define __device__
+#define __global__
+#define __host__
+#define __constant__
+#define __forceinline__ inline
+
+using namespace std;
+typedef unsigned int uint;
+
+// ---- device intrinsics used by the kernels, for one host thread ----
+static inline int atomicAdd(int* p, int v) { int o = *p; *p += v; return o; }
+static inline float atomicAdd(float* p, float v) { float o = *p; *p += v; return o; }
+static inline int atomicMin(int* p, int v) { int o = *p; *p = std::min(o, v); return o; }
+static inline int atomicMax(int* p, int v) { int o = *p; *p = std::max(o, v); return o; }
+static inline unsigned atomicMin(unsigned* p, unsigned v) { unsigned o = *p; *p = std::min(o, v); return o; }
+static inline unsigned atomicMax(unsigned* p, unsigned v) { unsigned o = *p; *p = std::max(o, v); return o; }
+static inline int __ffs(unsigned x) { return ffs((int)x); }
+static inline float __int_as_float(int x) { float f; memcpy(&f, &x, 4); return f; }
+static inline int __float_as_int(float x) { int i; memcpy(&i, &x, 4); return i; }
+static inline float __uint_as_float(unsigned x) { float f; memcpy(&f, &x, 4); return f; }
+static inline unsigned __float_as_uint(float x) { unsigned i; memcpy(&i, &x, 4); return i; }
+
+#include "kernel.cuh"
+#define ij (i * M + j)
+#include "mik_body.inc"
+#undef ij
+
+namespace {
+inline void at(int i, int j) {
+  blockIdx.x = i; blockIdx.y = j; blockIdx.z = 0;
+  threadIdx.x = threadIdx.y = threadIdx.z = 0;
+  blockDim.x = blockDim.y = blockDim.z = 1;
+}
+}  // namespace
+
+extern "C" {
+
+// pixInterpolation (G = 1) for every corner (N+1) x (M+1).
+void btref_map_pixinterp(const float* view, int M, int N, const float* grid,
+                         int GM, int GN1, int gridlvl, float hor, float ver,
+                         float* thphi, int* gap) {
+  float2 border[4] = {};
+  for (int i = 0; i <= N; i++)
+    for (int j = 0; j <= M; j++) {
+      at(i, j);
+      pixInterpolation((const float2*)view, M, N, 1, (float2*)thphi,
+                       (const float2*)grid, GM, GN1, hor, ver, gap, gridlvl,
+                       border, 1000, 0.f);
+    }
+}
+
+// findBlackPixels + findArea for every pixel.
+void btref_map_bh_area(const float* thphi, int M, int N, unsigned char* bh,
+                       float* area) {
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      findBlackPixels((const float2*)thphi, M, N, bh);
+      findArea((const float2*)thphi, M, N, area);
+    }
+}
+
+// smoothAreaH then smoothAreaV; area is updated in place (areaSmooth is the
+// intermediate, as in cudaPrep).
+void btref_map_smooth(float* area, float* areaSmooth, const unsigned char* bh,
+                      const int* gap, int M, int N) {
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      smoothAreaH(areaSmooth, area, bh, gap, M, N);
+    }
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      smoothAreaV(areaSmooth, area, bh, gap, M, N);
+    }
+}
+
+// Summed-area table of cudaPrep (BT/MakeImageKernel.cu:1312-1330) over a BGR8
+// image (cv::imread's channel order), rows x cols; out: rows*cols float4.
+void btref_map_sat(const unsigned char* bgr, int rows, int cols, float* out) {
+  float pxsz = PI2 / (1.f * cols);
+  for (int q = 0; q < cols; q++) {
+    float prev[4] = {0.f, 0.f, 0.f, 0.f};
+    float phi[4] = {pxsz * q, pxsz * q, pxsz * (q + 1), pxsz * (q + 1)};
+    for (int p = 0; p < rows; p++) {
+      float theta[4] = {pxsz * (p + 1), pxsz * p, pxsz * p, pxsz * (p + 1)};
+      float area = calcArea(theta, phi);
+      const unsigned char* px = bgr + ((size_t)p * cols + q) * 3;
+      prev[0] += powf(px[0], 2.2f) * area;
+      prev[1] += powf(px[1], 2.2f) * area;
+      prev[2] += powf(px[2], 2.2f) * area;
+      prev[3] += area;
+      memcpy(out + ((size_t)p * cols + q) * 4, prev, sizeof(prev));
+    }
+  }
+}
+
+// distortEnvironmentMap for every pixel; out is BGRA8.
+void btref_map_env(const float* thphi, unsigned char* out, const unsigned char* bh,
+                   int rows, int cols, int M, int N, float* sat,
+                   const float* cam7, const float* area, float* view, int lr) {
+  int2 imsize = {rows, cols};
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      distortEnvironmentMap((const float2*)thphi, (uchar4*)out, bh, imsize, M, N,
+                            0.f, (float4*)sat, cam7, 0, nullptr, area,
+                            (float2*)view, lr != 0);
+    }
+}
+
+// distortStarMap + sumStarLight (+ makePix) on frame 0 (no trails), per
+// pixel.  starLight scratch: N*M*(2step+1)^2 float3; search: N*M*searchNr.
+// out: BGRA8 star image; light: N*M float3 summed star light; cells_out
+// (optional): the splat scratch after distortStarMap.
+void btref_map_stars(const float* thphi, const unsigned char* bh,
+                     const float* stars, const int* tree, int starSize,
+                     const float* cam7, const float* mag, int treeLevel, int M,
+                     int N, int step, const float* view, int lr,
+                     const float* area, float* light, unsigned char* out,
+                     float* cells_out) {
+  const int filterW = 2 * step + 1;
+  const int searchNr = (int)powf(2, treeLevel / 3 * 2);
+  std::vector<float3> scratch((size_t)N * M * filterW * filterW);
+  std::vector<int> search((size_t)N * M * searchNr + 64 * searchNr);
+  const int trailnum = 30;
+  std::vector<int2> stCache((size_t)2 * starSize * trailnum, int2{-1, -1});
+  std::vector<int> stnums(starSize, 0);
+  std::vector<float3> trail((size_t)N * M, float3{0.f, 0.f, 0.f});
+  std::vector<float2> grad((size_t)(N + 1) * (M + 1), float2{0.f, 0.f});
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      distortStarMap(scratch.data(), (const float2*)thphi, bh, stars, tree,
+                     starSize, cam7, mag, treeLevel, M, N, step, 0.f,
+                     search.data(), searchNr, stCache.data(), stnums.data(),
+                     trail.data(), trailnum, grad.data(), 0, (const float2*)view,
+                     lr != 0, area);
+    }
+  if (cells_out)
+    memcpy(cells_out, scratch.data(), scratch.size() * sizeof(float3));
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      sumStarLight(scratch.data(), trail.data(), (float3*)light, step, M, N, filterW);
+    }
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      makePix((float3*)light, (uchar4*)out, M, N, nullptr);
+    }
+}
+
+// addStarsAndBackground per pixel (stars, background -> output, BGRA8).
+void btref_map_compose(const unsigned char* stars, const unsigned char* bg,
+                       unsigned char* out, int M, int N) {
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      addStarsAndBackground((uchar4*)stars, (uchar4*)bg, (uchar4*)out, M);
+    }
+}
+
+// searchTree for one bounding box (picheck = 0, as distortStarMap calls it).
+int btref_search_tree(const int* tree, const float* mn, const float* mx,
+                      int treeLevel, int* nodes, int cap) {
+  std::vector<int> buf(1 << 20);
+  int pos = 0;
+  searchTree(tree, mn, mx, treeLevel, buf.data(), 0, pos, 0);
+  for (int k = 0; k < pos && k < cap; k++) nodes[k] = buf[k];
+  return pos;
+}
+
+// The reference's device helpers, one call each (for unit checks).
+int btref_star_in_polygon(const float* t, const float* p, float st, float sp, int sgn) {
+  return starInPolygon(t, p, st, sp, sgn) ? 1 : 0;
+}
+void btref_interpolate(const float* t, const float* p, float* st, float* sp, int sgn) {
+  interpolate(t[0], t[1], t[2], t[3], p[0], p[1], p[2], p[3], *st, *sp, sgn, 0, 0);
+}
+float btref_calc_area(const float* t4, const float* p4) {
+  float t[4], p[4];
+  memcpy(t, t4, sizeof(t));
+  memcpy(p, p4, sizeof(p));
+  return calcArea(t, p);
+}
+float btref_redshift(float theta, float phi, const float* cam7) {
+  return redshift(theta, phi, cam7);
+}
+void btref_rgb_hsp(float r, float g, float b, float* hsp) {
+  RGBtoHSP(r, g, b, hsp[0], hsp[1], hsp[2]);
+}
+void btref_hsp_rgb(float h, float s, float p, float* rgb) {
+  HSPtoRGB(h, s, p, rgb[0], rgb[1], rgb[2]);
+}
+
+}  // extern "C"
