@@ -1,0 +1,428 @@
+#!/usr/bin/env python
+"""Benchmark of the BlackTracer hot path on B200.
+
+Headline (value): geodesics/s of building the adaptive camera-sky grid of the
+"single large adaptive grid" configuration -- Kerr a/M = 0.999, camera on a
+circular equatorial orbit at r = 5M boosted at Keplerian velocity, adaptive
+refinement from level 6 (64x128) to level 11 (2048x4096 equivalent) --
+through the C ABI (bt_grid_build), plain FP64 form (the form that reproduces
+the reference integrator; the mixed form is reported beside it).  One step =
+one complete grid build (all levels + T-vertex fix).  Also reported: 4K
+frames (3840x1920 BGRA8 from an 8192x4096 environment map and 10^6 stars,
+lensing + redshift on) per second and p50/p99 frame latency.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Multi-GPU (torchrun, one rank per GPU): every rank builds its own grid
+(replicas; the path has no data exchange), value = all ranks' rays / the
+slowest rank's time.  `--impl reference` times the reference's own CPU
+integrator on the box's host cores on the same ray set.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("geodesics/s & 4K frames/s, mixed vs plain FP64 on 1 B200 @≤1e-6 rad; p99 ms")
+# Algorithmic FP64 work of the plain integrator, counted once from the
+# reference's equations (BT/Metric.h:198-270; +,-,*,/,sqrt,sin,cos = 1 flop):
+F_EOM = 130          # derivs
+F_COMBINE = 270      # the Cash-Karp stage combinations of one attempt
+F_CONTROL = 45       # scale, error norm, step-size update
+F_ATTEMPT = 6 * F_EOM + F_COMBINE + F_CONTROL
+F_SETUP = 1000       # ray set-up + capture test (Newton + golden section), approx.
+WORKLOAD = dict(maxlevel=11, startlevel=6, a=0.999, r=5.0, theta=np.pi / 2)
+
+
+def c2_camera(bt):
+    return bt.Camera(WORKLOAD["theta"], 0.0, WORKLOAD["r"], 0.0, 0.0, 1.0, a=WORKLOAD["a"])
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_index):
+        self.dev = dev_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def value_noise_env(torch, rows, cols, seed, cell=64, octaves=4):
+    """Seeded value noise in [0, 255], BGR8 (rows, cols, 3) on the device."""
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    img = torch.zeros((rows, cols, 3), device="cuda", dtype=torch.float32)
+    amp, tot = 1.0, 0.0
+    for o in range(octaves):
+        c = max(2, cell >> o)
+        lat = torch.rand((rows // c + 2, cols // c + 2, 3), device="cuda", generator=g)
+        y = torch.arange(rows, device="cuda", dtype=torch.float32) / c
+        x = torch.arange(cols, device="cuda", dtype=torch.float32) / c
+        y0, x0 = y.floor().long(), x.floor().long()
+        fy = (y - y0)[:, None, None]
+        fx = (x - x0)[None, :, None]
+        fy, fx = fy * fy * (3 - 2 * fy), fx * fx * (3 - 2 * fx)
+        a = lat[y0][:, x0]
+        b = lat[y0][:, x0 + 1]
+        cc = lat[y0 + 1][:, x0]
+        d = lat[y0 + 1][:, x0 + 1]
+        img += amp * ((a * (1 - fx) + b * fx) * (1 - fy) + (cc * (1 - fx) + d * fx) * fy)
+        tot += amp
+        amp *= 0.5
+    return (img / tot * 255.0).clamp(0, 255).to(torch.uint8).contiguous()
+
+
+def synthetic_stars(n, seed, tmin=3000.0, tmax=30000.0):
+    rng = np.random.default_rng(seed)
+    theta = np.arccos(1 - 2 * rng.uniform(0, 1, n))
+    phi = 2 * np.pi * rng.uniform(0, 1, n)
+    mag = rng.exponential(2.0, n)
+    T = rng.uniform(tmin, tmax, n)
+    c = T / 4600.0
+    A, B, Cc = c, 2.32 * c - 2.0, 1.054 * c - 2.32
+    bv = ((-B + np.sqrt(B * B - 4 * A * Cc)) / (2 * A)) / 0.92
+    return [x.astype(np.float32) for x in (theta, phi, mag, bv)]
+
+
+def traffic_from_profiles():
+    """Per-launch DRAM bytes of the trace kernel from the committed ncu
+    summary (profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", "k_trace_lattice_plain_c2.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def cpu_reference_arm(args):
+    """--impl reference: the reference's own CPU integrator
+    (Grid::integration_wrapper, compiled in place into oracle/_ref) on all
+    host cores, over the rays the workload's grid traces."""
+    import oracle
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libbtref.so was not built (the reference tree was "
+                          "absent when the library was built)"}))
+        return 0
+    cam = oracle.camera_orbit(WORKLOAD["a"], WORKLOAD["theta"], 0.0, WORKLOAD["r"], 0, 0, 1)
+    g = oracle.grid_build(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam,
+                          WORKLOAD["a"], tfix=0)
+    # the ray set of the grid: every traced vertex (pole copies are not traced)
+    ii, jj = np.nonzero(g["exists"])
+    keep = ~(((ii == 0) | (ii == g["N"] - 1)) & (jj != 0))
+    ii, jj = ii[keep], jj[keep]
+    th = ii / (g["N"] - 1) * np.pi
+    ph = jj / g["M"] * 2 * np.pi
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.integrate_rays(cam, WORKLOAD["a"], th[:2000], ph[:2000], ref=True, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.integrate_rays(cam, WORKLOAD["a"], th, ph, ref=True, nthreads=cores)
+    el = time.perf_counter() - t0
+    v = len(th) * args.steps / el
+    line = {
+        "metric": METRIC, "value": v, "unit": "geodesics/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "adaptive grid L6->L11, a=0.999, r=5M equatorial Keplerian "
+                               "camera: the grid's traced rays", "rays": int(len(th)),
+                   "parallelism": f"{cores} host threads"},
+        "cpu_baseline": {"value": v, "unit": "geodesics/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{len(th)} rays of the workload's grid per step "
+                                   "through Grid::integration_wrapper, split over host threads"},
+        "e2e": {"value": v, "unit": "geodesics/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--frames", type=int, default=20, help="4K frames to time (0 = skip)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return cpu_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import blacktracer_b200 as bt
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def allmax(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    stream = torch.cuda.current_stream()
+    cam = c2_camera(bt)
+    opts = bt.IntegOpts("plain")
+    grid = bt.Grid(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam, opts=opts)
+    grid.set_timing(True)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
+
+    # algorithmic FP64 work of one build (identical every build)
+    grid.build()
+    d = grid.dense()
+    steps = d["steps"][d["status"] <= 2].to(torch.int64)
+    st_all = d["steps"].to(torch.int64)
+    integrated = (d["exists"] == 1) & (d["status"] != 1)
+    traced = int(grid.info().traced)
+    flops_build = float(((st_all[integrated] + 1).sum().item()) * F_ATTEMPT + traced * F_SETUP)
+    del d, steps, st_all, integrated
+
+    for _ in range(args.warmup):
+        grid.build()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    total_ms, trace_ms, launches, all_launches = 0.0, 0.0, 0, 0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        grid.build()
+        e1.record(stream)
+        inf = grid.info()  # synchronises
+        total_ms += e0.elapsed_time(e1)
+        trace_ms += float(inf.trace_ms)
+        launches += int(inf.trace_launches)
+        all_launches += int(inf.launches)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    max_ms = allmax(total_ms)
+    value = traced * args.steps * world / (max_ms / 1e3)
+
+    # mixed form, same workload (reported beside the headline)
+    gm = bt.Grid(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam, opts="mixed")
+    for _ in range(3):
+        gm.build()
+    torch.cuda.synchronize()
+    t_mixed = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        gm.build()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_mixed += e0.elapsed_time(e1)
+    mixed_value = int(gm.info().traced) * args.steps / (t_mixed / 1e3)
+    dp = grid.dense()
+    dm = gm.dense()
+    both = (dp["exists"] == 1) & (dm["exists"] == 1) & (dp["theta"] >= 0) & (dm["theta"] >= 0)
+    dth = (dp["theta"][both] - dm["theta"][both]).abs()
+    dph = (dp["phi"][both] - dm["phi"][both] + np.pi).remainder(2 * np.pi) - np.pi
+    err = torch.maximum(dth, dph.abs())
+    mixed_p99 = float(torch.quantile(err.float().cpu(), 0.99).item()) if err.numel() else None
+    mixed_topo = bool(torch.equal(dp["exists"], dm["exists"]) and torch.equal(dp["blevel"], dm["blevel"]))
+    del dp, dm, gm
+
+    # end to end through the C ABI with host buffers: build + compact export
+    # (CamToCel / steps / blockLevels) into pinned host memory every step
+    ex = grid.export()
+    bufs = ex["_buffers"]
+    nv, nb = len(ex["vi"]), len(ex["bi"])
+    d2h = nv * (4 + 4 + 8 + 8 + 4) + nb * (4 + 4 + 1)
+    h2d = 12 * 8 + 8  # camera fields + spin, passed by value
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        grid.build()
+        grid.export(out=bufs)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_s = allmax(time.perf_counter() - t0)
+    e2e_value = traced * args.steps * world / e2e_s
+
+    # roofline of the dominant kernel (the ray-tracing launches)
+    import ctypes as C
+    pk = C.c_double()
+    bt._lib.check(bt.lib().bt_probe_fp64_tflops(C.byref(pk), C.c_void_p(stream.cuda_stream)))
+    peak = pk.value
+    per_launch_ms = trace_ms / max(1, launches)
+    achieved = flops_build / (trace_ms / args.steps / 1e3) / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None,
+                "traffic": traffic_from_profiles(),
+                "kernel": "k_trace_lattice<PlainPolicy>",
+                "peak_source": "measured in this run: independent-chain DFMA probe "
+                               "(bt_probe_fp64_tflops); MEASURED_PEAKS.json has no FP64 entry",
+                "flops_per_build": flops_build, "trace_ms_per_build": trace_ms / args.steps,
+                "launches_per_build": launches / args.steps,
+                "avg_launch_ms": per_launch_ms}
+
+    # 4K frames with resident grid, environment and stars
+    frames = None
+    if args.frames > 0:
+        W, H = 3840, 1920
+        bgr = value_noise_env(torch, 4096, 8192, seed=20261204)
+        env = bt.Environment(bgr)
+        del bgr
+        stars = synthetic_stars(1_000_000, seed=20261205)
+        sp = bt.StarProcessor(*stars, treeLevel=14)
+        viewer = bt.Viewer(np.pi / 2, 0.0, 0.0, W, H, True)
+        R = bt.Renderer(W, H)
+        out = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+        host = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True)
+        for _ in range(3):
+            R.render(grid, viewer, cam, env=env, stars=sp, lr=True, out=out)
+        torch.cuda.synchronize()
+        lat = []
+        for _ in range(args.frames):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            R.render(grid, viewer, cam, env=env, stars=sp, lr=True, out=out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            lat.append(e0.elapsed_time(e1))
+        lat_e2e = []
+        for _ in range(args.frames):
+            t0 = time.perf_counter()
+            R.render(grid, viewer, cam, env=env, stars=sp, lr=True, out=out)
+            host.copy_(out, non_blocking=True)
+            torch.cuda.synchronize()
+            lat_e2e.append((time.perf_counter() - t0) * 1e3)
+        lat = np.array(lat)
+        frames = {"fps": float(1e3 / lat.mean()), "p50_ms": float(np.percentile(lat, 50)),
+                  "p99_ms": float(np.percentile(lat, 99)),
+                  "e2e_fps": float(1e3 / np.mean(lat_e2e)),
+                  "e2e_p99_ms": float(np.percentile(lat_e2e, 99)),
+                  "d2h_bytes_per_frame": W * H * 4, "width": W, "height": H,
+                  "env": "8192x4096 BGR8 value noise", "stars": 1_000_000, "tree_level": 14,
+                  "lensing_redshift": True}
+
+    # CPU baseline: the reference's own Grid constructor, one thread, full workload
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        if oracle.have_ref():
+            camr = oracle.camera_orbit(WORKLOAD["a"], WORKLOAD["theta"], 0.0, WORKLOAD["r"], 0, 0, 1,
+                                       ref=True)
+            secs, n = oracle.ref_grid_time(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, camr,
+                                           WORKLOAD["a"])
+            cpu = {"value": traced / secs, "unit": "geodesics/s", "cores": 1, "kind": "reference",
+                   "sample": f"one full grid build (Grid::Grid, L6->L11, {traced} rays, "
+                             f"{secs:.2f} s incl. its perfect hash) on one host thread"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "geodesics/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "adaptive grid L6->L11 (64x128 -> 2048x4096 equivalent), "
+                                   "Kerr a=0.999, camera r=5M theta=pi/2 Keplerian orbit; "
+                                   "plain FP64 integrator",
+                       "rays_per_build": traced, "l2": "flushed (256 MB write) before every step",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "e2e": {"value": e2e_value, "unit": "geodesics/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "api": "bt_grid_build + bt_grid_export to pinned host (CamToCel, steps, "
+                           "blockLevels as key-ordered lists)"},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": all_launches,
+            "mixed": {"value": mixed_value, "unit": "geodesics/s", "speedup_vs_plain":
+                      mixed_value / (traced * args.steps / (total_ms / 1e3)),
+                      "p99_rad_vs_plain": mixed_p99, "topology_exact": mixed_topo},
+            "frames_4k": frames,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

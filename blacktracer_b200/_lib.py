@@ -40,7 +40,17 @@ class bt_grid_info(C.Structure):
                 ("traced", C.c_int64), ("n_leaf_blocks", C.c_int64),
                 ("flags", C.c_uint32),
                 ("thphi", C.c_void_p), ("steps", C.c_void_p), ("exists", C.c_void_p),
-                ("blevel", C.c_void_p), ("status", C.c_void_p)]
+                ("blevel", C.c_void_p), ("status", C.c_void_p),
+                ("trace_ms", C.c_float), ("trace_launches", C.c_int32),
+                ("launches", C.c_int32)]
+
+
+class bt_grid_export_t(C.Structure):
+    _fields_ = [("vi", C.c_void_p), ("vj", C.c_void_p), ("theta", C.c_void_p),
+                ("phi", C.c_void_p), ("steps", C.c_void_p), ("cap_vertices", C.c_size_t),
+                ("bi", C.c_void_p), ("bj", C.c_void_p), ("level", C.c_void_p),
+                ("cap_blocks", C.c_size_t), ("n_vertices", C.c_size_t),
+                ("n_blocks", C.c_size_t)]
 
 
 class bt_frame(C.Structure):
@@ -79,6 +89,9 @@ _SIGS = {
     "bt_grid_export_dense": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "bt_grid_map_export": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int32),
                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), _vp]),
+    "bt_grid_export": (C.c_int, [_vp, C.POINTER(bt_grid_export_t), _vp]),
+    "bt_grid_set_timing": (C.c_int, [_vp, C.c_int]),
+    "bt_probe_fp64_tflops": (C.c_int, [C.POINTER(C.c_double), _vp]),
     "bt_view_sphere": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "bt_env_create": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp), _vp]),
     "bt_env_destroy": (None, [_vp]),

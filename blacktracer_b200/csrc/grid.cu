@@ -56,6 +56,16 @@ struct bt_grid {
   double a;
   int built;
   float2* mapgrid;  // float2 export for the map (lazy)
+  uint32_t* rowv;   // compact export: per-row vertex / block counts + totals
+  uint32_t* rowb;
+  uint64_t* totals;
+  uint64_t* totals_host;
+  char* compact;    // compact export staging (device), lazily sized
+  size_t compact_bytes;
+  int launches;     // kernels launched by the last build
+  int timing;       // record CUDA events around the trace launches
+  cudaEvent_t ev[2 * 16];
+  int n_ev;
   int32_t map_rows;
   int sym;
 };
@@ -535,6 +545,119 @@ __global__ void k_export_dense(LatticeView L, double* th, double* ph,
   }
 }
 
+// Compact export in key order (i, then j): per-row counts, a row scan,
+// then an ordered per-row compaction (one block per row).
+__global__ void k_row_count(const uint8_t* __restrict__ vflag, const int8_t* __restrict__ bl,
+                            int M, uint32_t* __restrict__ vcount,
+                            uint32_t* __restrict__ bcount) {
+  const int i = blockIdx.x;
+  uint32_t v = 0, b = 0;
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    v += vflag[(size_t)i * M + j] == 1;
+    b += bl[(size_t)i * M + j] >= 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  __shared__ uint32_t sv[32], sb[32];
+  if ((threadIdx.x & 31) == 0) {
+    sv[threadIdx.x >> 5] = v;
+    sb[threadIdx.x >> 5] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t tv = 0, tb = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      tv += sv[w];
+      tb += sb[w];
+    }
+    vcount[i] = tv;
+    bcount[i] = tb;
+  }
+}
+
+// Exclusive scan of N row counts in one block (N <= 16385 rows).
+__global__ void k_row_scan(uint32_t* vcount, uint32_t* bcount, int N, uint64_t* totals) {
+  if (threadIdx.x != 0) return;
+  uint64_t sv = 0, sb = 0;
+  for (int i = 0; i < N; i++) {
+    const uint32_t v = vcount[i], b = bcount[i];
+    vcount[i] = (uint32_t)sv;
+    bcount[i] = (uint32_t)sb;
+    sv += v;
+    sb += b;
+  }
+  totals[0] = sv;
+  totals[1] = sb;
+}
+
+struct CompactOut {
+  uint32_t* vi;
+  uint32_t* vj;
+  double* th;
+  double* ph;
+  int32_t* st;
+  uint32_t* bi;
+  uint32_t* bj;
+  int8_t* blv;
+};
+
+__global__ void k_row_compact(LatticeView L, const uint32_t* __restrict__ voff,
+                              const uint32_t* __restrict__ boff, CompactOut o) {
+  const int i = blockIdx.x;
+  const int M = L.M;
+  __shared__ uint32_t base_v, base_b;
+  __shared__ uint32_t wv[32], wb[32];
+  if (threadIdx.x == 0) {
+    base_v = voff[i];
+    base_b = boff[i];
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j0 = 0; j0 < M; j0 += blockDim.x) {
+    const int j = j0 + threadIdx.x;
+    const size_t id = (size_t)i * M + j;
+    const bool hv = j < M && L.vflag[id] == 1;
+    const bool hb = j < M && L.blevel[id] >= 0;
+    const unsigned mv = __ballot_sync(0xffffffffu, hv), mb = __ballot_sync(0xffffffffu, hb);
+    if (lane == 0) {
+      wv[w] = __popc(mv);
+      wb[w] = __popc(mb);
+    }
+    __syncthreads();
+    uint32_t pv = base_v, pb = base_b;
+    for (int ww = 0; ww < w; ww++) {
+      pv += wv[ww];
+      pb += wb[ww];
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    if (hv) {
+      const uint32_t k = pv + __popc(mv & lt);
+      const double2 v = L.thphi[id];
+      if (o.vi) o.vi[k] = i;
+      if (o.vj) o.vj[k] = j;
+      if (o.th) o.th[k] = v.x;
+      if (o.ph) o.ph[k] = v.y;
+      if (o.st) o.st[k] = L.steps[id];
+    }
+    if (hb) {
+      const uint32_t k = pb + __popc(mb & lt);
+      if (o.bi) o.bi[k] = i;
+      if (o.bj) o.bj[k] = j;
+      if (o.blv) o.blv[k] = L.blevel[id];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int ww = 0; ww < nw; ww++) {
+        base_v += wv[ww];
+        base_b += wb[ww];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 static unsigned grid_blocks(size_t work, int threads) {
   size_t b = (work + threads - 1) / threads;
   const size_t cap = (size_t)sm_count() * 8;
@@ -550,10 +673,12 @@ using namespace bt;
 static void grid_free_buffers(bt_grid* g) {
   void* ptrs[] = {g->L.thphi, g->L.steps, g->L.vflag, g->L.vstat, g->L.blevel,
                   g->B.list[0], g->B.list[1], g->B.trace, g->B.leaves,
-                  g->B.X[0], g->B.X[1], g->ctr, g->mapgrid};
+                  g->B.X[0], g->B.X[1], g->ctr, g->mapgrid,
+                  g->rowv, g->rowb, g->totals, g->compact};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (g->ctr_host) cudaFreeHost(g->ctr_host);
+  if (g->totals_host) cudaFreeHost(g->totals_host);
 }
 
 extern "C" {
@@ -599,8 +724,12 @@ int bt_grid_create(int maxlevel, int angle, bt_grid** out) {
   GALLOC(g->B.X[0], NM * sizeof(double2));
   GALLOC(g->B.X[1], NM * sizeof(double2));
   GALLOC(g->ctr, sizeof(GridCounters));
+  GALLOC(g->rowv, (size_t)N * sizeof(uint32_t));
+  GALLOC(g->rowb, (size_t)N * sizeof(uint32_t));
+  GALLOC(g->totals, 2 * sizeof(uint64_t));
 #undef GALLOC
   if (e == cudaSuccess) e = cudaMallocHost((void**)&g->ctr_host, sizeof(GridCounters));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&g->totals_host, 2 * sizeof(uint64_t));
   if (e != cudaSuccess) {
     set_error("grid allocation (N=%d M=%d) failed: %s", N, M, cudaGetErrorString(e));
     grid_free_buffers(g);
@@ -613,6 +742,8 @@ int bt_grid_create(int maxlevel, int angle, bt_grid** out) {
 
 void bt_grid_destroy(bt_grid* g) {
   if (!g) return;
+  if (g->timing)
+    for (int k = 0; k < 2 * 16; k++) cudaEventDestroy(g->ev[k]);
   grid_free_buffers(g);
   delete g;
 }
@@ -643,10 +774,18 @@ int bt_grid_build(bt_grid* g, const bt_camera* cam, double a, int startlevel,
   BT_CUDA_TRY(cudaMemsetAsync(L.steps, 0, NM * sizeof(int32_t), s));
   BT_CUDA_TRY(cudaMemsetAsync(L.blevel, 0xff, NM, s));
   BT_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(GridCounters), s));
+  g->n_ev = 0;
   auto trace = [&]() -> int {
-    return p.precision == BT_PRECISION_MIXED
-               ? launch_trace_mixed(p, L, g->B.trace, g->ctr, s)
-               : launch_trace_plain(p, L, g->B.trace, g->ctr, s);
+    const bool t = g->timing && g->n_ev + 2 <= 2 * 16;
+    if (t) BT_CUDA_TRY(cudaEventRecord(g->ev[g->n_ev], s));
+    const int rc = p.precision == BT_PRECISION_MIXED
+                       ? launch_trace_mixed(p, L, g->B.trace, g->ctr, s)
+                       : launch_trace_plain(p, L, g->B.trace, g->ctr, s);
+    if (t) {
+      BT_CUDA_TRY(cudaEventRecord(g->ev[g->n_ev + 1], s));
+      g->n_ev += 2;
+    }
+    return rc;
   };
   const SeedShape S = seed_shape(L);
   k_seed<<<grid_blocks((size_t)(S.rows + 1) * S.cols, 256), 256, 0, s>>>(
@@ -693,6 +832,11 @@ int bt_grid_build(bt_grid* g, const bt_camera* cam, double a, int startlevel,
   }
   BT_CUDA_TRY(cudaMemcpyAsync(g->ctr_host, g->ctr, sizeof(GridCounters),
                               cudaMemcpyDeviceToHost, s));
+  // seed, pole copy, finalize; per level: refine + trace + advance (the
+  // start level adds one trace and one advance); per fixed level: passes,
+  // commit, check
+  const int nlev = L.maxlevel - startlevel;
+  g->launches = 3 + 3 * nlev + 2 + nlev * (kMaxTfixPasses + 2);
   g->built = 1;
   return BT_OK;
 }
@@ -717,6 +861,14 @@ int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream) {
   info->exists = g->L.vflag;
   info->blevel = g->L.blevel;
   info->status = g->L.vstat;
+  info->launches = g->launches;
+  info->trace_ms = 0.f;
+  info->trace_launches = g->n_ev / 2;
+  for (int k = 0; k + 1 < g->n_ev; k += 2) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, g->ev[k], g->ev[k + 1]) == cudaSuccess)
+      info->trace_ms += ms;
+  }
   if (info->flags) {
     set_error("grid build flags 0x%x (1: T-vertex fix did not converge, "
               "2: fix stack overflow, 4: work list overflow)", info->flags);
@@ -735,6 +887,70 @@ int bt_grid_export_dense(const bt_grid* g, double* theta, double* phi,
   k_export_dense<<<grid_blocks(NM, 256), 256, 0, (cudaStream_t)stream>>>(
       g->L, theta, phi, exists, steps, blevel, status);
   BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
+int bt_grid_set_timing(bt_grid* g, int on) {
+  BT_ARG_CHECK(g != nullptr, "NULL grid");
+  if (on && !g->timing)
+    for (int k = 0; k < 2 * 16; k++) BT_CUDA_TRY(cudaEventCreate(&g->ev[k]));
+  g->timing = on ? 1 : g->timing;
+  if (!on) g->timing = 0;
+  return BT_OK;
+}
+
+int bt_grid_export(bt_grid* g, bt_grid_export_t* out, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(g && out, "NULL pointer");
+  BT_ARG_CHECK(g->built, "grid not built");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int N = g->L.N;
+  k_row_count<<<N, 256, 0, s>>>(g->L.vflag, g->L.blevel, g->L.M, g->rowv, g->rowb);
+  k_row_scan<<<1, 32, 0, s>>>(g->rowv, g->rowb, N, g->totals);
+  BT_CUDA_TRY(cudaGetLastError());
+  BT_CUDA_TRY(cudaMemcpyAsync(g->totals_host, g->totals, 2 * sizeof(uint64_t),
+                              cudaMemcpyDeviceToHost, s));
+  BT_CUDA_TRY(cudaStreamSynchronize(s));
+  const size_t nv = g->totals_host[0], nb = g->totals_host[1];
+  out->n_vertices = nv;
+  out->n_blocks = nb;
+  if (nv > out->cap_vertices || nb > out->cap_blocks) {
+    set_error("export capacity too small: need %zu vertices, %zu blocks", nv, nb);
+    return BT_ERR_ARG;
+  }
+  // stage on the device in key order, then one copy per array to the
+  // caller's buffers (host or device)
+  const size_t need = nv * (4 + 4 + 8 + 8 + 4) + nb * (4 + 4 + 1) + 64;
+  if (g->compact_bytes < need) {
+    if (g->compact) cudaFree(g->compact);
+    g->compact = nullptr;
+    g->compact_bytes = 0;
+    cudaError_t e = cudaMalloc((void**)&g->compact, need);
+    if (e != cudaSuccess) {
+      set_error("export staging allocation failed: %s", cudaGetErrorString(e));
+      return BT_ERR_NOMEM;
+    }
+    g->compact_bytes = need;
+  }
+  CompactOut o;
+  char* p = g->compact;
+  o.th = (double*)p; p += nv * 8;
+  o.ph = (double*)p; p += nv * 8;
+  o.vi = (uint32_t*)p; p += nv * 4;
+  o.vj = (uint32_t*)p; p += nv * 4;
+  o.st = (int32_t*)p; p += nv * 4;
+  o.bi = (uint32_t*)p; p += nb * 4;
+  o.bj = (uint32_t*)p; p += nb * 4;
+  o.blv = (int8_t*)p;
+  k_row_compact<<<N, 256, 0, s>>>(g->L, g->rowv, g->rowb, o);
+  BT_CUDA_TRY(cudaGetLastError());
+  struct { void* dst; const void* src; size_t bytes; } cp[] = {
+      {out->theta, o.th, nv * 8}, {out->phi, o.ph, nv * 8}, {out->vi, o.vi, nv * 4},
+      {out->vj, o.vj, nv * 4},    {out->steps, o.st, nv * 4}, {out->bi, o.bi, nb * 4},
+      {out->bj, o.bj, nb * 4},    {out->level, o.blv, nb}};
+  for (auto& c : cp)
+    if (c.dst && c.bytes)
+      BT_CUDA_TRY(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDefault, s));
   return BT_OK;
 }
 

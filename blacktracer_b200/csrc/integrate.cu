@@ -175,6 +175,18 @@ int launch_integrate(const RayParams& p, const double* th, const double* ph,
   return BT_OK;
 }
 
+// Independent DFMA chains: 8 accumulators per thread, no memory traffic.
+__global__ void k_fp64_probe(double* out, int iters, double a, double b) {
+  double x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4,
+         x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  for (int k = 0; k < iters; k++) {
+    x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+    x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+  }
+  const double r = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (r == 12345.678) out[0] = r;  // keeps the chains live
+}
+
 }  // namespace bt
 
 using namespace bt;
@@ -182,6 +194,35 @@ using namespace bt;
 extern "C" {
 
 const char* bt_last_error(void) { return bt::g_err; }
+
+int bt_probe_fp64_tflops(double* tflops, void* stream) {
+  BT_ARG_CHECK(tflops != nullptr, "NULL pointer");
+  cudaStream_t s = (cudaStream_t)stream;
+  double* sink = nullptr;
+  BT_CUDA_TRY(cudaMalloc((void**)&sink, sizeof(double)));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int blocks = sm_count() * 8, threads = 256, iters = 4096;
+  k_fp64_probe<<<blocks, threads, 0, s>>>(sink, iters, 0.999999, 1e-7);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 5; r++) {
+    cudaEventRecord(e0, s);
+    k_fp64_probe<<<blocks, threads, 0, s>>>(sink, iters, 0.999999, 1e-7);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  BT_CUDA_TRY(cudaGetLastError());
+  const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  return BT_OK;
+}
 
 const char* bt_version(void) {
   return "blacktracer_b200 abi " "1" " sm_100a";

@@ -198,6 +198,7 @@ class Grid:
         L.check(L.lib().bt_grid_build(self._h, C.byref(self.cam._c), self.a, self.STARTLVL,
                                       self.opts.ref, _stream_ptr(self._stream)))
         self._info = None
+        self._map = None
 
     def info(self) -> L.bt_grid_info:
         if self._info is None:
@@ -229,13 +230,48 @@ class Grid:
         self.info()
         return out
 
+    def set_timing(self, on=True):
+        """Record CUDA events around the ray-tracing launches (info().trace_ms)."""
+        L.check(L.lib().bt_grid_set_timing(self._h, 1 if on else 0))
+
+    def export(self, out=None, pinned=True):
+        """The grid as key-ordered lists (CamToCel, steps, blockLevels).
+
+        Returns dict of numpy arrays vi, vj, theta, phi, steps, bi, bj, level
+        (host copies).  `out` may pass preallocated arrays (reused)."""
+        torch = _torch()
+        if out is None:
+            inf = self.info()
+            nv = nb = int(inf.traced) + 2 * self.M + 16
+            mk = (lambda n, dt: torch.empty(n, dtype=dt, pin_memory=pinned))
+            out = dict(vi=mk(nv, torch.int32), vj=mk(nv, torch.int32),
+                       theta=mk(nv, torch.float64), phi=mk(nv, torch.float64),
+                       steps=mk(nv, torch.int32), bi=mk(nb, torch.int32),
+                       bj=mk(nb, torch.int32), level=mk(nb, torch.int8))
+        e = L.bt_grid_export_t()
+        for k in ("vi", "vj", "theta", "phi", "steps", "bi", "bj", "level"):
+            setattr(e, k, out[k].data_ptr())
+        e.cap_vertices = out["vi"].numel()
+        e.cap_blocks = out["bi"].numel()
+        L.check(L.lib().bt_grid_export(self._h, C.byref(e), _stream_ptr(self._stream)))
+        torch.cuda.current_stream().synchronize() if self._stream is None else self._stream.synchronize()
+        nv, nb = int(e.n_vertices), int(e.n_blocks)
+        res = {k: out[k][:nv] for k in ("vi", "vj", "theta", "phi", "steps")}
+        res.update({k: out[k][:nb] for k in ("bi", "bj", "level")})
+        res["_buffers"] = out
+        return res
+
     def map_grid(self):
-        """(pointer, rows, cols, sym) of the float2 map grid (makeGrid)."""
+        """(pointer, rows, cols, sym) of the float2 map grid (makeGrid);
+        exported once per build."""
+        if getattr(self, "_map", None) is not None:
+            return self._map
         p = C.c_void_p()
         rows, cols, sym = C.c_int32(), C.c_int32(), C.c_int32()
         L.check(L.lib().bt_grid_map_export(self._h, C.byref(p), C.byref(rows), C.byref(cols),
                                            C.byref(sym), _stream_ptr(self._stream)))
-        return p.value, rows.value, cols.value, sym.value
+        self._map = (p.value, rows.value, cols.value, sym.value)
+        return self._map
 
     # --- reference-shaped host views (slow; for compatibility and tests) ---
     @property

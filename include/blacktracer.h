@@ -142,7 +142,15 @@ typedef struct bt_grid_info {
   const uint8_t* exists;  /* N*M, 1 where CamToCel holds the key     */
   const int8_t* blevel;   /* N*M, blockLevels at the block origin    */
   const uint8_t* status;  /* N*M, BT_RAY_* of traced vertices        */
+  float trace_ms;         /* with bt_grid_set_timing: device time of
+                             the ray-tracing launches of the build   */
+  int32_t trace_launches;
+  int32_t launches;       /* kernels the last build launched          */
 } bt_grid_info;
+
+/* Records CUDA events around the ray-tracing launches of later builds
+ * (reported by bt_grid_query as trace_ms). */
+int bt_grid_set_timing(bt_grid* g, int on);
 
 /* Synchronises `stream` and reports the build.  Returns BT_ERR_NUMERIC when
  * a bounded loop (T-vertex fixed point) gave up. */
@@ -154,6 +162,29 @@ int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream);
 int bt_grid_export_dense(const bt_grid* g, double* theta, double* phi,
                          uint8_t* exists, int32_t* steps, int8_t* blevel,
                          uint8_t* status, void* stream);
+
+/* Compact export of the grid in key order (i, then j) -- the reference's
+ * CamToCel (BT/Grid.h:575), steps (:577) and blockLevels (:588) as sorted
+ * lists.  Destination pointers may be HOST (pageable or pinned) or DEVICE
+ * memory, or NULL to skip an array; cap_* give their capacities.  The
+ * function synchronises `stream` once (to learn the counts) and enqueues the
+ * copies; the caller synchronises before reading host buffers.  Returns
+ * BT_ERR_ARG (with n_* set) when a capacity is too small. */
+typedef struct bt_grid_export_t {
+  uint32_t* vi;          /* vertex row i                      */
+  uint32_t* vj;          /* vertex column j                   */
+  double* theta;         /* celestial theta                   */
+  double* phi;           /* celestial phi                     */
+  int32_t* steps;        /* integration steps                 */
+  size_t cap_vertices;
+  uint32_t* bi;          /* leaf-block origin row             */
+  uint32_t* bj;          /* leaf-block origin column          */
+  int8_t* level;         /* block level                       */
+  size_t cap_blocks;
+  size_t n_vertices;     /* out                               */
+  size_t n_blocks;       /* out                               */
+} bt_grid_export_t;
+int bt_grid_export(bt_grid* g, bt_grid_export_t* out, void* stream);
 
 /* The float2 grid the per-pixel map reads: replaces saveAsGpuHash
  * (BT/Grid.h:642-654) + the PSH tables + makeGrid
@@ -238,6 +269,11 @@ typedef struct bt_map_buffers {
   const uint8_t* env_img;
 } bt_map_buffers;
 int bt_map_scratch(const bt_map* m, bt_map_buffers* b);
+
+/* FP64 FMA throughput of the current device, TFLOP/s (2 flops per FMA),
+ * from an independent-chain DFMA kernel timed with CUDA events: the peak
+ * the FP64 integrator's roofline is reported against. */
+int bt_probe_fp64_tflops(double* tflops, void* stream);
 
 /* Message for the last error on this thread ("" when none). */
 const char* bt_last_error(void);

@@ -76,3 +76,20 @@ def test_grid_mixed_topology(bt, cuda, oracle_mod):
         err = ang_err(d["theta"][e], d["phi"][e], ref["theta"][e], ref["phi"][e])
         print(f"mixed grid: p99 {np.percentile(err, 99):.2e} max {err.max():.2e}")
     assert topo, "mixed-precision grid topology must match the FP64 reference"
+
+
+def test_compact_export_matches_dense(bt, cuda, oracle_mod):
+    cam, a = oracle_camera(oracle_mod, "c2")
+    grid, d = build(bt, cam, a, 8, 5, True)
+    ex = grid.export()
+    ii, jj = np.nonzero(d["exists"])  # row-major = key order
+    assert np.array_equal(ex["vi"].numpy(), ii) and np.array_equal(ex["vj"].numpy(), jj)
+    assert np.array_equal(ex["theta"].numpy(), d["theta"][ii, jj])
+    assert np.array_equal(ex["phi"].numpy(), d["phi"][ii, jj])
+    assert np.array_equal(ex["steps"].numpy(), d["steps"][ii, jj])
+    bi, bj = np.nonzero(d["blevel"] >= 0)
+    assert np.array_equal(ex["bi"].numpy(), bi) and np.array_equal(ex["bj"].numpy(), bj)
+    assert np.array_equal(ex["level"].numpy(), d["blevel"][bi, bj])
+    # the reference's CamToCel holds exactly these keys
+    ref = oracle_mod.grid_build(8, 5, True, cam, a, tfix=1)
+    assert len(ii) == int(ref["exists"].sum())
