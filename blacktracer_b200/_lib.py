@@ -80,6 +80,10 @@ _SIGS = {
     "bt_integrate_rays_host": (C.c_int, [C.POINTER(bt_camera), C.c_double, _vp, _vp,
                                          C.c_size_t, _vp, _vp, _vp, _vp,
                                          C.POINTER(bt_integ_opts), _vp]),
+    "bt_integrate_rays_host_static": (C.c_int, [C.POINTER(bt_camera), C.c_double, _vp, _vp,
+                                                C.c_size_t, _vp, _vp, _vp, _vp,
+                                                C.POINTER(bt_integ_opts), _vp]),
+    "bt_integrate_rays_host_static_capacity": (C.c_size_t, []),
     "bt_grid_dims": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "bt_grid_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(_vp)]),
     "bt_grid_destroy": (None, [_vp]),

@@ -32,6 +32,7 @@ UNITS = {
     "map.cu": ["--fmad=false"],
     "stars.cu": ["--fmad=false"],
     "map_api.cu": [],
+    "noalloc.cu": [],
 }
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
            if f.endswith((".h", ".cuh"))] + [os.path.join(ROOT, "include", "blacktracer.h")]

@@ -105,6 +105,26 @@ int bt_integrate_rays_host(const bt_camera* cam, double a, const double* theta,
                            double* phi_out, int32_t* steps, uint8_t* status,
                            const bt_integ_opts* o, void* stream);
 
+/* bt_integrate_rays_host without any allocation.  No counterpart in the
+ * reference.  For callers that cannot let the library allocate device
+ * memory: a render or serving thread that must not stall on the implicit
+ * device synchronisation of cudaMalloc/cudaFree, a plugin host with a fixed
+ * device-memory budget, middleware whose device memory belongs to another
+ * runtime.  The rays are staged in a fixed static device array of
+ * bt_integrate_rays_host_static_capacity() rays (65536), held by every GPU
+ * that loads this library until the process exits; larger n is rejected
+ * with BT_ERR_ARG.  The first call on a device looks up that array's
+ * address (once per device, with the device current); make that first call
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other threads or streams of the same device) race on
+ * it and must be serialised by the caller.  Synchronises `stream`. */
+int bt_integrate_rays_host_static(const bt_camera* cam, double a,
+                                  const double* theta, const double* phi,
+                                  size_t n, double* theta_out, double* phi_out,
+                                  int32_t* steps, uint8_t* status,
+                                  const bt_integ_opts* o, void* stream);
+size_t bt_integrate_rays_host_static_capacity(void);
+
 /* ------------------------------------------------------------------ grid */
 
 /* Lattice size of a grid with max level L: N = 2^L/(2-eq)+1 rows,
