@@ -1,0 +1,70 @@
+// Drives the C++ host mirror (include/blacktracer.hpp) the way the
+// reference's main() drives its classes (BT/BlackTracer.cpp:192-343), and
+// prints results for tests/test_cpp_host.py to check against the oracle.
+//   host_api_demo camera           (no GPU needed)
+//   host_api_demo grid             (GPU)
+//   host_api_demo frame            (GPU)
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "blacktracer.hpp"
+
+using namespace blacktracer;
+
+int main(int argc, char** argv) {
+  const char* mode = argc > 1 ? argv[1] : "camera";
+  BlackHole black(0.999);
+  Camera cam(M_PI / 2, 0.0, 5.0, 0.0, 0.0, 1.0);
+  if (!std::strcmp(mode, "camera")) {
+    printf("%.17g %.17g %.17g %.17g %.17g %.17g\n", cam.speed, cam.alpha, cam.w, cam.wbar,
+           cam.Delta, cam.ro);
+    BlackHole b2(0.6);
+    Camera c2(M_PI / 2, 0.0, 30.0, 0.0);
+    printf("%.17g %.17g %.17g %.17g %.17g %.17g\n", c2.speed, c2.alpha, c2.w, c2.wbar,
+           c2.Delta, c2.ro);
+    try {
+      Camera bad(M_PI / 2, 0.0, -1.0, 0.0);
+      printf("no error\n");
+    } catch (const Error& e) {
+      printf("error %d\n", e.code);
+    }
+    return 0;
+  }
+  if (!std::strcmp(mode, "grid")) {
+    Grid g(8, 5, true, &cam, &black);
+    auto& cc = g.CamToCel();
+    auto& bl = g.blockLevels();
+    long maxlvl = 0;
+    for (auto& e : bl) maxlvl = e.second > maxlvl ? e.second : maxlvl;
+    double sum = 0;
+    for (auto& e : cc) sum += e.second.x + e.second.y;
+    printf("%d %d %zu %zu %ld %.10f %lld\n", g.N, g.M, cc.size(), bl.size(), maxlvl, sum,
+           (long long)g.traced());
+    return 0;
+  }
+  if (!std::strcmp(mode, "frame")) {
+    std::vector<Grid> grids;
+    grids.emplace_back(8, 5, true, &cam, &black);
+    std::vector<Camera> cams{cam};
+    Viewer view(M_PI / 2, 0, 0, 256, 128, true);
+    std::vector<Star> stars;
+    for (int k = 0; k < 2000; k++) {
+      const float u = (k * 0.618034f) - std::floor(k * 0.618034f);
+      const float v = (k * 0.381966f * 1.7f) - std::floor(k * 0.381966f * 1.7f);
+      stars.push_back(Star{std::acos(1 - 2 * u), 2.f * (float)M_PI * v, 1.5f, 0.3f});
+    }
+    StarProcessor sp(stars, 6, 1000.f);
+    std::vector<uint8_t> env(128 * 256 * 3);
+    for (size_t q = 0; q < env.size(); q++) env[q] = (uint8_t)((q * 37) % 251);
+    Distorter d(&grids, &view, &sp, &cams, env.data(), 128, 256);
+    std::vector<uint8_t> img(256 * 128 * 4);
+    d.render(img.data());
+    long s = 0;
+    for (auto b : img) s += b;
+    printf("%ld %d\n", s, sp.starSize);
+    return 0;
+  }
+  return 2;
+}
