@@ -22,7 +22,9 @@
 //                 happens before any add (snapshot semantics).
 // Trails (addTrails, :98-174) are a multi-frame effect and are not part of
 // a single frame: on the first frame they leave the image unchanged.
+#include <algorithm>
 #include <cstring>
+#include <limits>
 #include <new>
 #include <vector>
 
@@ -39,6 +41,7 @@ struct bt_stars {
   float* pos;
   float* mag;
   int* tree;
+  float4* box;
   uchar3* psf;
 };
 
@@ -51,78 +54,221 @@ static dim3 grid2(int w, int h) {
   return dim3((unsigned)((w + TX - 1) / TX), (unsigned)((h + TY - 1) / TY));
 }
 
-// Star tests a pixel may spend in k_star_cells before it is handed to the
-// warp-cooperative kernel.  Pixels next to the shadow project onto slivers
-// whose bounding boxes cover most of the sky (hundreds of thousands of
-// candidate stars); one such lane would stall its warp for the whole frame.
+// Star tests (node tests count kNodeCost) a pixel may spend in the warp
+// path before it is handed to k_star_heavy, and the number of kd-tree
+// leaves it may list.  Pixels next to the shadow project onto quads that
+// hold up to hundreds of thousands of stars; they get a whole block.
 constexpr long kStarBudget = 2048;
+constexpr int kLeaves = 32;
+constexpr int kWarps = TX * TY / 32;
 
-// distortStarMap without trails: splat cells + flag per pixel; pixels over
-// the budget are queued for k_star_heavy.
-__global__ void k_star_cells(const float2* __restrict__ thphi,
-                             const uint8_t* __restrict__ bh, StarSet S, Cam7 cam,
-                             int M, int N, int step, const float2* __restrict__ view,
-                             int lr, const float* __restrict__ area,
-                             float3* __restrict__ cells, uint8_t* __restrict__ flag,
-                             uint32_t* __restrict__ heavy, uint32_t* nheavy) {
-  const int j = blockIdx.x * TX + threadIdx.x;
-  const int i = blockIdx.y * TY + threadIdx.y;
-  if (i >= N || j >= M) return;
-  const size_t ij = (size_t)i * M + j;
-  const int fw = 2 * step + 1;
-  const int r = pixel_stars(thphi, bh, S, cam.v, M, N, step, view, lr, area, i, j,
-                            cells + ij * fw * fw, kStarBudget);
-  flag[ij] = r == 1 ? 1 : 0;
-  if (r == 2) heavy[atomicAdd(nheavy, 1u)] = (uint32_t)ij;
+// Broadcast of a star hit from lane b.
+__device__ __forceinline__ StarHit shfl_hit(const StarHit& h, int b) {
+  StarHit o;
+  o.st = __shfl_sync(0xffffffffu, h.st, b);
+  o.sp = __shfl_sync(0xffffffffu, h.sp, b);
+  o.part = __shfl_sync(0xffffffffu, h.part, b);
+  o.hsp.x = __shfl_sync(0xffffffffu, h.hsp.x, b);
+  o.hsp.y = __shfl_sync(0xffffffffu, h.hsp.y, b);
+  o.hsp.z = __shfl_sync(0xffffffffu, h.hsp.z, b);
+  return o;
 }
 
-constexpr int kHeavyThreads = 256;  // one block per deferred pixel
-constexpr int kHeavyNodes = 2048;   // nodes per search pass (shared memory)
-constexpr int kMaxCells = 25;       // (2s+1)^2 for step <= 2 in registers
-
-// The deferred pixels, one block each.  Thread 0 walks the kd-tree (in
-// passes of kHeavyNodes emitted nodes) into shared memory with a prefix sum
-// of the nodes' star counts; then all threads sweep the concatenated star
-// ranges, each accumulating its hits into its own cell registers, and a
-// block reduction adds the partial cells.  Sums are reassociated (not in the
-// reference's star order), which changes them only by float rounding.
-__global__ void __launch_bounds__(kHeavyThreads)
-k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
+// distortStarMap without trails, one warp per 32 pixels of a row.
+// Phase A, lane = pixel: corners, lensing, redshift, kd-tree search; the
+// leaves whose stars may fall inside the pixel's quad are listed in shared
+// memory (pixels over the budget go to the heavy list).  Phase B, for each
+// pixel of the warp in turn: the warp tests the listed stars 32 at a time,
+// the lanes holding a hit place their star in the pixel (bisection) and
+// colour it, and the hits are splatted in star order: lane c < (2s+1)^2
+// owns cell c and adds each star's contribution in the order the reference
+// does, so every cell is bit-identical to the reference's.
+__global__ void __launch_bounds__(TX * TY)
+k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
              StarSet S, Cam7 cam, int M, int N, int step,
              const float2* __restrict__ view, int lr, const float* __restrict__ area,
              float3* __restrict__ cells, uint8_t* __restrict__ flag,
-             const uint32_t* __restrict__ heavy, const uint32_t* nheavy) {
-  __shared__ int sh_node[kHeavyNodes];
-  __shared__ int sh_end[kHeavyNodes];  // inclusive prefix of star counts
-  __shared__ int sh_count, sh_more, sh_total;
-  __shared__ float sh_red[kHeavyThreads / 32][kMaxCells * 3];
-  __shared__ int sh_any;
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const uint32_t n = *nheavy;
+             uint32_t* __restrict__ heavy, uint32_t* nheavy) {
+  __shared__ int sh_leaf[kWarps][kLeaves][32];
+  __shared__ PixelCore sh_core[kWarps][32];
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const int j = blockIdx.x * TX + lane;
+  const int i = blockIdx.y * TY + w;
+  const bool valid = i < N && j < M;
+  const size_t ij = valid ? (size_t)i * M + j : 0;
   const int fw = 2 * step + 1, fw2 = fw * fw;
-  for (uint32_t item = blockIdx.x; item < n; item += gridDim.x) {
-    const uint32_t ij = heavy[item];
+
+  // ---- phase A: this lane's pixel ----
+  int nleaf = 0;
+  if (valid) {
+    PixelStars P;
+    float mn[2], mx[2];
+    if (pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, i, j, P, mn, mx)) {
+      P.budget = kStarBudget;
+      tree_search(S, mn, mx, [&](int node) {
+        walk_leaves(P, S, node, node_level(node), [&](int leaf) {
+          int a0, a1;
+          node_range(S, leaf, a0, a1);
+          P.tested += a1 - a0;
+          if (P.tested > P.budget || nleaf == kLeaves) {
+            P.abort = true;
+            return false;
+          }
+          sh_leaf[w][nleaf++][lane] = leaf;
+          return true;
+        });
+        return !P.abort;
+      });
+      if (P.abort) {
+        heavy[atomicAdd(nheavy, 1u)] = (uint32_t)ij;
+        nleaf = 0;
+      } else if (nleaf) {
+        sh_core[w][lane] = core_of(P);
+      }
+    }
+  }
+  __syncwarp();
+
+  // ---- phase B: the warp splats each listed pixel ----
+  int my_any = 0;
+  for (int px = 0; px < 32; px++) {
+    const int n = __shfl_sync(0xffffffffu, nleaf, px);
+    if (n == 0) continue;
+    PixelStars P;
+    stars_of(sh_core[w][px], step, P);
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+    bool any = false;
+    for (int k = 0; k < n; k++) {
+      int a0, a1;
+      node_range(S, sh_leaf[w][k][px], a0, a1);
+      for (int base = a0; base < a1; base += 32) {
+        const int q = base + lane;
+        float st = 0.f, sp = 0.f;
+        const bool in = q < a1 && star_test(P, S, q, st, sp);
+        unsigned ball = __ballot_sync(0xffffffffu, in);
+        if (!ball) continue;
+        any = true;
+        StarHit h{};
+        if (in) h = star_hit(P, S, q, st, sp);
+        while (ball) {
+          const int b = __ffs(ball) - 1;
+          ball &= ball - 1;
+          const StarHit hb = shfl_hit(h, b);
+          float3 l;
+          if (lane < fw2 && cell_light(P, hb, lane / fw, lane % fw, l)) {
+            acc.x += l.x;
+            acc.y += l.y;
+            acc.z += l.z;
+          }
+        }
+      }
+    }
+    if (any) {
+      const size_t pij = (size_t)i * M + (blockIdx.x * TX + px);
+      if (lane < fw2) cells[pij * fw2 + lane] = acc;
+      if (lane == px) my_any = 1;
+    }
+  }
+  // heavy pixels are written 0 here and flagged again by k_star_heavy
+  if (valid) flag[ij] = (uint8_t)my_any;
+}
+
+constexpr int kHeavyThreads = 512;  // one block per deferred pixel
+constexpr int kHeavyWarps = kHeavyThreads / 32;
+constexpr int kHeavyNodes = 1024;   // nodes per search pass (shared memory)
+// Deferred pixels with at least this many candidate leaves are scheduled
+// first, so that the longest pixels do not start last.
+constexpr long long kGiantLeaves = 512;
+
+// heavy_count layout: [0] deferred pixels, [1] giant, [2] other, [3] the
+// workers' shared item counter.
+enum { kHcDeferred = 0, kHcGiant = 1, kHcOther = 2, kHcNext = 3, kHcWords = 4 };
+
+// Sorts the deferred pixels into two queues in `order`: giant pixels from
+// the front, the others from the back.
+__global__ void k_heavy_plan(const float2* __restrict__ thphi,
+                             const uint8_t* __restrict__ bh, StarSet S, Cam7 cam,
+                             int M, int step, const float2* __restrict__ view, int lr,
+                             const float* __restrict__ area,
+                             const uint32_t* __restrict__ heavy, uint32_t* hc,
+                             uint32_t* __restrict__ order, uint32_t np) {
+  const uint32_t n = hc[kHcDeferred];
+  const int L = S.treeLevel;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += gridDim.x * blockDim.x) {
+    const uint32_t ij = heavy[k];
+    PixelStars P;
+    float mn[2], mx[2];
+    pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, ij / M, ij % M, P, mn, mx);
+    long long leaves = 0;
+    tree_search(S, mn, mx, [&](int node) {
+      leaves += 1ll << (L - node_level(node));
+      return leaves < kGiantLeaves;
+    });
+    if (leaves >= kGiantLeaves) order[atomicAdd(&hc[kHcGiant], 1u)] = ij;
+    else order[np - 1 - atomicAdd(&hc[kHcOther], 1u)] = ij;
+  }
+}
+
+// The deferred pixels, one block at a time each, taken from the queues by a
+// shared counter (giant pixels first).  Thread 0 walks the kd-tree (in
+// passes of kHeavyNodes emitted nodes) into shared memory with a prefix sum
+// of the number of leaves under each node.  The block then takes that flat
+// range of candidate leaves 256 at a time: each thread tests one leaf's
+// bounding box against the pixel's quad, the survivors are compacted in
+// thread order, and each warp sweeps the stars of one surviving leaf at a
+// time, 32 stars per step.  A thread that holds a hit splats it into its own
+// (2s+1)^2 cell registers with the per-star form of the brightness
+// (star_fast); the threads' cells are added by a block reduction at the end.
+// Sums are reassociated relative to the reference's star order, which
+// changes them only by float rounding; the order is fixed, so frames are
+// reproducible.
+template <int kStep>
+__global__ void __launch_bounds__(kHeavyThreads, 1)
+k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
+             StarSet S, Cam7 cam, int M, int N, const float2* __restrict__ view,
+             int lr, const float* __restrict__ area, float3* __restrict__ cells,
+             uint8_t* __restrict__ flag, const uint32_t* __restrict__ order,
+             uint32_t* hc, uint32_t np) {
+  constexpr int FW = 2 * kStep + 1, FW2 = FW * FW;
+  __shared__ int sh_node[kHeavyNodes];
+  __shared__ long long sh_end[kHeavyNodes];  // inclusive prefix of leaf counts
+  __shared__ int sh_count, sh_more;
+  __shared__ long long sh_total;
+  __shared__ int sh_surv[kHeavyThreads];
+  __shared__ int sh_wcount[kHeavyWarps];
+  __shared__ float3 sh_red[kHeavyWarps][FW2];
+  __shared__ uint32_t sh_item;
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int L = S.treeLevel;
+  for (;;) {
+    if (tid == 0) sh_item = atomicAdd(&hc[kHcNext], 1u);
+    __syncthreads();
+    const uint32_t item = sh_item;
+    const uint32_t ng = hc[kHcGiant], no = hc[kHcOther];
+    __syncthreads();
+    if (item >= ng + no) break;
+    const uint32_t ij = item < ng ? order[item] : order[np - 1 - (item - ng)];
     const int i = ij / M, j = ij % M;
     PixelStars P;
     float mn[2], mx[2];
-    pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, i, j, P, mn, mx);
-    float3 acc[kMaxCells];
+    pixel_setup(thphi, bh, cam.v, M, kStep, view, lr, area, i, j, P, mn, mx);
+    float3 acc[FW2];
 #pragma unroll
-    for (int c = 0; c < kMaxCells; c++) acc[c] = make_float3(0.f, 0.f, 0.f);
+    for (int c = 0; c < FW2; c++) acc[c] = make_float3(0.f, 0.f, 0.f);
     int any = 0;
     int skip = 0;
     for (;;) {
       if (tid == 0) {
-        int emitted = 0, count = 0, more = 0, total = 0;
+        int emitted = 0, count = 0, more = 0;
+        long long total = 0;
         tree_search(S, mn, mx, [&](int node) {
           if (emitted >= skip + kHeavyNodes) {
             more = 1;
             return false;
           }
           if (emitted >= skip) {
-            int startN = 0;
-            if (node != 0 && ((node + 1) & node) != 0) startN = S.tree[node - 1];
-            total += S.tree[node] - startN;
+            total += 1ll << (L - node_level(node));
             sh_node[count] = node;
             sh_end[count] = total;
             count++;
@@ -135,67 +281,94 @@ k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
         sh_total = total;
       }
       __syncthreads();
-      const int count = sh_count, total = sh_total;
-      for (int k = tid; k < total; k += kHeavyThreads) {
-        // node holding the k-th candidate: first end > k
-        int lo = 0, hi = count - 1;
-        while (lo < hi) {
-          const int mid = (lo + hi) >> 1;
-          if (sh_end[mid] > k) hi = mid;
-          else lo = mid + 1;
+      const int count = sh_count;
+      const long long total = sh_total;
+      for (long long base = 0; base < total; base += kHeavyThreads) {
+        const long long k = base + tid;
+        int leaf = -1;
+        if (k < total) {
+          int lo = 0, hi = count - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (sh_end[mid] > k) hi = mid;
+            else lo = mid + 1;
+          }
+          const int node = sh_node[lo];
+          const int d = L - node_level(node);
+          leaf = (int)((((long long)node + 1) << d) - 1 + (k - (lo ? sh_end[lo - 1] : 0)));
+          if (node_excluded(P, S.box[leaf])) leaf = -1;
         }
-        const int node = sh_node[lo];
-        int startN = 0;
-        if (node != 0 && ((node + 1) & node) != 0) startN = S.tree[node - 1];
-        const int q = startN + (k - (lo ? sh_end[lo - 1] : 0));
-        float st, sp;
-        if (!star_test(P, S, q, st, sp)) continue;
-        any = 1;
-        const StarHit h = star_hit(P, S, q, st, sp);
+        // compaction in thread order
+        const unsigned keep = __ballot_sync(0xffffffffu, leaf >= 0);
+        if (lane == 0) sh_wcount[w] = __popc(keep);
+        __syncthreads();
+        int wbase = 0, ns = 0;
+        for (int ww = 0; ww < kHeavyWarps; ww++) {
+          if (ww < w) wbase += sh_wcount[ww];
+          ns += sh_wcount[ww];
+        }
+        if (leaf >= 0) sh_surv[wbase + __popc(keep & ((1u << lane) - 1u))] = leaf;
+        __syncthreads();
+        for (int s = w; s < ns; s += kHeavyWarps) {
+          int a0, a1;
+          node_range(S, sh_surv[s], a0, a1);
+          for (int q = a0 + lane; q < a1; q += 32) {
+            float st, sp;
+            if (!star_test(P, S, q, st, sp)) continue;
+            any = 1;
+            const StarHit h = star_hit(P, S, q, st, sp);
+            const StarFast f = star_fast(P, h);
 #pragma unroll
-        for (int c = 0; c < kMaxCells; c++) {
-          if (c >= fw2) break;
-          float3 l;
-          if (cell_light(P, h, c / fw, c % fw, l)) {
-            acc[c].x += l.x;
-            acc[c].y += l.y;
-            acc[c].z += l.z;
+            for (int c = 0; c < FW2; c++) {
+              float3 l;
+              if (cell_light_fast(P, h, f, c / FW, c % FW, l)) {
+                acc[c].x += l.x;
+                acc[c].y += l.y;
+                acc[c].z += l.z;
+              }
+            }
           }
         }
+        __syncthreads();
       }
       const int more = sh_more;
       __syncthreads();
       if (!more) break;
       skip += kHeavyNodes;
     }
-    // block reduction of the cells
     any = __syncthreads_or(any);
     if (any) {
 #pragma unroll
-      for (int c = 0; c < kMaxCells; c++) {
-        if (c >= fw2) break;
+      for (int c = 0; c < FW2; c++) {
         float x = acc[c].x, y = acc[c].y, z = acc[c].z;
         for (int o = 16; o > 0; o >>= 1) {
           x += __shfl_xor_sync(0xffffffffu, x, o);
           y += __shfl_xor_sync(0xffffffffu, y, o);
           z += __shfl_xor_sync(0xffffffffu, z, o);
         }
-        if (lane == 0) {
-          sh_red[w][3 * c] = x;
-          sh_red[w][3 * c + 1] = y;
-          sh_red[w][3 * c + 2] = z;
-        }
+        if (lane == 0) sh_red[w][c] = make_float3(x, y, z);
       }
       __syncthreads();
-      if (tid < 3 * fw2) {
-        float v = 0.f;
-        for (int ww = 0; ww < kHeavyThreads / 32; ww++) v += sh_red[ww][tid];
-        ((float*)(cells + (size_t)ij * fw2))[tid] = v;
+      if (tid < FW2) {
+        float3 v = make_float3(0.f, 0.f, 0.f);
+        for (int ww = 0; ww < kHeavyWarps; ww++) {
+          v.x += sh_red[ww][tid].x;
+          v.y += sh_red[ww][tid].y;
+          v.z += sh_red[ww][tid].z;
+        }
+        cells[(size_t)ij * FW2 + tid] = v;
       }
     }
     if (tid == 0) flag[ij] = any ? 1 : 0;
     __syncthreads();
   }
+}
+
+template <int kStep>
+void launch_heavy(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
+  k_star_heavy<kStep><<<sm_count() * 2, kHeavyThreads, 0, s>>>(
+      Sc.thphi, Sc.bh, *F.stars, F.cam, Sc.M, Sc.N, F.view, F.lr, Sc.area, Sc.cells,
+      Sc.flag, Sc.heavy_order, Sc.heavy_count, (uint32_t)((size_t)Sc.M * Sc.N));
 }
 
 // sumStarLight (+ makePix + addStarsAndBackground when no diffraction).
@@ -350,13 +523,16 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
     set_error("star splat step > 2 is not supported");
     return BT_ERR_ARG;
   }
-  BT_CUDA_TRY(cudaMemsetAsync(Sc.heavy_count, 0, sizeof(uint32_t), s));
+  BT_CUDA_TRY(cudaMemsetAsync(Sc.heavy_count, 0, kHcWords * sizeof(uint32_t), s));
   k_star_cells<<<grid2(M, N), dim3(TX, TY), 0, s>>>(
       Sc.thphi, Sc.bh, *F.stars, F.cam, M, N, F.step, F.view, F.lr, Sc.area,
-      Sc.cells, Sc.flag, Sc.heavy_list, Sc.heavy_count);
-  k_star_heavy<<<sm_count() * 4, kHeavyThreads, 0, s>>>(
-      Sc.thphi, Sc.bh, *F.stars, F.cam, M, N, F.step, F.view, F.lr, Sc.area,
-      Sc.cells, Sc.flag, Sc.heavy_list, Sc.heavy_count);
+      Sc.cells, Sc.flag, Sc.heavy_list, Sc.heavy_count + kHcDeferred);
+  k_heavy_plan<<<sm_count() * 2, 128, 0, s>>>(
+      Sc.thphi, Sc.bh, *F.stars, F.cam, M, F.step, F.view, F.lr, Sc.area, Sc.heavy_list,
+      Sc.heavy_count, Sc.heavy_order, (uint32_t)np);
+  if (F.step == 0) launch_heavy<0>(Sc, F, s);
+  else if (F.step == 1) launch_heavy<1>(Sc, F, s);
+  else launch_heavy<2>(Sc, F, s);
   BT_CUDA_TRY(cudaGetLastError());
   const bool diff = F.diffraction && F.stars->psf && F.stars->psf_size > 0;
   if (!diff) {
@@ -437,6 +613,40 @@ struct TreeBuilder {
   }
 };
 
+// Bounding box of every node's stars (theta_min, phi_min, theta_max,
+// phi_max), leaves from their star ranges, inner nodes from their children.
+// NaN coordinates are left out: the quad test rejects such stars.  Returns
+// false when the tree's cumulative counts do not describe ranges inside
+// [0, n) -- the kernels would read past the star arrays.
+bool node_boxes(const float* pos, int n, const int* tree, int L,
+                std::vector<float4>& box) {
+  const size_t nodes = ((size_t)2 << L) - 1;
+  const float inf = std::numeric_limits<float>::infinity();
+  box.assign(nodes, make_float4(inf, inf, -inf, -inf));
+  const size_t first = ((size_t)1 << L) - 1;
+  int prev = 0;
+  for (size_t k = first; k < nodes; k++) {
+    const int start = k == first ? 0 : prev;
+    const int end = tree[k];
+    if (end < start || end > n) return false;
+    prev = end;
+    float4 b = box[k];
+    for (int q = start; q < end; q++) {
+      const float t = pos[2 * (size_t)q], p = pos[2 * (size_t)q + 1];
+      if (t != t || p != p) continue;
+      b.x = std::min(b.x, t); b.y = std::min(b.y, p);
+      b.z = std::max(b.z, t); b.w = std::max(b.w, p);
+    }
+    box[k] = b;
+  }
+  for (size_t k = first; k-- > 0;) {
+    const float4 a = box[2 * k + 1], c = box[2 * k + 2];
+    box[k] = make_float4(std::min(a.x, c.x), std::min(a.y, c.y), std::max(a.z, c.z),
+                         std::max(a.w, c.w));
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" {
@@ -482,12 +692,22 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   if (!st) return BT_ERR_NOMEM;
   std::memset(st, 0, sizeof(*st));
   const size_t tsize = (size_t)bt_stars_tree_size(treeLevel);
+  std::vector<float4> box;
+  if (!node_boxes(star_pos, n, tree, treeLevel, box)) {
+    delete st;
+    set_error("invalid argument: the star tree's counts do not match %d stars", n);
+    return BT_ERR_ARG;
+  }
   cudaStream_t s = (cudaStream_t)stream;
   cudaError_t e = cudaMalloc((void**)&st->pos, (size_t)2 * n * sizeof(float) + 16);
   if (e == cudaSuccess) e = cudaMalloc((void**)&st->mag, (size_t)2 * n * sizeof(float) + 16);
   if (e == cudaSuccess) e = cudaMalloc((void**)&st->tree, tsize * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&st->box, box.size() * sizeof(float4));
   if (e == cudaSuccess && psf_size)
     e = cudaMalloc((void**)&st->psf, (size_t)psf_size * psf_size * 3);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(st->box, box.data(), box.size() * sizeof(float4),
+                        cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess && n)
     e = cudaMemcpyAsync(st->pos, star_pos, (size_t)2 * n * sizeof(float),
                         cudaMemcpyHostToDevice, s);
@@ -501,7 +721,8 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
                         cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
-    cudaFree(st->pos); cudaFree(st->mag); cudaFree(st->tree); cudaFree(st->psf);
+    cudaFree(st->pos); cudaFree(st->mag); cudaFree(st->tree); cudaFree(st->box);
+    cudaFree(st->psf);
     delete st;
     set_error("star set upload failed: %s", cudaGetErrorString(e));
     return BT_ERR_CUDA;
@@ -511,6 +732,7 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   st->s.pos = st->pos;
   st->s.mag = st->mag;
   st->s.tree = st->tree;
+  st->s.box = st->box;
   st->s.psf = st->psf;
   st->s.psf_size = psf_size;
   *out = st;
@@ -522,6 +744,7 @@ void bt_stars_destroy(bt_stars* st) {
   cudaFree(st->pos);
   cudaFree(st->mag);
   cudaFree(st->tree);
+  cudaFree(st->box);
   if (st->psf) cudaFree(st->psf);
   delete st;
 }

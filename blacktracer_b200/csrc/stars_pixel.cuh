@@ -21,6 +21,10 @@ struct StarSet {
   const int* tree;   // 2^(treeLevel+1)-1 cumulative counts
   const uchar3* psf; // diffraction sprite, psf_size^2 (may be NULL)
   int psf_size;
+  // Bounding box of each node's stars, (theta_min, phi_min, theta_max,
+  // phi_max); min > max for a node without stars.  Not part of the
+  // reference's layout: derived from pos and tree when the set is created.
+  const float4* box;
 };
 
 #define BT_HD __host__ __device__ __forceinline__
@@ -33,6 +37,13 @@ BT_HD int ffs_u32(unsigned x) {
 #endif
 }
 BT_HD int imax(int a, int b) { return a > b ? a : b; }
+BT_HD int clz_u32(unsigned x) {
+#ifdef __CUDA_ARCH__
+  return __clz((int)x);
+#else
+  return x ? __builtin_clz(x) : 32;
+#endif
+}
 BT_HD int imin(int a, int b) { return a < b ? a : b; }
 
 using namespace mapm;
@@ -113,6 +124,9 @@ BT_HD void in_pixel(float t0, float t1, float t2, float t3, float p0,
 struct PixelStars {
   float t[4], p[4];
   int sgn;
+  // Edge k of the quad test as cross_pos computes it: c1 = sgn * (corner k -
+  // corner k+1), anchored at corner k+1.
+  float et[4], ep[4];
   bool picheck;
   long tested, budget;  // star tests so far / allowed before deferring
   bool abort;
@@ -129,9 +143,12 @@ struct PixelStars {
 template <class Emit>
 BT_HD void tree_search(const StarSet& S, const float* mn, const float* mx,
                        Emit&& emit) {
+  // nodeStart / nodeSize of the reference as scalars (axis 0: theta, 1: phi)
+  // so that nothing is indexed by the run-time axis.
+  const float mn0 = mn[0], mn1 = mn[1], mx0 = mx[0], mx1 = mx[1];
   const int L = S.treeLevel;
-  float nodeStart[2] = {0.f, 0.f};
-  float nodeSize[2] = {PI, PI2};
+  float st0 = 0.f, st1 = 0.f;
+  float sz0 = PI, sz1 = PI2;
   int node = 0;
   unsigned bitMask = (unsigned)powf(2, L);
   int level = 0, lvl = 0;
@@ -142,20 +159,19 @@ BT_HD void tree_search(const StarSet& S, const float* mn, const float* mx,
       int star_n = S.tree[node];
       if (node != 0 && ((node + 1) & node) != 0) star_n -= S.tree[node - 1];
       const int tp = lvl & 1;
-      const float x_overlap = fmaxf(0.f, fminf(mx[0], nodeStart[0] + nodeSize[0]) -
-                                             fmaxf(mn[0], nodeStart[0]));
-      const float y_overlap = fmaxf(0.f, fminf(mx[1], nodeStart[1] + nodeSize[1]) -
-                                             fmaxf(mn[1], nodeStart[1]));
+      const float x_overlap = fmaxf(0.f, fminf(mx0, st0 + sz0) - fmaxf(mn0, st0));
+      const float y_overlap = fmaxf(0.f, fminf(mx1, st1 + sz1) - fmaxf(mn1, st1));
       const float overlapArea = x_overlap * y_overlap;
-      const bool size = overlapArea / (nodeSize[0] * nodeSize[1]) > 0.8f;
-      nodeSize[tp] = nodeSize[tp] * .5f;
+      const bool size = overlapArea / (sz0 * sz1) > 0.8f;
+      if (tp) sz1 = sz1 * .5f;
+      else sz0 = sz0 * .5f;
       if (star_n == 0) {
         node = node * 2 + 1;
         break;
       }
-      const float check = nodeStart[tp] + nodeSize[tp];
-      const bool lu = mn[tp] < check;
-      const bool rd = mx[tp] >= check;
+      const float check = tp ? st1 + sz1 : st0 + sz0;
+      const bool lu = (tp ? mn1 : mn0) < check;
+      const bool rd = (tp ? mx1 : mx0) >= check;
       if (lvl == L || (rd && lu && size)) {
         if (rd && !emit(node * 2 + 2)) return;
         if (lu && !emit(node * 2 + 1)) return;
@@ -170,14 +186,18 @@ BT_HD void tree_search(const StarSet& S, const float* mn, const float* mx,
     if (level >= 0) {
       const int diff = lvl - level;
       for (int k = 0; k < diff; k++) {
-        const int tp = (lvl - k) & 1;
-        if (!(node & 1)) nodeStart[tp] -= nodeSize[tp];
-        nodeSize[tp] = nodeSize[tp] * 2.f;
+        if ((lvl - k) & 1) {
+          if (!(node & 1)) st1 -= sz1;
+          sz1 = sz1 * 2.f;
+        } else {
+          if (!(node & 1)) st0 -= sz0;
+          sz0 = sz0 * 2.f;
+        }
         node = (node - 1) / 2;
       }
       node++;
-      const int tp = level & 1;
-      nodeStart[tp] += nodeSize[tp];
+      if (level & 1) st1 += sz1;
+      else st0 += sz0;
     }
   }
 }
@@ -207,6 +227,12 @@ BT_HD bool pixel_setup(const float2* thphi, const uint8_t* bh, const float* cam,
   const float orient = (t[1] - t[0]) * (p[1] + p[0]) + (t[2] - t[1]) * (p[2] + p[1]) +
                        (t[3] - t[2]) * (p[3] + p[2]) + (t[0] - t[3]) * (p[0] + p[3]);
   P.sgn = orient < 0 ? -1 : 1;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int k1 = (k + 1) & 3;
+    P.et[k] = (float)P.sgn * (t[k] - t[k1]);
+    P.ep[k] = (float)P.sgn * (p[k] - p[k1]);
+  }
   P.redshft = 1.f;
   P.frac = 1.f;
   if (lr) lensing_redshift(P.t, P.p, M, ind, cam, view, P.frac, P.redshft, area[ij]);
@@ -260,14 +286,15 @@ BT_HD StarHit star_hit(const PixelStars& P, const StarSet& S, int q, float st,
 
 // Contribution of a star to cell (u, v) of its pixel, squared RGB
 // (BT/MakeImageKernel.cu:305-320).  Returns false outside the splat radius.
-BT_HD bool cell_light(const PixelStars& P, const StarHit& h, int u, int v,
-                      float3& out) {
-  const float dist = dist_sq(-P.step + u + .5f, h.st, -P.step + v + .5f, h.sp);
-  if (dist > P.maxDistSq) return false;
-  const float appMag = h.part - 2.5f * log10f(P.frac * gaussian(dist));
+BT_HD bool cell_light_v(int step, float maxDistSq, float frac, float st, float sp,
+                        float part, float hx, float hy, float hz, int u, int v,
+                        float3& out) {
+  const float dist = dist_sq(-step + u + .5f, st, -step + v + .5f, sp);
+  if (dist > maxDistSq) return false;
+  const float appMag = part - 2.5f * log10f(frac * gaussian(dist));
   const float brightness = 100 * exp10f(-.4f * appMag);
   float r, g, b;
-  hsp_to_rgb(h.hsp.x, h.hsp.y, h.hsp.z * brightness, r, g, b);
+  hsp_to_rgb(hx, hy, hz * brightness, r, g, b);
   r *= 255.f;
   g *= 255.f;
   b *= 255.f;
@@ -275,56 +302,194 @@ BT_HD bool cell_light(const PixelStars& P, const StarHit& h, int u, int v,
   return true;
 }
 
-// Tests and splats the stars of one tree node (distortStarMap's inner loop,
-// BT/MakeImageKernel.cu:278-324, without trails).
-BT_HD void splat_node(PixelStars& P, const StarSet& S, int node) {
-  int startN = 0;
-  if (node != 0 && ((node + 1) & node) != 0) startN = S.tree[node - 1];
-  const int endN = S.tree[node];
-  P.tested += endN - startN;
-  if (P.tested > P.budget) {
-    P.abort = true;
-    return;
+BT_HD bool cell_light(const PixelStars& P, const StarHit& h, int u, int v,
+                      float3& out) {
+  return cell_light_v(P.step, P.maxDistSq, P.frac, h.st, h.sp, h.part, h.hsp.x, h.hsp.y,
+                      h.hsp.z, u, v, out);
+}
+
+// True when no star inside box b (theta/phi ranges) can pass the quad test
+// of pixel P: for one of the four edges, every point of the box lies on the
+// rejecting side by more than the rounding error of cross_pos's float
+// evaluation.  cross_pos(k) is c1t*(sp - pb) - (st - tb)*c1p > 0, linear in
+// the star position, so its maximum over the box is at a corner; that maximum
+// is compared against a bound of the float evaluation's error.  Both that evaluation and this one (in float too) are within a few
+// units of 2^-24 of the terms' magnitudes (mag); the margin is 1e-5 * mag.
+BT_HD bool box_outside(const PixelStars& P, float tmin, float pmin, float tmax,
+                       float pmax) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int k1 = (k + 1) & 3;
+    const float c1t = P.et[k], c1p = P.ep[k];
+    const float tb = P.t[k1], pb = P.p[k1];
+    const float sp = c1t > 0 ? pmax : pmin;
+    const float st = c1p > 0 ? tmin : tmax;
+    const float fmax = c1t * (sp - pb) - (st - tb) * c1p;
+    const float mag = fabsf(c1t) * fmaxf(fabsf(pmax - pb), fabsf(pmin - pb)) +
+                      fabsf(c1p) * fmaxf(fabsf(tmax - tb), fabsf(tmin - tb));
+    if (fmax < -(1e-5f * mag + 1e-30f)) return true;
   }
-  const int fw = 2 * P.step + 1;
-  for (int q = startN; q < endN; q++) {
-    float st, sp;
-    if (!star_test(P, S, q, st, sp)) continue;
-    if (!P.any) {
-      for (int c = 0; c < fw * fw; c++) P.cells[c] = make_float3(0.f, 0.f, 0.f);
-      P.any = true;
+  return false;
+}
+
+// True when star_test rejects every star of a node with bounding box b,
+// including the seam retry at phi + 2pi that pixels straddling phi = 0 take
+// for stars with phi < 0.2 * 2pi.
+BT_HD bool node_excluded(const PixelStars& P, float4 b) {
+  if (!(b.x <= b.z) || !(b.y <= b.w)) return true;  // no stars
+  if (!box_outside(P, b.x, b.y, b.z, b.w)) return false;
+  if (!P.picheck || !(b.y < PI2 * .2f)) return true;
+  const float lo = b.y + PI2, hi = fminf(b.w, PI2 * .2f) + PI2;
+  return box_outside(P, b.x, lo - 1e-5f, b.z, hi + 1e-5f);
+}
+
+// Visits, left to right, the leaves under `root` (a node at level `lvl`)
+// that hold a star which may pass the pixel's quad test; subtrees whose
+// bounding box excludes every star are skipped.  Leaf star ranges are
+// contiguous in tree order, so the visited stars keep the order of a plain
+// scan of root's range, minus stars the test rejects anyway.
+template <class Visit>
+BT_HD bool walk_leaves(PixelStars& P, const StarSet& S, int root, int lvl,
+                       Visit&& visit) {
+  const int L = S.treeLevel;
+  int k = root, l = lvl;
+  for (;;) {
+    // a node test costs about as much as four star tests
+    P.tested += 4;
+    if (P.tested > P.budget) {
+      P.abort = true;
+      return false;
     }
-    const StarHit h = star_hit(P, S, q, st, sp);
-    for (int u = 0; u <= 2 * P.step; u++)
-      for (int v = 0; v <= 2 * P.step; v++) {
-        float3 l;
-        if (!cell_light(P, h, u, v, l)) continue;
-        float3& c = P.cells[fw * u + v];
-        c.x += l.x;
-        c.y += l.y;
-        c.z += l.z;
+    if (!node_excluded(P, S.box[k])) {
+      if (l >= L) {
+        if (!visit(k)) return false;
+      } else {
+        k = 2 * k + 1;
+        l++;
+        continue;
       }
+    }
+    // next node in pre-order inside root's subtree
+    while (k != root && (k & 1) == 0) {
+      k = (k - 1) >> 1;
+      l--;
+    }
+    if (k == root) return true;
+    k++;
   }
 }
 
-// The whole of distortStarMap for pixel (i, j) (no trails).  Returns 0 (no
-// star), 1 (stars; cells written) or 2 (more than `budget` star tests:
-// nothing written, the pixel is left to the warp-cooperative path).
-BT_HD int pixel_stars(const float2* thphi, const uint8_t* bh, const StarSet& S,
-                      const float* cam, int M, int N, int step, const float2* view,
-                      int lr, const float* area, int i, int j, float3* cells,
-                      long budget = 0x7fffffffffffL) {
-  PixelStars P;
-  float mn[2], mx[2];
-  P.cells = cells;
-  if (!pixel_setup(thphi, bh, cam, M, step, view, lr, area, i, j, P, mn, mx)) return 0;
-  P.budget = budget;
-  tree_search(S, mn, mx, [&](int node) {
-    splat_node(P, S, node);
-    return !P.abort;
-  });
-  if (P.abort) return 2;
-  return P.any ? 1 : 0;
+// Level of node k in the implicit complete binary tree.
+BT_HD int node_level(int k) { return 31 - clz_u32((unsigned)k + 1u); }
+
+// Star tests a node costs in a pixel's budget (about four star tests).
+constexpr int kNodeCost = 4;
+
+// Start and end of a node's star range.
+BT_HD void node_range(const StarSet& S, int node, int& a0, int& a1) {
+  a0 = (node != 0 && ((node + 1) & node) != 0) ? S.tree[node - 1] : 0;
+  a1 = S.tree[node];
+}
+
+// The per-pixel values the star tests and the splat need, compact enough to
+// pass between lanes through shared memory.
+struct PixelCore {
+  float t[4], p[4];
+  float red, redshft, frac;
+  int bits;  // bit 0: picheck, bit 1: sgn < 0
+};
+
+BT_HD PixelCore core_of(const PixelStars& P) {
+  PixelCore c;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    c.t[k] = P.t[k];
+    c.p[k] = P.p[k];
+  }
+  c.red = P.red;
+  c.redshft = P.redshft;
+  c.frac = P.frac;
+  c.bits = (P.picheck ? 1 : 0) | (P.sgn < 0 ? 2 : 0);
+  return c;
+}
+
+BT_HD void stars_of(const PixelCore& c, int step, PixelStars& P) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    P.t[k] = c.t[k];
+    P.p[k] = c.p[k];
+  }
+  P.sgn = (c.bits & 2) ? -1 : 1;
+  P.picheck = (c.bits & 1) != 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int k1 = (k + 1) & 3;
+    P.et[k] = (float)P.sgn * (P.t[k] - P.t[k1]);
+    P.ep[k] = (float)P.sgn * (P.p[k] - P.p[k1]);
+  }
+  P.red = c.red;
+  P.redshft = c.redshft;
+  P.frac = c.frac;
+  P.step = step;
+  P.maxDistSq = (step + .5f) * (step + .5f);
+  P.tested = 0;
+  P.budget = 0x7fffffffffffL;
+  P.abort = false;
+  P.any = false;
+  P.cells = nullptr;
+}
+
+// Per-star factors of the splat in a cheaper form.  cell_light computes
+//   100 * 10^(-0.4 * (part - 2.5 log10(frac * g))) = 100 * 10^(-0.4 part) * frac * g
+// and HSPtoRGB(h, s, p * b) = b * HSPtoRGB(h, s, p) (the HSP model is
+// linear in its perceived brightness), so a star's colour and brightness are
+// computed once and each cell needs only its Gaussian.  The two forms agree
+// to float rounding (relative ~1e-6).  `ok` is false where the rewrite could
+// differ by more than rounding -- a magnification factor that is not a
+// positive finite number, or a brightness large enough for HSPtoRGB's P*P to
+// overflow -- and those stars take cell_light.
+struct StarFast {
+  float b0;          // 100 * 10^(-0.4 part) * frac
+  float r0, g0, bl0; // 255 * HSPtoRGB(h, s, p)
+  bool ok;
+};
+
+BT_HD StarFast star_fast(const PixelStars& P, const StarHit& h) {
+  StarFast f;
+  f.b0 = 100.f * exp10f(-.4f * h.part) * P.frac;
+  float r, g, b;
+  hsp_to_rgb(h.hsp.x, h.hsp.y, h.hsp.z, r, g, b);
+  f.r0 = 255.f * r;
+  f.g0 = 255.f * g;
+  f.bl0 = 255.f * b;
+  f.ok = P.frac > 0.f && f.b0 < 1e15f && f.b0 > 0.f && h.hsp.z <= 1.f;
+  return f;
+}
+
+// cell_light kept out of line for the rare stars star_fast does not cover,
+// so that the unrolled cell loops around cell_light_fast stay small.
+#ifdef __CUDA_ARCH__
+__device__ __noinline__
+#else
+inline
+#endif
+bool cell_light_slow(int step, float maxDistSq, float frac, float st, float sp, float part,
+                     float hx, float hy, float hz, int u, int v, float3& out) {
+  return cell_light_v(step, maxDistSq, frac, st, sp, part, hx, hy, hz, u, v, out);
+}
+
+BT_HD bool cell_light_fast(const PixelStars& P, const StarHit& h, const StarFast& f,
+                           int u, int v, float3& out) {
+  if (!f.ok)
+    return cell_light_slow(P.step, P.maxDistSq, P.frac, h.st, h.sp, h.part, h.hsp.x,
+                           h.hsp.y, h.hsp.z, u, v, out);
+  const float dist = dist_sq(-P.step + u + .5f, h.st, -P.step + v + .5f, h.sp);
+  if (dist > P.maxDistSq) return false;
+  // gaussian(dist) = exp(-dist / (2 sigma^2)) / (sigma sqrt(2 pi)), sigma = 0.4
+  const float b = f.b0 * (expf(-3.125f * dist) * 0.99735570f);
+  const float r = f.r0 * b, g = f.g0 * b, bl = f.bl0 * b;
+  out = make_float3(r * r, g * g, bl * bl);
+  return true;
 }
 
 #undef BT_HD

@@ -119,9 +119,11 @@ def test_render_argument_errors(bt, cuda):
         R.render_raw(0, 9, 16, 3, cuda.zeros(17 * 9 * 2, device="cuda"), [0] * 7)
 
 
-def test_heavy_pixels_vs_reference(bt, cuda, oracle_mod):
+@pytest.mark.parametrize("step", [1, 0, 2])
+def test_heavy_pixels_vs_reference(bt, cuda, oracle_mod, step):
     """Many candidate stars per pixel (shallow tree, 60k stars): most pixels
-    exceed the per-thread budget and take the warp-cooperative path."""
+    exceed the warp path's budget and take the block-per-pixel path; every
+    splat radius the renderer supports."""
     case = ("g_c2_l7s4", 128, 64, 128, 60000, 4)
     g, cam, grid, ref_grid, rows, GM, bgr, stars, W, H, tl = setup_case(bt, cuda, oracle_mod, case)
     cam7 = cam.getParamArray()
@@ -129,11 +131,30 @@ def test_heavy_pixels_vs_reference(bt, cuda, oracle_mod):
     viewer = bt.Viewer(np.pi / 2, 0, 0, W, H, True)
     R = bt.Renderer(W, H)
     sp = bt.StarProcessor(*stars, treeLevel=tl)
-    out = R.render(grid, viewer, cam, stars=sp, lr=True).cpu().numpy()
+    out = R.render(grid, viewer, cam, stars=sp, lr=True, step=step).cpu().numpy()
     pos, mg, tree = oracle_mod.ref_star_tree(*stars, tl)
     ref = oracle_mod.ref_map_frame(ref_grid, rows, GM, grid.MAXLEVEL, view, W, H, cam7,
-                                   stars=(pos, mg, tree, tl))
-    compare_img(out, ref["image"].reshape(H, W, 4), "heavy stars")
+                                   stars=(pos, mg, tree, tl), step=step)
+    compare_img(out, ref["image"].reshape(H, W, 4), f"heavy stars step {step}")
+    again = R.render(grid, viewer, cam, stars=sp, lr=True, step=step).cpu().numpy()
+    assert np.array_equal(out, again), "frames must be reproducible"
+
+
+@pytest.mark.parametrize("step", [0, 2])
+def test_splat_step_vs_reference(bt, cuda, oracle_mod, step):
+    """Splat radius 0 and 2 through the warp path (deep tree): exact cells."""
+    g, cam, grid, ref_grid, rows, GM, bgr, stars, W, H, tl = setup_case(bt, cuda, oracle_mod,
+                                                                         CASES[0])
+    cam7 = cam.getParamArray()
+    view = sphere_view(W, H)
+    viewer = bt.Viewer(np.pi / 2, 0, 0, W, H, True)
+    R = bt.Renderer(W, H)
+    sp = bt.StarProcessor(*stars, treeLevel=tl)
+    out = R.render(grid, viewer, cam, stars=sp, lr=True, step=step).cpu().numpy()
+    pos, mg, tree = oracle_mod.ref_star_tree(*stars, tl)
+    ref = oracle_mod.ref_map_frame(ref_grid, rows, GM, grid.MAXLEVEL, view, W, H, cam7,
+                                   stars=(pos, mg, tree, tl), step=step)
+    compare_img(out, ref["image"].reshape(H, W, 4), f"stars step {step}", exact_frac=0.999)
 
 
 def test_colour_index_clamped_to_table(bt, cuda, oracle_mod):
