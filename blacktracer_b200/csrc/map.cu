@@ -151,33 +151,79 @@ __device__ __forceinline__ float4 sat_lin(const float4* sat, long idx, long tota
   return sat[idx];
 }
 
+// Colour of a pixel from its summed environment (B, G, R, solid angle):
+// gamma, HSP, lensing and redshift (BT/MakeImageKernel.cu:725-750); BGRA8.
+__device__ __forceinline__ uchar4 env_finish(float4 color, const float* t, const float* p,
+                                             int M, int ind, const Cam7& cam,
+                                             const float2* view, float solidangle, int lr) {
+  color.x = fminf(255.f, powf(color.x / color.w, 1.f / 2.2f));
+  color.y = fminf(255.f, powf(color.y / color.w, 1.f / 2.2f));
+  color.z = fminf(255.f, powf(color.z / color.w, 1.f / 2.2f));
+  float H, S, P;
+  rgb_to_hsp(color.z / 255.f, color.y / 255.f, color.x / 255.f, H, S, P);
+  if (lr) {
+    float redshft, frac;
+    lensing_redshift(t, p, M, ind, cam.v, view, frac, redshft, solidangle);
+    P *= frac;
+    P = powf(P, redshft);
+  }
+  hsp_to_rgb(H, S, fminf(1.f, P), color.z, color.y, color.x);
+  return make_uchar4((unsigned char)min(255, int(color.x * 255)),
+                     (unsigned char)min(255, int(color.y * 255)),
+                     (unsigned char)min(255, int(color.z * 255)), 255);
+}
+
+// Columns of the environment map a projected pixel spans (BT/MakeImageKernel.cu:650-657).
+struct EnvSpan {
+  float pixSize;
+  int pixMin, pixNum;
+};
+
+__device__ __forceinline__ EnvSpan env_span(const float* p, int rows) {
+  EnvSpan e;
+  e.pixSize = PI / float(rows);
+  const float phMax = fmaxf(fmaxf(p[0], p[1]), fmaxf(p[2], p[3]));
+  const float phMin = fminf(fminf(p[0], p[1]), fminf(p[2], p[3]));
+  const int pixMax = int(phMax / e.pixSize);
+  e.pixMin = int(phMin / e.pixSize);
+  e.pixNum = pixMax - e.pixMin + 1;
+  if (e.pixNum > 1 && pixMax * e.pixSize > phMax) e.pixNum -= 1;
+  return e;
+}
+
+// Pixels spanning at least this many environment columns are integrated by
+// a warp each (k_env_wide); next to the shadow a pixel can span all of them.
+constexpr int kEnvWide = 48;
+
 // distortEnvironmentMap (BT/MakeImageKernel.cu:631-751): integrate the
 // environment over the projected pixel column by column with two
 // summed-area reads per column, gamma, HSP, lensing and redshift; BGRA8.
+// Pixels spanning kEnvWide columns or more are queued for k_env_wide.
 __global__ void k_env(const float2* __restrict__ thphi, uchar4* __restrict__ out,
                       const uint8_t* __restrict__ bh, int rows, int cols, int M,
                       int N, const float4* __restrict__ sat, Cam7 cam,
                       const float* __restrict__ solidangle,
-                      const float2* __restrict__ view, int lr) {
+                      const float2* __restrict__ view, int lr,
+                      uint32_t* __restrict__ wide, uint32_t* nwide) {
   const int j = blockIdx.x * TX + threadIdx.x;
   const int i = blockIdx.y * TY + threadIdx.y;
   if (i >= N || j >= M) return;
   const size_t ij = (size_t)i * M + j;
   const long total = (long)rows * cols;
-  float4 color = make_float4(0.f, 0.f, 0.f, 0.f);
   if (bh[ij] == 0) {
     float t[4], p[4];
     bool picheck = false;
     const int ind = i * (M + 1) + j;
     const bool ok = pixel_corners(thphi, ind, M, t, p, picheck, 0.f);
     if (ok && ind > 0) {  // pixel (0,0) is never coloured by the reference
-      const float pixSize = PI / float(rows);
-      const float phMax = fmaxf(fmaxf(p[0], p[1]), fmaxf(p[2], p[3]));
-      const float phMin = fminf(fminf(p[0], p[1]), fminf(p[2], p[3]));
-      const int pixMax = int(phMax / pixSize);
-      const int pixMin = int(phMin / pixSize);
-      int pixNum = pixMax - pixMin + 1;
-      if (pixNum > 1 && pixMax * pixSize > phMax) pixNum -= 1;
+      const EnvSpan e = env_span(p, rows);
+      const float pixSize = e.pixSize;
+      const int pixMin = e.pixMin, pixNum = e.pixNum;
+      if (pixNum >= kEnvWide) {
+        wide[atomicAdd(nwide, 1u)] = (uint32_t)ij;
+        return;
+      }
+      float4 color = make_float4(0.f, 0.f, 0.f, 0.f);
       if (pixNum == 1) {
         const float thMax = fmaxf(fmaxf(t[0], t[1]), fmaxf(t[2], t[3]));
         const float thMin = fminf(fminf(t[0], t[1]), fminf(t[2], t[3]));
@@ -188,6 +234,8 @@ __global__ void k_env(const float2* __restrict__ thphi, uchar4* __restrict__ out
         color.z += mx.z - mn.z;
         color.w += mx.w - mn.w;
       } else if (pixNum < cols) {
+        // max2/min2 are running extremes over all boundaries so far, as in
+        // the reference (they are not reset per column)
         float max1 = -100, min1 = cols + 1, max2 = -100, min2 = cols + 1;
         for (int s = 0; s <= pixNum; s++) {
           const float cp = (pixMin + s) * pixSize;
@@ -232,23 +280,122 @@ __global__ void k_env(const float2* __restrict__ thphi, uchar4* __restrict__ out
           color.w += mx.w - mn.w;
         }
       }
-      color.x = fminf(255.f, powf(color.x / color.w, 1.f / 2.2f));
-      color.y = fminf(255.f, powf(color.y / color.w, 1.f / 2.2f));
-      color.z = fminf(255.f, powf(color.z / color.w, 1.f / 2.2f));
-      float H, S, P;
-      rgb_to_hsp(color.z / 255.f, color.y / 255.f, color.x / 255.f, H, S, P);
-      if (lr) {
-        float redshft, frac;
-        lensing_redshift(t, p, M, ind, cam.v, view, frac, redshft, solidangle[ij]);
-        P *= frac;
-        P = powf(P, redshft);
-      }
-      hsp_to_rgb(H, S, fminf(1.f, P), color.z, color.y, color.x);
+      out[ij] = env_finish(color, t, p, M, ind, cam, view, solidangle[ij], lr);
+      return;
     }
   }
-  out[ij] = make_uchar4((unsigned char)min(255, int(color.x * 255)),
-                        (unsigned char)min(255, int(color.y * 255)),
-                        (unsigned char)min(255, int(color.z * 255)), 255);
+  out[ij] = make_uchar4(0, 0, 0, 255);
+}
+
+// Adds the per-column differences d of 32 consecutive columns (one per lane,
+// `n` of them valid, lane order = column order) to `color` one after the
+// other, as the reference's sequential loop does; every lane ends with the
+// same color.
+__device__ __forceinline__ void add_in_order(float4& color, float4 d, int n) {
+  for (int b = 0; b < n; b++) {
+    color.x += __shfl_sync(0xffffffffu, d.x, b);
+    color.y += __shfl_sync(0xffffffffu, d.y, b);
+    color.z += __shfl_sync(0xffffffffu, d.z, b);
+    color.w += __shfl_sync(0xffffffffu, d.w, b);
+  }
+}
+
+// The wide pixels of k_env, one warp each: 32 columns per step, the running
+// theta extremes of the reference as a warp prefix max/min, column sums
+// added in column order (bit-identical to the per-thread loop).
+__global__ void k_env_wide(const float2* __restrict__ thphi, uchar4* __restrict__ out,
+                           int rows, int cols, int M, const float4* __restrict__ sat,
+                           Cam7 cam, const float* __restrict__ solidangle,
+                           const float2* __restrict__ view, int lr,
+                           const uint32_t* __restrict__ wide, const uint32_t* nwide) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t n = *nwide;
+  const long total = (long)rows * cols;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t item = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; item < n;
+       item += warps) {
+    const uint32_t ij = wide[item];
+    const int i = ij / M, j = ij % M;
+    float t[4], p[4];
+    bool picheck = false;
+    const int ind = i * (M + 1) + j;
+    pixel_corners(thphi, ind, M, t, p, picheck, 0.f);
+    const EnvSpan e = env_span(p, rows);
+    const float pixSize = e.pixSize;
+    const int pixMin = e.pixMin, pixNum = e.pixNum;
+    float4 color = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (pixNum < cols) {
+      float cmax = -100, cmin = cols + 1;  // running extremes before this step
+      for (int s0 = 0; s0 <= pixNum; s0 += 32) {
+        const int s = s0 + lane;
+        float lmax = -100, lmin = cols + 1;
+        if (s <= pixNum) {
+          const float cp = (pixMin + s) * pixSize;
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const float ap = p[q], bp = p[(q + 1) & 3];
+            const float at = t[q], bt = t[(q + 1) & 3];
+            if ((cp - ap) * (cp - bp) <= 0) {
+              const float ct = at + (bt - at) / (bp - ap) * (cp - ap);
+              lmin = ct < lmin ? ct : lmin;
+              lmax = ct > lmax ? ct : lmax;
+            }
+          }
+        }
+        // inclusive prefix max / min over the lanes, then the carry
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const float a = __shfl_up_sync(0xffffffffu, lmax, o);
+          const float b = __shfl_up_sync(0xffffffffu, lmin, o);
+          if (lane >= o) {
+            lmax = a > lmax ? a : lmax;
+            lmin = b < lmin ? b : lmin;
+          }
+        }
+        lmax = lmax > cmax ? lmax : cmax;
+        lmin = lmin < cmin ? lmin : cmin;
+        float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (s >= 1 && s <= pixNum) {
+          const int col = (pixMin + s) % cols;
+          const long index1 = (long)int(lmax / pixSize) * cols + col;
+          const long index2 = (long)(int(lmin / pixSize) - 1) * cols + col;
+          const float4 mx = sat_lin(sat, index1, total);
+          const float4 mn = index2 > 0 ? sat_lin(sat, index2, total)
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+          d = make_float4(mx.x - mn.x, mx.y - mn.y, mx.z - mn.z, mx.w - mn.w);
+        }
+        // columns s >= 1 only: lane 0 of the first step holds boundary 0
+        const int first = s0 == 0 ? 1 : 0;
+        const int last = min(31, pixNum - s0);
+        for (int b = first; b <= last; b++) {
+          color.x += __shfl_sync(0xffffffffu, d.x, b);
+          color.y += __shfl_sync(0xffffffffu, d.y, b);
+          color.z += __shfl_sync(0xffffffffu, d.z, b);
+          color.w += __shfl_sync(0xffffffffu, d.w, b);
+        }
+        cmax = __shfl_sync(0xffffffffu, lmax, 31);
+        cmin = __shfl_sync(0xffffffffu, lmin, 31);
+      }
+    } else {
+      const float thMax = fmaxf(fmaxf(t[0], t[1]), fmaxf(t[2], t[3]));
+      const float thMin = fminf(fminf(t[0], t[1]), fminf(t[2], t[3]));
+      const long thMaxPix = (long)int(thMax / pixSize) * cols;
+      const long thMinPix = (long)int(thMin / pixSize) * cols;
+      for (int q0 = 0; q0 < pixNum; q0 += 32) {
+        const int q = q0 + lane;
+        float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (q < pixNum) {
+          const int col = (pixMin + q) % cols;
+          const float4 mx = sat_lin(sat, thMaxPix + col, total);
+          const float4 mn = sat_lin(sat, thMinPix + col, total);
+          d = make_float4(mx.x - mn.x, mx.y - mn.y, mx.z - mn.z, mx.w - mn.w);
+        }
+        add_in_order(color, d, min(32, pixNum - q0));
+      }
+    }
+    const uchar4 px = env_finish(color, t, p, M, ind, cam, view, solidangle[ij], lr);
+    if (lane == 0) out[ij] = px;
+  }
 }
 
 int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s) {
@@ -261,9 +408,13 @@ int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s) {
   k_smooth_v<<<grid2(M, N), dim3(TX, TY), 0, s>>>(S.area_tmp, S.area, S.bh, S.gap, M, N);
   BT_CUDA_TRY(cudaGetLastError());
   if (F.map && F.env) {
+    BT_CUDA_TRY(cudaMemsetAsync(S.env_wide_count, 0, sizeof(uint32_t), s));
     k_env<<<grid2(M, N), dim3(TX, TY), 0, s>>>(
         S.thphi, (uchar4*)F.out_bg, S.bh, F.env->rows, F.env->cols, M, N,
-        F.env->sat, F.cam, S.area, F.view, F.lr);
+        F.env->sat, F.cam, S.area, F.view, F.lr, S.env_wide, S.env_wide_count);
+    k_env_wide<<<sm_count() * 8, 256, 0, s>>>(
+        S.thphi, (uchar4*)F.out_bg, F.env->rows, F.env->cols, M, F.env->sat, F.cam,
+        S.area, F.view, F.lr, S.env_wide, S.env_wide_count);
     BT_CUDA_TRY(cudaGetLastError());
   }
   return BT_OK;

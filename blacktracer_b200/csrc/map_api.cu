@@ -24,7 +24,8 @@ void map_free(bt_map* m) {
   void* ptrs[] = {m->S.thphi, m->S.gap,   m->S.bh,        m->S.area,
                   m->S.area_tmp, m->S.light, m->S.light2, m->S.stars_img,
                   m->S.flag, m->S.cells, m->S.diff_list, m->S.diff_count,
-                  m->S.heavy_list, m->S.heavy_order, m->S.heavy_count, m->tmp_img};
+                  m->S.heavy_list, m->S.heavy_order, m->S.heavy_count, m->S.env_wide,
+                  m->S.env_wide_count, m->tmp_img};
   for (void* p : ptrs)
     if (p) cudaFree(p);
 }
@@ -126,6 +127,8 @@ int bt_map_create(int width, int height, bt_map** out) {
   MALLOC(S.diff_count, sizeof(uint32_t));
   MALLOC(S.heavy_list, np * sizeof(uint32_t));
   MALLOC(S.heavy_order, np * sizeof(uint32_t));
+  MALLOC(S.env_wide, np * sizeof(uint32_t));
+  MALLOC(S.env_wide_count, sizeof(uint32_t));
   MALLOC(S.heavy_count, 4 * sizeof(uint32_t));
   MALLOC(m->tmp_img, np * 4);
 #undef MALLOC

@@ -32,6 +32,8 @@ struct MapScratch {
   int cells_fw;         // 2s+1 the cells were sized for
   uint32_t* diff_list;  // bright pixels (diffraction)
   uint32_t* diff_count;
+  uint32_t* env_wide;   // pixels spanning many environment columns
+  uint32_t* env_wide_count;
   uint32_t* heavy_list; // pixels deferred to the block-per-pixel star path
   uint32_t* heavy_order;// the same, queued giant-first
   uint32_t* heavy_count;// 4 counters (deferred, giant, other, next item)

@@ -42,6 +42,7 @@ struct bt_stars {
   float* mag;
   int* tree;
   float4* box;
+  float4* bb;  // 2 * kBlackbodyEntries: HSP, then RGB at unit brightness
   uchar3* psf;
 };
 
@@ -239,6 +240,8 @@ k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
   __shared__ int sh_wcount[kHeavyWarps];
   __shared__ float3 sh_red[kHeavyWarps][FW2];
   __shared__ uint32_t sh_item;
+  __shared__ int sh_q[kHeavyWarps][64];
+  __shared__ float2 sh_qpos[kHeavyWarps][64];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int L = S.treeLevel;
   for (;;) {
@@ -258,6 +261,24 @@ k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
     for (int c = 0; c < FW2; c++) acc[c] = make_float3(0.f, 0.f, 0.f);
     int any = 0;
     int skip = 0;
+    // Stars that passed the quad test wait in a per-warp queue and are
+    // placed, coloured and splatted 32 at a time, one per lane.
+    int qn = 0;
+    auto splat_queued = [&](int k) {
+      const int q = sh_q[w][k];
+      const float2 pos = sh_qpos[w][k];
+      const StarHit h = star_hit(P, S, q, pos.x, pos.y);
+      const StarFast f = star_fast(P, S, h);
+#pragma unroll
+      for (int c = 0; c < FW2; c++) {
+        float3 l;
+        if (cell_light_fast(P, h, f, c / FW, c % FW, l)) {
+          acc[c].x += l.x;
+          acc[c].y += l.y;
+          acc[c].z += l.z;
+        }
+      }
+    };
     for (;;) {
       if (tid == 0) {
         int emitted = 0, count = 0, more = 0;
@@ -312,20 +333,29 @@ k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
         for (int s = w; s < ns; s += kHeavyWarps) {
           int a0, a1;
           node_range(S, sh_surv[s], a0, a1);
-          for (int q = a0 + lane; q < a1; q += 32) {
-            float st, sp;
-            if (!star_test(P, S, q, st, sp)) continue;
+          for (int qb = a0; qb < a1; qb += 32) {
+            const int q = qb + lane;
+            float st = 0.f, sp = 0.f;
+            const bool in = q < a1 && star_test(P, S, q, st, sp);
+            const unsigned ball = __ballot_sync(0xffffffffu, in);
+            if (!ball) continue;
             any = 1;
-            const StarHit h = star_hit(P, S, q, st, sp);
-            const StarFast f = star_fast(P, h);
-#pragma unroll
-            for (int c = 0; c < FW2; c++) {
-              float3 l;
-              if (cell_light_fast(P, h, f, c / FW, c % FW, l)) {
-                acc[c].x += l.x;
-                acc[c].y += l.y;
-                acc[c].z += l.z;
+            if (in) {
+              const int at = qn + __popc(ball & ((1u << lane) - 1u));
+              sh_q[w][at] = q;
+              sh_qpos[w][at] = make_float2(st, sp);
+            }
+            qn += __popc(ball);
+            if (qn >= 32) {
+              __syncwarp();
+              splat_queued(lane);
+              __syncwarp();
+              if (lane < qn - 32) {
+                sh_q[w][lane] = sh_q[w][lane + 32];
+                sh_qpos[w][lane] = sh_qpos[w][lane + 32];
               }
+              qn -= 32;
+              __syncwarp();
             }
           }
         }
@@ -336,6 +366,8 @@ k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
       if (!more) break;
       skip += kHeavyNodes;
     }
+    if (lane < qn) splat_queued(lane);
+    __syncwarp();
     any = __syncthreads_or(any);
     if (any) {
 #pragma unroll
@@ -362,6 +394,17 @@ k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
     if (tid == 0) flag[ij] = any ? 1 : 0;
     __syncthreads();
   }
+}
+
+// The per-entry colour tables of StarSet (bb_hsp, bb_rgb).
+__global__ void k_blackbody_tables(float4* __restrict__ bb) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= kBlackbodyEntries) return;
+  const float3 h = blackbody_hsp(k);
+  float r, g, b;
+  hsp_to_rgb(h.x, h.y, h.z, r, g, b);
+  bb[k] = make_float4(h.x, h.y, h.z, 0.f);
+  bb[kBlackbodyEntries + k] = make_float4(255.f * r, 255.f * g, 255.f * b, 0.f);
 }
 
 template <int kStep>
@@ -703,6 +746,11 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   if (e == cudaSuccess) e = cudaMalloc((void**)&st->mag, (size_t)2 * n * sizeof(float) + 16);
   if (e == cudaSuccess) e = cudaMalloc((void**)&st->tree, tsize * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void**)&st->box, box.size() * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&st->bb, 2 * kBlackbodyEntries * sizeof(float4));
+  if (e == cudaSuccess) {
+    k_blackbody_tables<<<(kBlackbodyEntries + 127) / 128, 128, 0, s>>>(st->bb);
+    e = cudaGetLastError();
+  }
   if (e == cudaSuccess && psf_size)
     e = cudaMalloc((void**)&st->psf, (size_t)psf_size * psf_size * 3);
   if (e == cudaSuccess)
@@ -722,7 +770,7 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     cudaFree(st->pos); cudaFree(st->mag); cudaFree(st->tree); cudaFree(st->box);
-    cudaFree(st->psf);
+    cudaFree(st->bb); cudaFree(st->psf);
     delete st;
     set_error("star set upload failed: %s", cudaGetErrorString(e));
     return BT_ERR_CUDA;
@@ -733,6 +781,8 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   st->s.mag = st->mag;
   st->s.tree = st->tree;
   st->s.box = st->box;
+  st->s.bb_hsp = st->bb;
+  st->s.bb_rgb = st->bb + kBlackbodyEntries;
   st->s.psf = st->psf;
   st->s.psf_size = psf_size;
   *out = st;
@@ -745,6 +795,7 @@ void bt_stars_destroy(bt_stars* st) {
   cudaFree(st->mag);
   cudaFree(st->tree);
   cudaFree(st->box);
+  cudaFree(st->bb);
   if (st->psf) cudaFree(st->psf);
   delete st;
 }

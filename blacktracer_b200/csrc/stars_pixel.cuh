@@ -21,6 +21,10 @@ struct StarSet {
   const int* tree;   // 2^(treeLevel+1)-1 cumulative counts
   const uchar3* psf; // diffraction sprite, psf_size^2 (may be NULL)
   int psf_size;
+  // Per blackbody entry: RGBtoHSP of its colour (h, s, p) and
+  // 255 * HSPtoRGB(h, s, p), computed once on the device by the same code.
+  const float4* bb_hsp;
+  const float4* bb_rgb;
   // Bounding box of each node's stars, (theta_min, phi_min, theta_max,
   // phi_max); min > max for a node without stars.  Not part of the
   // reference's layout: derived from pos and tree when the set is created.
@@ -245,7 +249,29 @@ BT_HD bool pixel_setup(const float2* thphi, const uint8_t* bh, const float* cam,
 struct StarHit {
   float st, sp, part;
   float3 hsp;
+  int bb;  // blackbody entry
 };
+
+// Blackbody entry of a star of colour index bv seen with redshift factor
+// redshft (BT/MakeImageKernel.cu:294-297).
+BT_HD int blackbody_index(float bv, float redshft) {
+  const float temp = 46.f / redshft *
+                         ((1.f / ((0.92f * bv) + 1.7f)) + (1.f / ((0.92f * bv) + 0.62f))) -
+                     10.f;
+  // The reference clamps to 1170 (BT/MakeImageKernel.cu:297), the length of
+  // the flattened table minus 3, then reads tempToRGB[3*index]: shifted
+  // temperatures above 40000 K read past its 391 entries.  Clamped to the
+  // last entry (40000 K) here.
+  return imax(0, imin((int)floorf(temp), kBlackbodyEntries - 1));
+}
+
+// RGBtoHSP of blackbody entry k (BT/MakeImageKernel.cu:298-301).
+BT_HD float3 blackbody_hsp(int k) {
+  float3 h;
+  rgb_to_hsp((float)blackbody(3 * k) / 255.f, (float)blackbody(3 * k + 1) / 255.f,
+             (float)blackbody(3 * k + 2) / 255.f, h.x, h.y, h.z);
+  return h;
+}
 
 // The quad test of star q (with the seam retry), BT/MakeImageKernel.cu:285-291.
 BT_HD bool star_test(const PixelStars& P, const StarSet& S, int q, float& st,
@@ -270,17 +296,9 @@ BT_HD StarHit star_hit(const PixelStars& P, const StarSet& S, int q, float st,
   h.st = st;
   h.sp = sp;
   h.part = S.mag[2 * q] + P.red;
-  const float bv = S.mag[2 * q + 1];
-  const float temp = 46.f / P.redshft *
-                         ((1.f / ((0.92f * bv) + 1.7f)) + (1.f / ((0.92f * bv) + 0.62f))) -
-                     10.f;
-  // The reference clamps to 1170 (BT/MakeImageKernel.cu:297), the length of
-  // the flattened table minus 3, then reads tempToRGB[3*index]: shifted
-  // temperatures above 40000 K read past its 391 entries.  Clamped to the
-  // last entry (40000 K) here.
-  const int index = imax(0, imin((int)floorf(temp), kBlackbodyEntries - 1));
-  rgb_to_hsp((float)blackbody(3 * index) / 255.f, (float)blackbody(3 * index + 1) / 255.f,
-             (float)blackbody(3 * index + 2) / 255.f, h.hsp.x, h.hsp.y, h.hsp.z);
+  h.bb = blackbody_index(S.mag[2 * q + 1], P.redshft);
+  const float4 c = S.bb_hsp[h.bb];
+  h.hsp = make_float3(c.x, c.y, c.z);
   return h;
 }
 
@@ -454,14 +472,13 @@ struct StarFast {
   bool ok;
 };
 
-BT_HD StarFast star_fast(const PixelStars& P, const StarHit& h) {
+BT_HD StarFast star_fast(const PixelStars& P, const StarSet& S, const StarHit& h) {
   StarFast f;
   f.b0 = 100.f * exp10f(-.4f * h.part) * P.frac;
-  float r, g, b;
-  hsp_to_rgb(h.hsp.x, h.hsp.y, h.hsp.z, r, g, b);
-  f.r0 = 255.f * r;
-  f.g0 = 255.f * g;
-  f.bl0 = 255.f * b;
+  const float4 c = S.bb_rgb[h.bb];
+  f.r0 = c.x;
+  f.g0 = c.y;
+  f.bl0 = c.z;
   f.ok = P.frac > 0.f && f.b0 < 1e15f && f.b0 > 0.f && h.hsp.z <= 1.f;
   return f;
 }
@@ -486,7 +503,12 @@ BT_HD bool cell_light_fast(const PixelStars& P, const StarHit& h, const StarFast
   const float dist = dist_sq(-P.step + u + .5f, h.st, -P.step + v + .5f, h.sp);
   if (dist > P.maxDistSq) return false;
   // gaussian(dist) = exp(-dist / (2 sigma^2)) / (sigma sqrt(2 pi)), sigma = 0.4
-  const float b = f.b0 * (expf(-3.125f * dist) * 0.99735570f);
+#ifdef __CUDA_ARCH__
+  const float gauss = __expf(-3.125f * dist) * 0.99735570f;
+#else
+  const float gauss = expf(-3.125f * dist) * 0.99735570f;
+#endif
+  const float b = f.b0 * gauss;
   const float r = f.r0 * b, g = f.g0 * b, bl = f.bl0 * b;
   out = make_float3(r * r, g * g, bl * bl);
   return true;
