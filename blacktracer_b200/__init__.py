@@ -8,10 +8,11 @@ reference interfaces; device buffers are torch CUDA tensors.
 """
 from ._lib import (BtError, PRECISION_MIXED, PRECISION_PLAIN, RAY_CAPTURED,  # noqa: F401
                    RAY_ESCAPED, RAY_MAXSTEP, RAY_NONCONVERGED, lib)
-from .host import (BlackHole, Camera, Grid, IntegOpts, grid_dims,  # noqa: F401
+from .host import (BlackHole, Camera, Grid, GridSet, IntegOpts, grid_dims,  # noqa: F401
                    integrate_rays, integrate_rays_host)
 
 from .render import Environment, Renderer, StarProcessor, Viewer  # noqa: F401
 
-__all__ = ["Environment", "Renderer", "StarProcessor", "Viewer", "BlackHole", "Camera", "Grid", "IntegOpts", "grid_dims", "integrate_rays",
+__all__ = ["Environment", "Renderer", "StarProcessor", "Viewer", "BlackHole", "Camera", "Grid",
+           "GridSet", "IntegOpts", "grid_dims", "integrate_rays",
            "integrate_rays_host", "BtError", "lib"]

@@ -53,6 +53,16 @@ class bt_grid_export_t(C.Structure):
                 ("n_blocks", C.c_size_t)]
 
 
+class bt_trace_shape(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("blocks_per_sm", C.c_int32)]
+
+
+class bt_batch_info(C.Structure):
+    _fields_ = [("count", C.c_int32), ("traced", C.c_int64), ("flags", C.c_uint32),
+                ("trace_ms", C.c_float), ("trace_launches", C.c_int32),
+                ("launches", C.c_int32), ("graph", C.c_int32), ("shape", bt_trace_shape)]
+
+
 class bt_frame(C.Structure):
     _fields_ = [("grid", C.c_void_p), ("grid_rows", C.c_int32), ("grid_cols", C.c_int32),
                 ("grid_level", C.c_int32), ("view", C.c_void_p), ("hor", C.c_float),
@@ -95,6 +105,19 @@ _SIGS = {
                                      C.POINTER(C.c_int32), C.POINTER(C.c_int32), _vp]),
     "bt_grid_export": (C.c_int, [_vp, C.POINTER(bt_grid_export_t), _vp]),
     "bt_grid_set_timing": (C.c_int, [_vp, C.c_int]),
+    "bt_grid_set_graph": (C.c_int, [_vp, C.c_int]),
+    "bt_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
+    "bt_batch_destroy": (None, [_vp]),
+    "bt_batch_build": (C.c_int, [_vp, C.POINTER(bt_camera), C.POINTER(C.c_double), C.c_int,
+                                 C.POINTER(bt_integ_opts), _vp]),
+    "bt_batch_grid": (_vp, [_vp, C.c_int]),
+    "bt_batch_set_graph": (C.c_int, [_vp, C.c_int]),
+    "bt_batch_set_timing": (C.c_int, [_vp, C.c_int]),
+    "bt_batch_set_shape": (C.c_int, [_vp, C.POINTER(bt_trace_shape)]),
+    "bt_batch_query": (C.c_int, [_vp, C.POINTER(bt_batch_info), _vp]),
+    "bt_batch_autotune": (C.c_int, [_vp, C.POINTER(bt_camera), C.POINTER(C.c_double), C.c_int,
+                                    C.POINTER(bt_integ_opts), C.c_int,
+                                    C.POINTER(bt_trace_shape), C.POINTER(C.c_float), _vp]),
     "bt_probe_fp64_tflops": (C.c_int, [C.POINTER(C.c_double), _vp]),
     "bt_view_sphere": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "bt_env_create": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp), _vp]),

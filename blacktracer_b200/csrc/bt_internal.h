@@ -93,14 +93,34 @@ struct GridCounters {
   uint32_t err;       // nonzero: a bounded loop gave up
 };
 
-// Traces the vertices listed in keys[0..*count) (lattice indices) into the
-// lattice.  Plain form in integrate.cu, mixed form in mixed.cu.
-int launch_trace_plain(const RayParams& p, const LatticeView& L,
-                       const uint32_t* keys, GridCounters* ctr,
-                       cudaStream_t s);
-int launch_trace_mixed(const RayParams& p, const LatticeView& L,
-                       const uint32_t* keys, GridCounters* ctr,
-                       cudaStream_t s);
+// One grid of a build set as the build kernels see it (device memory, one
+// entry per grid): lattice, ray parameters of its camera and spin, work
+// lists and counters.
+struct GridDesc {
+  LatticeView L;
+  RayParams p;
+  uint32_t* list[2];  // block lists of consecutive levels (ping-pong)
+  uint32_t* trace;    // vertices to trace this level
+  uint32_t* leaves;   // leaf blocks (level < max) in level order
+  double2* X[2];      // T-vertex fix pass buffers
+  GridCounters* ctr;
+};
+
+// Launch shape of the ray-tracing kernel: threads per block (64, 128 or
+// 256) and resident blocks per SM (0 = as many as fit).
+struct TraceShape {
+  int threads;
+  int blocks_per_sm;
+};
+
+// Traces the listed vertices of all G grids in one persistent launch: the
+// per-grid trace counts are laid end to end (qoff[g] = first queue entry of
+// grid g, qoff[G] = total) and lanes take entries from the shared queue head
+// *qfetch.  Plain form in integrate.cu, mixed form in mixed.cu.
+int launch_trace_plain(const GridDesc* D, int G, const uint32_t* qoff,
+                       uint32_t* qfetch, TraceShape shape, cudaStream_t s);
+int launch_trace_mixed(const GridDesc* D, int G, const uint32_t* qoff,
+                       uint32_t* qfetch, TraceShape shape, cudaStream_t s);
 
 }  // namespace bt
 

@@ -14,6 +14,16 @@
 // host: every launch reads its work count from device memory, so a whole
 // build is asynchronous and graph-capturable.
 //
+// Grids are built in sets (bt_batch): G grids of the same size, each with
+// its own camera and spin, advance through the levels together -- every
+// build kernel covers all G grids (blockIdx.y = grid), and each level's rays
+// of all grids go through one persistent trace launch with a shared work
+// queue, so that the long rays of one grid overlap the work of the others.
+// A lone grid (bt_grid_create) is a set of one.  The launch sequence of a
+// set depends only on its shape, start level, precision and trace launch
+// shape, so it can be captured once as a CUDA graph and replayed; cameras
+// and spins reach the kernels through device-resident descriptors.
+//
 // The T-vertex fix of the reference iterates an unordered_map, so its result
 // depends on the hash table's iteration order.  This build fixes blocks in a
 // canonical order -- level ascending, then key i<<32|j ascending, then edge
@@ -35,22 +45,18 @@
 namespace bt {
 
 constexpr int kMaxTfixPasses = 8;
-
-struct GridBuffers {
-  uint32_t* list[2];  // block lists of consecutive levels (ping-pong)
-  uint32_t* trace;    // vertices to trace this level
-  uint32_t* leaves;   // leaf blocks (level < max) in level order
-  double2* X[2];      // T-vertex fix pass buffers
-  size_t cap;         // capacity of each list (entries)
-};
+constexpr int kParamSlots = 2;  // pinned descriptor staging slots
 
 }  // namespace bt
 
+struct bt_batch;
+
 struct bt_grid {
-  bt::LatticeView L;
-  bt::GridBuffers B;
-  bt::GridCounters* ctr;       // device
-  bt::GridCounters* ctr_host;  // pinned mirror
+  bt_batch* set;               // the build set this grid belongs to
+  int index;                   // position in the set
+  bt::LatticeView L;           // slices of the set's arrays
+  bt::GridCounters* ctr;       // device (slice)
+  bt::GridCounters* ctr_host;  // pinned mirror (slice)
   bt::RayParams params;
   bt_camera cam;
   double a;
@@ -62,12 +68,46 @@ struct bt_grid {
   uint64_t* totals_host;
   char* compact;    // compact export staging (device), lazily sized
   size_t compact_bytes;
-  int launches;     // kernels launched by the last build
-  int timing;       // record CUDA events around the trace launches
-  cudaEvent_t ev[2 * 16];
-  int n_ev;
   int32_t map_rows;
   int sym;
+};
+
+struct bt_batch {
+  int G, N, M, eq, maxlevel;
+  size_t NM;
+  int standalone;  // created by bt_grid_create (a set of one)
+  bt_grid* grids;
+  // arrays of all members; member g at offset g*NM (lists: 4 per member,
+  // fix buffers: 2 per member)
+  double2* thphi;
+  int32_t* steps;
+  uint8_t* vflag;
+  uint8_t* vstat;
+  int8_t* blevel;
+  uint32_t* lists;
+  double2* X;
+  bt::GridCounters* ctr;
+  bt::GridCounters* ctr_host;
+  bt::GridDesc* D;        // device descriptors
+  bt::GridDesc* Dh[bt::kParamSlots];  // pinned staging
+  cudaEvent_t Dev[bt::kParamSlots];   // staging slot reusable once passed
+  int slot;
+  uint32_t* qoff;         // G + 1
+  uint32_t* qfetch;
+  bt::TraceShape shape;
+  int startlevel, precision;
+  int launches;           // kernels of the last build
+  int built;
+  // timing of the trace launches (eager builds only)
+  int timing;
+  cudaEvent_t ev[2 * 16];
+  int n_ev;
+  // graph replay
+  int graph;
+  cudaStream_t cap_stream;
+  cudaGraphExec_t exec;
+  int exec_startlevel, exec_precision;
+  bt::TraceShape exec_shape;
 };
 
 namespace bt {
@@ -94,8 +134,12 @@ static SeedShape seed_shape(const LatticeView& L) {
   return s;
 }
 
-__global__ void k_seed(LatticeView L, SeedShape S, uint32_t* trace,
-                       uint32_t* check, GridCounters* ctr) {
+__global__ void k_seed(const GridDesc* __restrict__ D, SeedShape S) {
+  const GridDesc& d = D[blockIdx.y];
+  const LatticeView L = d.L;
+  uint32_t* trace = d.trace;
+  uint32_t* check = d.list[0];
+  GridCounters* ctr = d.ctr;
   const uint32_t M = L.M;
   const bool uniform = L.maxlevel == L.startlevel;
   const uint32_t total = S.rows * S.cols;
@@ -132,7 +176,8 @@ __global__ void k_seed(LatticeView L, SeedShape S, uint32_t* trace,
 }
 
 // Pole copies of raytrace (BT/Grid.h:303-315), after the poles are traced.
-__global__ void k_pole_copy(LatticeView L) {
+__global__ void k_pole_copy(const GridDesc* __restrict__ D) {
+  const LatticeView L = D[blockIdx.y].L;
   const uint32_t gap = pow2u(L.maxlevel - L.startlevel);
   const uint32_t M = L.M, N = L.N;
   for (uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) * gap; j < M;
@@ -149,6 +194,32 @@ __global__ void k_pole_copy(LatticeView L) {
       L.vstat[s0 + j] = L.vstat[s0];
       L.vflag[s0 + j] = 1;
     }
+  }
+}
+
+// Queue offsets of the next trace launch: qoff[g] = rays of grids < g.
+__global__ void k_queue(const GridDesc* __restrict__ D, int G, uint32_t* qoff,
+                        uint32_t* qfetch) {
+  __shared__ uint32_t s[1024];
+  const int t = threadIdx.x, T = blockDim.x;
+  uint32_t carry = 0;
+  for (int base = 0; base < G; base += T) {
+    const uint32_t v = base + t < G ? *(volatile uint32_t*)&D[base + t].ctr->n_trace : 0u;
+    s[t] = v;
+    __syncthreads();
+    for (int o = 1; o < T; o <<= 1) {
+      const uint32_t a = t >= o ? s[t - o] : 0u;
+      __syncthreads();
+      s[t] += a;
+      __syncthreads();
+    }
+    if (base + t < G) qoff[base + t + 1] = carry + s[t];
+    carry += s[T - 1];
+    __syncthreads();
+  }
+  if (t == 0) {
+    qoff[0] = 0;
+    *qfetch = 0;
   }
 }
 
@@ -174,9 +245,14 @@ __device__ __forceinline__ void claim_vertex(const LatticeView& L, uint32_t i,
 
 // One level of adaptiveBlockIntegration (BT/Grid.h:476-497) with
 // refineCheck (:410-445) and fillVector (:453-459).
-__global__ void k_refine(LatticeView L, int level, const uint32_t* check,
-                         uint32_t* next, uint32_t* trace, uint32_t* leaves,
-                         GridCounters* ctr) {
+__global__ void k_refine(const GridDesc* __restrict__ D, int level, int cur) {
+  const GridDesc& d = D[blockIdx.y];
+  const LatticeView L = d.L;
+  const uint32_t* check = d.list[cur];
+  uint32_t* next = d.list[cur ^ 1];
+  uint32_t* trace = d.trace;
+  uint32_t* leaves = d.leaves;
+  GridCounters* ctr = d.ctr;
   const uint32_t n = *(volatile uint32_t*)&ctr->n_check;
   const uint32_t M = L.M;
   const uint32_t gap = pow2u(L.maxlevel - level);
@@ -213,9 +289,13 @@ __global__ void k_refine(LatticeView L, int level, const uint32_t* check,
   }
 }
 
-// Level hand-over.  after_seed: only account the seeded rays; otherwise the
-// next list becomes the check list and the leaf offset of `slot` is set.
-__global__ void k_advance(GridCounters* ctr, int after_seed, int slot) {
+// Level hand-over, one thread per grid.  after_seed: only account the
+// seeded rays; otherwise the next list becomes the check list and the leaf
+// offset of `slot` is set.
+__global__ void k_advance(const GridDesc* __restrict__ D, int G, int after_seed, int slot) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G) return;
+  GridCounters* ctr = D[g].ctr;
   uint64_t t = ((uint64_t)ctr->traced_hi << 32 | ctr->traced_lo) + ctr->n_trace;
   ctr->traced_lo = (uint32_t)t;
   ctr->traced_hi = (uint32_t)(t >> 32);
@@ -229,12 +309,13 @@ __global__ void k_advance(GridCounters* ctr, int after_seed, int slot) {
 }
 
 // Blocks left at the last level get level = MAXLEVEL (BT/Grid.h:503-504).
-__global__ void k_finalize(LatticeView L, const uint32_t* check,
-                           GridCounters* ctr) {
-  const uint32_t n = *(volatile uint32_t*)&ctr->n_check;
+__global__ void k_finalize(const GridDesc* __restrict__ D, int cur) {
+  const GridDesc& d = D[blockIdx.y];
+  const uint32_t n = *(volatile uint32_t*)&d.ctr->n_check;
+  const uint32_t* check = d.list[cur];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n;
        t += gridDim.x * blockDim.x)
-    L.blevel[check[t]] = (int8_t)L.maxlevel;
+    d.L.blevel[check[t]] = (int8_t)d.L.maxlevel;
 }
 
 // ------------------------------------------------------------ T-vertex fix
@@ -445,7 +526,24 @@ __device__ bool fix_edge(const TfixArgs& A, const Edge& E) {
   return changed;
 }
 
-__global__ void k_tfix_pass(TfixArgs A) {
+__device__ __forceinline__ TfixArgs tfix_args(const GridDesc& d, int level, int pass,
+                                              int lo, int hi_slot) {
+  TfixArgs A;
+  A.L = d.L;
+  A.level = level;
+  A.pass = pass;
+  A.leaves = d.leaves;
+  A.lo = lo;
+  A.hi_slot = hi_slot;
+  A.Xcur = d.X[pass & 1];
+  A.Xprev = d.X[(pass - 1) & 1];
+  A.ctr = d.ctr;
+  return A;
+}
+
+__global__ void k_tfix_pass(const GridDesc* __restrict__ D, int level, int pass, int lo_slot,
+                            int hi_slot) {
+  const TfixArgs A = tfix_args(D[blockIdx.y], level, pass, lo_slot, hi_slot);
   GridCounters* ctr = A.ctr;
   if (A.pass > 1 && *(volatile uint32_t*)&ctr->tfix_flags[A.pass - 1] == 0)
     return;  // converged already
@@ -473,16 +571,21 @@ __global__ void k_tfix_pass(TfixArgs A) {
     atomicOr(&ctr->tfix_flags[A.pass], 1u);
 }
 
-// Copies the converged values of a level's T-vertices into the lattice.
-__global__ void k_tfix_commit(TfixArgs A) {
-  GridCounters* ctr = A.ctr;
-  const uint32_t lo = ctr->leaf_off[A.lo], hi = ctr->leaf_off[A.hi_slot];
-  const LatticeView& L = A.L;
+// Copies the converged values of a level's T-vertices into the lattice (the
+// last pass wrote X[0]; passes skipped after convergence left both buffers
+// equal on every written vertex).
+__global__ void k_tfix_commit(const GridDesc* __restrict__ D, int level, int lo_slot,
+                              int hi_slot) {
+  const GridDesc& d = D[blockIdx.y];
+  GridCounters* ctr = d.ctr;
+  const uint32_t lo = ctr->leaf_off[lo_slot], hi = ctr->leaf_off[hi_slot];
+  const LatticeView L = d.L;
+  const double2* X = d.X[0];
   const uint32_t M = L.M;
-  const uint32_t g = pow2u(L.maxlevel - A.level);
+  const uint32_t g = pow2u(L.maxlevel - level);
   for (uint32_t t = lo + blockIdx.x * blockDim.x + threadIdx.x; t < hi;
        t += gridDim.x * blockDim.x) {
-    const uint32_t key = A.leaves[t];
+    const uint32_t key = d.leaves[t];
     const uint32_t i = key / M, j = key % M;
     if (L.thphi[key].y < 0) continue;
     const uint32_t k = i + g, l = (j + g) % M;
@@ -492,12 +595,15 @@ __global__ void k_tfix_commit(TfixArgs A) {
       for (uint32_t o = 1; o < g; o++) {
         const uint32_t ip = si[e] + ud[e] * o, jp = sj[e] + (1 - ud[e]) * o;
         const size_t id = (size_t)ip * M + jp;
-        if (L.vflag[id] == 1) L.thphi[id] = A.Xcur[id];
+        if (L.vflag[id] == 1) L.thphi[id] = X[id];
       }
   }
 }
 
-__global__ void k_tfix_check(GridCounters* ctr, int passes) {
+__global__ void k_tfix_check(const GridDesc* __restrict__ D, int G, int passes) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= G) return;
+  GridCounters* ctr = D[g].ctr;
   bool conv = false;
   for (int t = 2; t <= passes; t++)
     if (ctr->tfix_flags[t] == 0) conv = true;
@@ -577,19 +683,40 @@ __global__ void k_row_count(const uint8_t* __restrict__ vflag, const int8_t* __r
   }
 }
 
-// Exclusive scan of N row counts in one block (N <= 16385 rows).
+// Exclusive scan of N row counts in one block: each thread scans a
+// contiguous chunk, the chunk totals are scanned in shared memory.
 __global__ void k_row_scan(uint32_t* vcount, uint32_t* bcount, int N, uint64_t* totals) {
-  if (threadIdx.x != 0) return;
-  uint64_t sv = 0, sb = 0;
-  for (int i = 0; i < N; i++) {
-    const uint32_t v = vcount[i], b = bcount[i];
-    vcount[i] = (uint32_t)sv;
-    bcount[i] = (uint32_t)sb;
-    sv += v;
-    sb += b;
+  __shared__ uint64_t sv[1024], sb[1024];
+  const int t = threadIdx.x, T = blockDim.x;
+  const int chunk = (N + T - 1) / T;
+  const int i0 = min(N, t * chunk), i1 = min(N, i0 + chunk);
+  uint64_t v = 0, b = 0;
+  for (int i = i0; i < i1; i++) {
+    v += vcount[i];
+    b += bcount[i];
   }
-  totals[0] = sv;
-  totals[1] = sb;
+  sv[t] = v;
+  sb[t] = b;
+  __syncthreads();
+  for (int o = 1; o < T; o <<= 1) {
+    const uint64_t av = t >= o ? sv[t - o] : 0, ab = t >= o ? sb[t - o] : 0;
+    __syncthreads();
+    sv[t] += av;
+    sb[t] += ab;
+    __syncthreads();
+  }
+  uint64_t pv = sv[t] - v, pb = sb[t] - b;
+  for (int i = i0; i < i1; i++) {
+    const uint32_t cv = vcount[i], cb = bcount[i];
+    vcount[i] = (uint32_t)pv;
+    bcount[i] = (uint32_t)pb;
+    pv += cv;
+    pb += cb;
+  }
+  if (t == T - 1) {
+    totals[0] = sv[t];
+    totals[1] = sb[t];
+  }
 }
 
 struct CompactOut {
@@ -666,20 +793,314 @@ static unsigned grid_blocks(size_t work, int threads) {
   return (unsigned)b;
 }
 
+// Blocks per grid of a set-wide launch (grid dimension y = the G grids),
+// so that the whole launch covers the device a few times over.
+static unsigned set_blocks(size_t work, int threads, int G) {
+  size_t b = (work + threads - 1) / threads;
+  size_t cap = ((size_t)sm_count() * 8 + G - 1) / G;
+  if (cap < 2) cap = 2;
+  if (b > cap) b = cap;
+  if (b < 1) b = 1;
+  return (unsigned)b;
+}
+
 }  // namespace bt
 
 using namespace bt;
 
-static void grid_free_buffers(bt_grid* g) {
-  void* ptrs[] = {g->L.thphi, g->L.steps, g->L.vflag, g->L.vstat, g->L.blevel,
-                  g->B.list[0], g->B.list[1], g->B.trace, g->B.leaves,
-                  g->B.X[0], g->B.X[1], g->ctr, g->mapgrid,
-                  g->rowv, g->rowb, g->totals, g->compact};
+namespace {
+
+void batch_free(bt_batch* b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  if (b->timing)
+    for (int k = 0; k < 2 * 16; k++) cudaEventDestroy(b->ev[k]);
+  for (int k = 0; k < kParamSlots; k++) {
+    if (b->Dev[k]) cudaEventDestroy(b->Dev[k]);
+    if (b->Dh[k]) cudaFreeHost(b->Dh[k]);
+  }
+  if (b->grids) {
+    for (int g = 0; g < b->G; g++) {
+      bt_grid* m = &b->grids[g];
+      void* ptrs[] = {m->mapgrid, m->rowv, m->rowb, m->totals, m->compact};
+      for (void* p : ptrs)
+        if (p) cudaFree(p);
+      if (m->totals_host) cudaFreeHost(m->totals_host);
+    }
+    delete[] b->grids;
+  }
+  void* ptrs[] = {b->thphi, b->steps, b->vflag, b->vstat, b->blevel, b->lists,
+                  b->X,     b->ctr,   b->D,     b->qoff,  b->qfetch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
-  if (g->ctr_host) cudaFreeHost(g->ctr_host);
-  if (g->totals_host) cudaFreeHost(g->totals_host);
+  if (b->ctr_host) cudaFreeHost(b->ctr_host);
+  delete b;
 }
+
+int batch_create(int maxlevel, int angle, int count, bt_batch** out) {
+  BT_ARG_CHECK(out != nullptr, "out is NULL");
+  *out = nullptr;
+  BT_ARG_CHECK(count >= 1 && count <= 65535, "set size out of [1, 65535]");
+  int32_t N, M;
+  if (int rc = bt_grid_dims(maxlevel, angle, &N, &M)) return rc;
+  bt_batch* b = new (std::nothrow) bt_batch;
+  if (!b) return BT_ERR_NOMEM;
+  std::memset(b, 0, sizeof(*b));
+  b->G = count;
+  b->N = N;
+  b->M = M;
+  b->eq = angle ? 1 : 0;
+  b->maxlevel = maxlevel;
+  b->NM = (size_t)N * M;
+  b->shape = TraceShape{128, 0};
+  b->grids = new (std::nothrow) bt_grid[count];
+  if (!b->grids) {
+    delete b;
+    return BT_ERR_NOMEM;
+  }
+  std::memset(b->grids, 0, sizeof(bt_grid) * count);
+  const size_t G = (size_t)count, NM = b->NM;
+  cudaError_t e = cudaSuccess;
+#define GALLOC(ptr, bytes) \
+  if (e == cudaSuccess) e = cudaMalloc((void**)&(ptr), (bytes));
+  GALLOC(b->thphi, G * NM * sizeof(double2));
+  GALLOC(b->steps, G * NM * sizeof(int32_t));
+  GALLOC(b->vflag, G * NM + 4);
+  GALLOC(b->vstat, G * NM);
+  GALLOC(b->blevel, G * NM);
+  GALLOC(b->lists, 4 * G * NM * sizeof(uint32_t));
+  GALLOC(b->X, 2 * G * NM * sizeof(double2));
+  GALLOC(b->ctr, G * sizeof(GridCounters));
+  GALLOC(b->D, G * sizeof(GridDesc));
+  GALLOC(b->qoff, (G + 1) * sizeof(uint32_t));
+  GALLOC(b->qfetch, sizeof(uint32_t));
+  for (size_t g = 0; g < G; g++) {
+    bt_grid* m = &b->grids[g];
+    GALLOC(m->rowv, (size_t)N * sizeof(uint32_t));
+    GALLOC(m->rowb, (size_t)N * sizeof(uint32_t));
+    GALLOC(m->totals, 2 * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&m->totals_host, 2 * sizeof(uint64_t));
+  }
+#undef GALLOC
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->ctr_host, G * sizeof(GridCounters));
+  for (int k = 0; k < kParamSlots && e == cudaSuccess; k++) {
+    e = cudaMallocHost((void**)&b->Dh[k], G * sizeof(GridDesc));
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->Dev[k], cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) {
+    set_error("grid set allocation (%d grids, N=%d M=%d) failed: %s", count, N, M,
+              cudaGetErrorString(e));
+    batch_free(b);
+    return BT_ERR_NOMEM;
+  }
+  for (size_t g = 0; g < G; g++) {
+    bt_grid* m = &b->grids[g];
+    m->set = b;
+    m->index = (int)g;
+    m->L.N = N;
+    m->L.M = M;
+    m->L.eq = b->eq;
+    m->L.maxlevel = maxlevel;
+    m->L.thphi = b->thphi + g * NM;
+    m->L.steps = b->steps + g * NM;
+    m->L.vflag = b->vflag + g * NM;
+    m->L.vstat = b->vstat + g * NM;
+    m->L.blevel = b->blevel + g * NM;
+    m->ctr = b->ctr + g;
+    m->ctr_host = b->ctr_host + g;
+  }
+  *out = b;
+  return BT_OK;
+}
+
+// Descriptor of member g for a build from `startlevel` with ray params p.
+GridDesc member_desc(bt_batch* b, int g, int startlevel, const RayParams& p) {
+  const size_t NM = b->NM, G = b->G;
+  bt_grid* m = &b->grids[g];
+  GridDesc d;
+  d.L = m->L;
+  d.L.startlevel = startlevel;
+  d.p = p;
+  d.list[0] = b->lists + (0 * G + g) * NM;
+  d.list[1] = b->lists + (1 * G + g) * NM;
+  d.trace = b->lists + (2 * G + g) * NM;
+  d.leaves = b->lists + (3 * G + g) * NM;
+  d.X[0] = b->X + (0 * G + g) * NM;
+  d.X[1] = b->X + (1 * G + g) * NM;
+  d.ctr = b->ctr + g;
+  return d;
+}
+
+// The launch sequence of one build of the whole set (no host
+// synchronisation).  Returns the number of kernels launched in *launches.
+int batch_enqueue(bt_batch* b, int startlevel, int precision, cudaStream_t s,
+                  bool timing, int* launches) {
+  const int G = b->G;
+  const size_t NM = b->NM;
+  int nk = 0;
+  BT_CUDA_TRY(cudaMemsetAsync(b->vflag, 0, G * NM + 4, s));
+  BT_CUDA_TRY(cudaMemsetAsync(b->vstat, 0, G * NM, s));
+  BT_CUDA_TRY(cudaMemsetAsync(b->steps, 0, G * NM * sizeof(int32_t), s));
+  BT_CUDA_TRY(cudaMemsetAsync(b->blevel, 0xff, G * NM, s));
+  BT_CUDA_TRY(cudaMemsetAsync(b->ctr, 0, G * sizeof(GridCounters), s));
+  b->n_ev = 0;
+  auto trace = [&]() -> int {
+    const bool t = timing && b->timing && b->n_ev + 2 <= 2 * 16;
+    k_queue<<<1, 1024, 0, s>>>(b->D, G, b->qoff, b->qfetch);
+    if (t) BT_CUDA_TRY(cudaEventRecord(b->ev[b->n_ev], s));
+    const int rc = precision == BT_PRECISION_MIXED
+                       ? launch_trace_mixed(b->D, G, b->qoff, b->qfetch, b->shape, s)
+                       : launch_trace_plain(b->D, G, b->qoff, b->qfetch, b->shape, s);
+    if (t) {
+      BT_CUDA_TRY(cudaEventRecord(b->ev[b->n_ev + 1], s));
+      b->n_ev += 2;
+    }
+    nk += 2;
+    return rc;
+  };
+  const unsigned ga = (G + 127) / 128;
+  LatticeView L0 = b->grids[0].L;
+  L0.startlevel = startlevel;
+  const SeedShape S = seed_shape(L0);
+  k_seed<<<dim3(set_blocks((size_t)(S.rows + 1) * S.cols, 256, G), G), 256, 0, s>>>(b->D, S);
+  BT_CUDA_TRY(cudaGetLastError());
+  nk++;
+  if (int rc = trace()) return rc;
+  k_pole_copy<<<dim3(set_blocks(S.cols, 256, G), G), 256, 0, s>>>(b->D);
+  k_advance<<<ga, 128, 0, s>>>(b->D, G, 1, 0);
+  BT_CUDA_TRY(cudaGetLastError());
+  nk += 2;
+  int cur = 0;
+  for (int level = startlevel; level < b->maxlevel; level++) {
+    k_refine<<<dim3(set_blocks(NM / 4, 256, G), G), 256, 0, s>>>(b->D, level, cur);
+    BT_CUDA_TRY(cudaGetLastError());
+    nk++;
+    if (int rc = trace()) return rc;
+    k_advance<<<ga, 128, 0, s>>>(b->D, G, 0, level - startlevel + 1);
+    BT_CUDA_TRY(cudaGetLastError());
+    nk++;
+    cur ^= 1;
+  }
+  k_finalize<<<dim3(set_blocks(NM / 4, 256, G), G), 256, 0, s>>>(b->D, cur);
+  BT_CUDA_TRY(cudaGetLastError());
+  nk++;
+  // T-vertex fix, level by level (coarse to fine)
+  const unsigned nb = set_blocks(NM / 16, 128, G);
+  for (int level = startlevel; level < b->maxlevel; level++) {
+    const int lo = level - startlevel, hi = level - startlevel + 1;
+    for (int pass = 1; pass <= kMaxTfixPasses; pass++)
+      k_tfix_pass<<<dim3(nb, G), 128, 0, s>>>(b->D, level, pass, lo, hi);
+    k_tfix_commit<<<dim3(nb, G), 128, 0, s>>>(b->D, level, lo, hi);
+    k_tfix_check<<<ga, 128, 0, s>>>(b->D, G, kMaxTfixPasses);
+    BT_CUDA_TRY(cudaGetLastError());
+    nk += kMaxTfixPasses + 2;
+  }
+  BT_CUDA_TRY(cudaMemcpyAsync(b->ctr_host, b->ctr, G * sizeof(GridCounters),
+                              cudaMemcpyDeviceToHost, s));
+  *launches = nk;
+  return BT_OK;
+}
+
+int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int startlevel,
+                const bt_integ_opts* o, cudaStream_t s) {
+  BT_ARG_CHECK(cams && spins, "NULL cameras or spins");
+  BT_ARG_CHECK(startlevel >= 1 && startlevel <= b->maxlevel,
+               "startlevel out of [1, maxlevel]");
+  BT_ARG_CHECK(b->maxlevel - startlevel <= 12, "maxlevel - startlevel > 12 is not supported");
+  const int G = b->G;
+  // descriptors into the next pinned staging slot, once its last copy ran
+  const int slot = b->slot;
+  b->slot = (slot + 1) % kParamSlots;
+  BT_CUDA_TRY(cudaEventSynchronize(b->Dev[slot]));
+  GridDesc* Dh = b->Dh[slot];
+  int precision = -1;
+  for (int g = 0; g < G; g++) {
+    RayParams p;
+    if (make_ray_params(&cams[g], spins[g], o, &p)) {
+      set_error("invalid camera or integrator options (grid %d)", g);
+      return BT_ERR_ARG;
+    }
+    precision = p.precision;
+    Dh[g] = member_desc(b, g, startlevel, p);
+    bt_grid* m = &b->grids[g];
+    m->params = p;
+    m->cam = cams[g];
+    m->a = spins[g];
+    m->L.startlevel = startlevel;
+    m->built = 0;
+  }
+  b->built = 0;
+  BT_CUDA_TRY(cudaMemcpyAsync(b->D, Dh, G * sizeof(GridDesc), cudaMemcpyHostToDevice, s));
+  BT_CUDA_TRY(cudaEventRecord(b->Dev[slot], s));
+  int launches = 0;
+  if (b->graph) {
+    const bool same = b->exec && b->exec_startlevel == startlevel &&
+                      b->exec_precision == precision &&
+                      b->exec_shape.threads == b->shape.threads &&
+                      b->exec_shape.blocks_per_sm == b->shape.blocks_per_sm;
+    if (!same) {
+      if (b->exec) cudaGraphExecDestroy(b->exec);
+      b->exec = nullptr;
+      if (!b->cap_stream)
+        BT_CUDA_TRY(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
+      BT_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
+      int rc = batch_enqueue(b, startlevel, precision, b->cap_stream, false, &launches);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(b->cap_stream, &graph);
+      if (rc == BT_OK && e != cudaSuccess) {
+        set_error("build capture failed: %s", cudaGetErrorString(e));
+        rc = BT_ERR_CUDA;
+      }
+      if (rc == BT_OK) {
+        const cudaError_t ie = cudaGraphInstantiate(&b->exec, graph, 0);
+        if (ie != cudaSuccess) {
+          set_error("build graph instantiation failed: %s", cudaGetErrorString(ie));
+          rc = BT_ERR_CUDA;
+          b->exec = nullptr;
+        }
+      }
+      if (graph) cudaGraphDestroy(graph);
+      if (rc) return rc;
+      b->exec_startlevel = startlevel;
+      b->exec_precision = precision;
+      b->exec_shape = b->shape;
+      b->launches = launches;
+    }
+    BT_CUDA_TRY(cudaGraphLaunch(b->exec, s));
+    b->n_ev = 0;
+  } else {
+    if (int rc = batch_enqueue(b, startlevel, precision, s, true, &launches)) return rc;
+    b->launches = launches;
+  }
+  b->startlevel = startlevel;
+  b->precision = precision;
+  b->built = 1;
+  for (int g = 0; g < G; g++) b->grids[g].built = 1;
+  return BT_OK;
+}
+
+float batch_trace_ms(const bt_batch* b) {
+  float total = 0.f;
+  for (int k = 0; k + 1 < b->n_ev; k += 2) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, b->ev[k], b->ev[k + 1]) == cudaSuccess) total += ms;
+  }
+  return total;
+}
+
+int batch_set_timing(bt_batch* b, int on) {
+  if (on && !b->timing)
+    for (int k = 0; k < 2 * 16; k++) BT_CUDA_TRY(cudaEventCreate(&b->ev[k]));
+  if (!on && b->timing) {
+    for (int k = 0; k < 2 * 16; k++) cudaEventDestroy(b->ev[k]);
+    b->n_ev = 0;
+  }
+  b->timing = on ? 1 : 0;
+  return BT_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -697,148 +1118,24 @@ int bt_grid_create(int maxlevel, int angle, bt_grid** out) {
   clear_error();
   BT_ARG_CHECK(out != nullptr, "out is NULL");
   *out = nullptr;
-  int32_t N, M;
-  int rc = bt_grid_dims(maxlevel, angle, &N, &M);
-  if (rc) return rc;
-  bt_grid* g = new (std::nothrow) bt_grid;
-  if (!g) return BT_ERR_NOMEM;
-  std::memset(g, 0, sizeof(*g));
-  g->L.N = N;
-  g->L.M = M;
-  g->L.eq = angle ? 1 : 0;
-  g->L.maxlevel = maxlevel;
-  const size_t NM = (size_t)N * M;
-  g->B.cap = NM;
-  cudaError_t e = cudaSuccess;
-#define GALLOC(ptr, bytes)                                   \
-  if (e == cudaSuccess) e = cudaMalloc((void**)&(ptr), (bytes));
-  GALLOC(g->L.thphi, NM * sizeof(double2));
-  GALLOC(g->L.steps, NM * sizeof(int32_t));
-  GALLOC(g->L.vflag, NM + 4);
-  GALLOC(g->L.vstat, NM);
-  GALLOC(g->L.blevel, NM);
-  GALLOC(g->B.list[0], NM * sizeof(uint32_t));
-  GALLOC(g->B.list[1], NM * sizeof(uint32_t));
-  GALLOC(g->B.trace, NM * sizeof(uint32_t));
-  GALLOC(g->B.leaves, NM * sizeof(uint32_t));
-  GALLOC(g->B.X[0], NM * sizeof(double2));
-  GALLOC(g->B.X[1], NM * sizeof(double2));
-  GALLOC(g->ctr, sizeof(GridCounters));
-  GALLOC(g->rowv, (size_t)N * sizeof(uint32_t));
-  GALLOC(g->rowb, (size_t)N * sizeof(uint32_t));
-  GALLOC(g->totals, 2 * sizeof(uint64_t));
-#undef GALLOC
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&g->ctr_host, sizeof(GridCounters));
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&g->totals_host, 2 * sizeof(uint64_t));
-  if (e != cudaSuccess) {
-    set_error("grid allocation (N=%d M=%d) failed: %s", N, M, cudaGetErrorString(e));
-    grid_free_buffers(g);
-    delete g;
-    return BT_ERR_NOMEM;
-  }
-  *out = g;
+  bt_batch* b = nullptr;
+  if (int rc = batch_create(maxlevel, angle, 1, &b)) return rc;
+  b->standalone = 1;
+  *out = &b->grids[0];
   return BT_OK;
 }
 
 void bt_grid_destroy(bt_grid* g) {
-  if (!g) return;
-  if (g->timing)
-    for (int k = 0; k < 2 * 16; k++) cudaEventDestroy(g->ev[k]);
-  grid_free_buffers(g);
-  delete g;
+  if (!g || !g->set->standalone) return;  // members go with their set
+  batch_free(g->set);
 }
 
 int bt_grid_build(bt_grid* g, const bt_camera* cam, double a, int startlevel,
                   const bt_integ_opts* o, void* stream) {
   clear_error();
   BT_ARG_CHECK(g && cam, "NULL pointer");
-  BT_ARG_CHECK(startlevel >= 1 && startlevel <= g->L.maxlevel,
-               "startlevel out of [1, maxlevel]");
-  BT_ARG_CHECK(g->L.maxlevel - startlevel <= 12,
-               "maxlevel - startlevel > 12 is not supported");
-  RayParams p;
-  if (make_ray_params(cam, a, o, &p)) {
-    set_error("invalid camera or integrator options");
-    return BT_ERR_ARG;
-  }
-  cudaStream_t s = (cudaStream_t)stream;
-  g->params = p;
-  g->cam = *cam;
-  g->a = a;
-  g->L.startlevel = startlevel;
-  g->built = 0;
-  LatticeView L = g->L;
-  const size_t NM = (size_t)L.N * L.M;
-  BT_CUDA_TRY(cudaMemsetAsync(L.vflag, 0, NM + 4, s));
-  BT_CUDA_TRY(cudaMemsetAsync(L.vstat, 0, NM, s));
-  BT_CUDA_TRY(cudaMemsetAsync(L.steps, 0, NM * sizeof(int32_t), s));
-  BT_CUDA_TRY(cudaMemsetAsync(L.blevel, 0xff, NM, s));
-  BT_CUDA_TRY(cudaMemsetAsync(g->ctr, 0, sizeof(GridCounters), s));
-  g->n_ev = 0;
-  auto trace = [&]() -> int {
-    const bool t = g->timing && g->n_ev + 2 <= 2 * 16;
-    if (t) BT_CUDA_TRY(cudaEventRecord(g->ev[g->n_ev], s));
-    const int rc = p.precision == BT_PRECISION_MIXED
-                       ? launch_trace_mixed(p, L, g->B.trace, g->ctr, s)
-                       : launch_trace_plain(p, L, g->B.trace, g->ctr, s);
-    if (t) {
-      BT_CUDA_TRY(cudaEventRecord(g->ev[g->n_ev + 1], s));
-      g->n_ev += 2;
-    }
-    return rc;
-  };
-  const SeedShape S = seed_shape(L);
-  k_seed<<<grid_blocks((size_t)(S.rows + 1) * S.cols, 256), 256, 0, s>>>(
-      L, S, g->B.trace, g->B.list[0], g->ctr);
-  BT_CUDA_TRY(cudaGetLastError());
-  if (int rc = trace()) return rc;
-  k_pole_copy<<<grid_blocks(S.cols, 256), 256, 0, s>>>(L);
-  k_advance<<<1, 1, 0, s>>>(g->ctr, 1, 0);
-  BT_CUDA_TRY(cudaGetLastError());
-  int cur = 0;
-  for (int level = startlevel; level < L.maxlevel; level++) {
-    k_refine<<<grid_blocks(NM / 4, 256), 256, 0, s>>>(
-        L, level, g->B.list[cur], g->B.list[cur ^ 1], g->B.trace, g->B.leaves,
-        g->ctr);
-    BT_CUDA_TRY(cudaGetLastError());
-    if (int rc = trace()) return rc;
-    k_advance<<<1, 1, 0, s>>>(g->ctr, 0, level - startlevel + 1);
-    BT_CUDA_TRY(cudaGetLastError());
-    cur ^= 1;
-  }
-  k_finalize<<<grid_blocks(NM / 4, 256), 256, 0, s>>>(L, g->B.list[cur], g->ctr);
-  BT_CUDA_TRY(cudaGetLastError());
-  // T-vertex fix, level by level (coarse to fine)
-  for (int level = startlevel; level < L.maxlevel; level++) {
-    TfixArgs A;
-    A.L = L;
-    A.level = level;
-    A.leaves = g->B.leaves;
-    A.lo = level - startlevel;
-    A.hi_slot = level - startlevel + 1;
-    A.ctr = g->ctr;
-    const unsigned nb = grid_blocks(NM / 16, 128);
-    for (int pass = 1; pass <= kMaxTfixPasses; pass++) {
-      A.pass = pass;
-      A.Xcur = g->B.X[pass & 1];
-      A.Xprev = g->B.X[(pass - 1) & 1];
-      k_tfix_pass<<<nb, 128, 0, s>>>(A);
-      BT_CUDA_TRY(cudaGetLastError());
-    }
-    A.Xcur = g->B.X[0];
-    k_tfix_commit<<<nb, 128, 0, s>>>(A);
-    k_tfix_check<<<1, 1, 0, s>>>(g->ctr, kMaxTfixPasses);
-    BT_CUDA_TRY(cudaGetLastError());
-  }
-  BT_CUDA_TRY(cudaMemcpyAsync(g->ctr_host, g->ctr, sizeof(GridCounters),
-                              cudaMemcpyDeviceToHost, s));
-  // seed, pole copy, finalize; per level: refine + trace + advance (the
-  // start level adds one trace and one advance); per fixed level: passes,
-  // commit, check
-  const int nlev = L.maxlevel - startlevel;
-  g->launches = 3 + 3 * nlev + 2 + nlev * (kMaxTfixPasses + 2);
-  g->built = 1;
-  return BT_OK;
+  BT_ARG_CHECK(g->set->standalone, "the grid belongs to a set: build the set (bt_batch_build)");
+  return batch_build(g->set, cam, &a, startlevel, o, (cudaStream_t)stream);
 }
 
 int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream) {
@@ -861,19 +1158,25 @@ int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream) {
   info->exists = g->L.vflag;
   info->blevel = g->L.blevel;
   info->status = g->L.vstat;
-  info->launches = g->launches;
-  info->trace_ms = 0.f;
-  info->trace_launches = g->n_ev / 2;
-  for (int k = 0; k + 1 < g->n_ev; k += 2) {
-    float ms = 0.f;
-    if (cudaEventElapsedTime(&ms, g->ev[k], g->ev[k + 1]) == cudaSuccess)
-      info->trace_ms += ms;
-  }
+  info->launches = g->set->launches;
+  info->trace_ms = batch_trace_ms(g->set);
+  info->trace_launches = g->set->n_ev / 2;
   if (info->flags) {
     set_error("grid build flags 0x%x (1: T-vertex fix did not converge, "
               "2: fix stack overflow, 4: work list overflow)", info->flags);
     return BT_ERR_NUMERIC;
   }
+  return BT_OK;
+}
+
+int bt_grid_set_timing(bt_grid* g, int on) {
+  BT_ARG_CHECK(g != nullptr, "NULL grid");
+  return batch_set_timing(g->set, on);
+}
+
+int bt_grid_set_graph(bt_grid* g, int on) {
+  BT_ARG_CHECK(g != nullptr, "NULL grid");
+  g->set->graph = on ? 1 : 0;
   return BT_OK;
 }
 
@@ -890,15 +1193,6 @@ int bt_grid_export_dense(const bt_grid* g, double* theta, double* phi,
   return BT_OK;
 }
 
-int bt_grid_set_timing(bt_grid* g, int on) {
-  BT_ARG_CHECK(g != nullptr, "NULL grid");
-  if (on && !g->timing)
-    for (int k = 0; k < 2 * 16; k++) BT_CUDA_TRY(cudaEventCreate(&g->ev[k]));
-  g->timing = on ? 1 : g->timing;
-  if (!on) g->timing = 0;
-  return BT_OK;
-}
-
 int bt_grid_export(bt_grid* g, bt_grid_export_t* out, void* stream) {
   clear_error();
   BT_ARG_CHECK(g && out, "NULL pointer");
@@ -906,7 +1200,7 @@ int bt_grid_export(bt_grid* g, bt_grid_export_t* out, void* stream) {
   cudaStream_t s = (cudaStream_t)stream;
   const int N = g->L.N;
   k_row_count<<<N, 256, 0, s>>>(g->L.vflag, g->L.blevel, g->L.M, g->rowv, g->rowb);
-  k_row_scan<<<1, 32, 0, s>>>(g->rowv, g->rowb, N, g->totals);
+  k_row_scan<<<1, 1024, 0, s>>>(g->rowv, g->rowb, N, g->totals);
   BT_CUDA_TRY(cudaGetLastError());
   BT_CUDA_TRY(cudaMemcpyAsync(g->totals_host, g->totals, 2 * sizeof(uint64_t),
                               cudaMemcpyDeviceToHost, s));
@@ -979,6 +1273,124 @@ int bt_grid_map_export(bt_grid* g, const float** grid_out, int32_t* rows,
   if (rows) *rows = GN1;
   if (cols) *cols = GM;
   if (sym) *sym = symv;
+  return BT_OK;
+}
+
+
+int bt_batch_create(int maxlevel, int angle, int count, bt_batch** out) {
+  clear_error();
+  return batch_create(maxlevel, angle, count, out);
+}
+
+void bt_batch_destroy(bt_batch* b) {
+  if (b && !b->standalone) batch_free(b);
+}
+
+int bt_batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int startlevel,
+                   const bt_integ_opts* o, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(b != nullptr, "NULL set");
+  return batch_build(b, cams, spins, startlevel, o, (cudaStream_t)stream);
+}
+
+bt_grid* bt_batch_grid(bt_batch* b, int k) {
+  if (!b || k < 0 || k >= b->G) return nullptr;
+  return &b->grids[k];
+}
+
+int bt_batch_set_graph(bt_batch* b, int on) {
+  BT_ARG_CHECK(b != nullptr, "NULL set");
+  b->graph = on ? 1 : 0;
+  return BT_OK;
+}
+
+int bt_batch_set_timing(bt_batch* b, int on) {
+  BT_ARG_CHECK(b != nullptr, "NULL set");
+  return batch_set_timing(b, on);
+}
+
+int bt_batch_set_shape(bt_batch* b, const bt_trace_shape* shape) {
+  clear_error();
+  BT_ARG_CHECK(b && shape, "NULL pointer");
+  BT_ARG_CHECK(shape->threads == 64 || shape->threads == 128 || shape->threads == 256,
+               "threads must be 64, 128 or 256");
+  BT_ARG_CHECK(shape->blocks_per_sm >= 0 && shape->blocks_per_sm <= 32,
+               "blocks_per_sm out of [0, 32]");
+  b->shape = TraceShape{shape->threads, shape->blocks_per_sm};
+  return BT_OK;
+}
+
+int bt_batch_query(bt_batch* b, bt_batch_info* info, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(b && info, "NULL pointer");
+  BT_ARG_CHECK(b->built, "set not built");
+  BT_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  std::memset(info, 0, sizeof(*info));
+  info->count = b->G;
+  for (int g = 0; g < b->G; g++) {
+    const GridCounters& c = b->ctr_host[g];
+    info->traced += ((int64_t)c.traced_hi << 32) | c.traced_lo;
+    info->flags |= c.err | (c.overflow ? 4u : 0u);
+  }
+  info->trace_ms = batch_trace_ms(b);
+  info->trace_launches = b->n_ev / 2;
+  info->launches = b->launches;
+  info->graph = b->graph;
+  info->shape.threads = b->shape.threads;
+  info->shape.blocks_per_sm = b->shape.blocks_per_sm;
+  if (info->flags) {
+    set_error("grid set build flags 0x%x", info->flags);
+    return BT_ERR_NUMERIC;
+  }
+  return BT_OK;
+}
+
+int bt_batch_autotune(bt_batch* b, const bt_camera* cams, const double* spins, int startlevel,
+                      const bt_integ_opts* o, int repeats, bt_trace_shape* best,
+                      float* best_ms, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(b != nullptr, "NULL set");
+  BT_ARG_CHECK(repeats >= 1 && repeats <= 100, "repeats out of [1, 100]");
+  cudaStream_t s = (cudaStream_t)stream;
+  const TraceShape saved = b->shape;
+  const int graph = b->graph;
+  b->graph = 0;  // time eager builds; the chosen shape is captured later
+  static const TraceShape cand[] = {{128, 0}, {128, 4}, {128, 5}, {64, 0}, {256, 0}};
+  cudaEvent_t e0, e1;
+  BT_CUDA_TRY(cudaEventCreate(&e0));
+  BT_CUDA_TRY(cudaEventCreate(&e1));
+  float best_t = 3.4e38f;
+  TraceShape best_s = saved;
+  int rc = BT_OK;
+  for (const TraceShape& c : cand) {
+    b->shape = c;
+    if ((rc = batch_build(b, cams, spins, startlevel, o, s))) break;  // warm-up
+    float t_min = 3.4e38f;
+    for (int r = 0; r < repeats && rc == BT_OK; r++) {
+      cudaEventRecord(e0, s);
+      rc = batch_build(b, cams, spins, startlevel, o, s);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = BT_ERR_CUDA;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < t_min) t_min = ms;
+    }
+    if (rc) break;
+    if (t_min < best_t) {
+      best_t = t_min;
+      best_s = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->graph = graph;
+  b->shape = rc == BT_OK ? best_s : saved;
+  if (rc) return rc;
+  if (best) {
+    best->threads = best_s.threads;
+    best->blocks_per_sm = best_s.blocks_per_sm;
+  }
+  if (best_ms) *best_ms = best_t;
   return BT_OK;
 }
 

@@ -42,11 +42,21 @@ __device__ __forceinline__ double sqd(double x) { return x * x; }
 // reference's association: Delta = (r^2 - 2r) + a^2, rho^2 = r^2 + a^2 cos^2,
 // P = (r^2 + a^2) - a b, R = P^2 - Delta((b-a)^2 + q),
 // Theta = q - cos^2 (b^2/sin^2 - a^2).
-__device__ __forceinline__ void eom(const double* y, double* f, double b,
-                                    double q, double a, double asq) {
-  const double r = y[0], pr = y[3], pt = y[4];
+//
+// Kept out of line: an attempt evaluates it five times (and the step start
+// once more), and each evaluation holds about sixteen IEEE divisions and a
+// sincos, so inlining every call site makes the ray loop larger than the
+// instruction cache.  One copy, called six times, keeps it resident; the
+// arithmetic is the same either way.
+struct Slope {
+  double f0, f1, f2, f3, f4;
+};
+
+static __device__ __noinline__ Slope eom_call(double r, double th, double pr, double pt,
+                                       double b, double q, double a, double asq) {
+  double f[5];
   double sinv, cosv;
-  sincos(y[1], &sinv, &cosv);
+  sincos(th, &sinv, &cosv);
   const double cossq = sqd(cosv);
   const double sinsq = sqd(sinv);
   const double bsq = sqd(b);
@@ -76,6 +86,17 @@ __device__ __forceinline__ void eom(const double* y, double* f, double b,
              (rosq * 2 * delta) -
          (4 * acs * ptsq) / rosqsq - (4 * acs * prsq * delta) / rosqsq +
          (acs * (bth * delta + R)) / sqrosqdel;
+  return Slope{f[0], f[1], f[2], f[3], f[4]};
+}
+
+__device__ __forceinline__ void eom(const double* y, double* f, double b,
+                                    double q, double a, double asq) {
+  const Slope s = eom_call(y[0], y[1], y[3], y[4], b, q, a, asq);
+  f[0] = s.f0;
+  f[1] = s.f1;
+  f[2] = s.f2;
+  f[3] = s.f3;
+  f[4] = s.f4;
 }
 
 // One Cash-Karp attempt (BT/Metric.h:228-251).  Stage slopes k1..k5 are

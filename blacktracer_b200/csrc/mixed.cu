@@ -59,18 +59,9 @@ int launch_integrate_mixed(const RayParams& p, const double* th,
   return BT_OK;
 }
 
-int launch_trace_mixed(const RayParams& p, const LatticeView& L,
-                       const uint32_t* keys, GridCounters* ctr,
-                       cudaStream_t s) {
-  static int per_sm = 0;
-  if (!per_sm) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, k_trace_lattice<MixedPolicy>, 128, 0);
-    if (per_sm < 1) per_sm = 1;
-  }
-  k_trace_lattice<MixedPolicy><<<sm_count() * per_sm, 128, 0, s>>>(p, L, keys, ctr);
-  BT_CUDA_TRY(cudaGetLastError());
-  return BT_OK;
+int launch_trace_mixed(const GridDesc* D, int G, const uint32_t* qoff,
+                       uint32_t* qfetch, TraceShape shape, cudaStream_t s) {
+  return launch_trace_shape<MixedPolicy>(D, G, qoff, qfetch, shape, s);
 }
 
 }  // namespace bt

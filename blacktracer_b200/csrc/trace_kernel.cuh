@@ -25,16 +25,32 @@ __device__ __forceinline__ void lattice_seed(const LatticeView& L, uint32_t key,
   ph = (double)j / L.M * kPi2;
 }
 
-// Traces lattice vertices keys[0 .. ctr->n_trace) into the lattice.
-template <class Policy>
-__global__ void __launch_bounds__(128)
-k_trace_lattice(const RayParams p, const LatticeView L,
-                const uint32_t* __restrict__ keys, GridCounters* ctr) {
-  const uint32_t n = *(volatile uint32_t*)&ctr->n_trace;
+// Grid of queue entry k: the last g with qoff[g] <= k (empty grids have
+// qoff[g] == qoff[g + 1] and are never chosen).
+__device__ __forceinline__ int queue_grid(const uint32_t* __restrict__ qoff, int G,
+                                          uint32_t k) {
+  int lo = 0, hi = G - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (qoff[mid] <= k) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Traces the listed vertices of G grids into their lattices.  Queue entry k
+// is vertex trace[k - qoff[g]] of grid g; each grid's rays use that grid's
+// camera and spin (D[g].p).
+template <class Policy, int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+k_trace_lattice(const GridDesc* __restrict__ D, int G,
+                const uint32_t* __restrict__ qoff, uint32_t* qfetch) {
+  const uint32_t n = qoff[G];
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
   uint32_t slot = kLaneIdle;
   uint32_t key = 0;
+  int g = 0;
   typename Policy::State st;
   for (;;) {
     const bool need = slot == kLaneIdle;
@@ -42,23 +58,25 @@ k_trace_lattice(const RayParams p, const LatticeView L,
     if (m) {
       const int leader = __ffs(m) - 1;
       uint32_t base = 0;
-      if ((int)lane == leader) base = atomicAdd(&ctr->fetch, (uint32_t)__popc(m));
+      if ((int)lane == leader) base = atomicAdd(qfetch, (uint32_t)__popc(m));
       base = __shfl_sync(0xffffffffu, base, leader);
       if (need) {
         const uint32_t k = base + (uint32_t)__popc(m & lt_mask);
         if (k < n) {
-          key = keys[k];
+          g = queue_grid(qoff, G, k);
+          const GridDesc& d = D[g];
+          key = d.trace[k - qoff[g]];
           double th, ph, to, po;
           int32_t s;
           uint8_t ss;
-          lattice_seed(L, key, th, ph);
-          if (Policy::begin(p, th, ph, st, to, po, s, ss)) {
+          lattice_seed(d.L, key, th, ph);
+          if (Policy::begin(d.p, th, ph, st, to, po, s, ss)) {
             slot = k;
           } else {
-            L.thphi[key] = make_double2(to, po);
-            L.steps[key] = s;
-            L.vstat[key] = ss;
-            L.vflag[key] = 1;
+            d.L.thphi[key] = make_double2(to, po);
+            d.L.steps[key] = s;
+            d.L.vstat[key] = ss;
+            d.L.vflag[key] = 1;
           }
         } else {
           slot = kLaneDone;
@@ -67,18 +85,53 @@ k_trace_lattice(const RayParams p, const LatticeView L,
     }
     if (__all_sync(0xffffffffu, slot == kLaneDone)) break;
     if (slot < kLaneDone) {
-      if (Policy::attempt(p, st)) {
+      const GridDesc& d = D[g];
+      if (Policy::attempt(d.p, st)) {
         double to, po;
         int32_t s;
         uint8_t ss;
-        Policy::finish(p, st, to, po, s, ss);
-        L.thphi[key] = make_double2(to, po);
-        L.steps[key] = s;
-        L.vstat[key] = ss;
-        L.vflag[key] = 1;
+        Policy::finish(d.p, st, to, po, s, ss);
+        d.L.thphi[key] = make_double2(to, po);
+        d.L.steps[key] = s;
+        d.L.vstat[key] = ss;
+        d.L.vflag[key] = 1;
         slot = kLaneIdle;
       }
     }
+  }
+}
+
+// Launch of k_trace_lattice: one block per SM times the requested (or the
+// largest resident) number of blocks.  128-thread blocks come in three
+// register budgets -- as compiled (3 blocks per SM), capped for 4 and for 5
+// resident blocks (with a few spills) -- picked by blocks_per_sm 0-3, 4, 5+.
+template <class Policy>
+int launch_trace_shape(const GridDesc* D, int G, const uint32_t* qoff,
+                       uint32_t* qfetch, TraceShape shape, cudaStream_t s) {
+  static int resident[5] = {0, 0, 0, 0, 0};  // per variant, for this Policy
+  auto go = [&](auto kernel, int threads, int variant) -> int {
+    int& per_sm_max = resident[variant];
+    if (!per_sm_max) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_max, kernel, threads, 0);
+      if (per_sm_max < 1) per_sm_max = 1;
+    }
+    int per_sm = per_sm_max;
+    if (shape.blocks_per_sm > 0 && shape.blocks_per_sm < per_sm) per_sm = shape.blocks_per_sm;
+    kernel<<<sm_count() * per_sm, threads, 0, s>>>(D, G, qoff, qfetch);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      set_error("trace launch: %s", cudaGetErrorString(e));
+      return BT_ERR_CUDA;
+    }
+    return BT_OK;
+  };
+  switch (shape.threads) {
+    case 64: return go(k_trace_lattice<Policy, 64, 1>, 64, 0);
+    case 256: return go(k_trace_lattice<Policy, 256, 1>, 256, 1);
+    default:
+      if (shape.blocks_per_sm >= 5) return go(k_trace_lattice<Policy, 128, 5>, 128, 4);
+      if (shape.blocks_per_sm == 4) return go(k_trace_lattice<Policy, 128, 4>, 128, 3);
+      return go(k_trace_lattice<Policy, 128, 1>, 128, 2);
   }
 }
 

@@ -234,6 +234,10 @@ class Grid:
         """Record CUDA events around the ray-tracing launches (info().trace_ms)."""
         L.check(L.lib().bt_grid_set_timing(self._h, 1 if on else 0))
 
+    def set_graph(self, on=True):
+        """Capture later builds once into a CUDA graph and replay it."""
+        L.check(L.lib().bt_grid_set_graph(self._h, 1 if on else 0))
+
     def export(self, out=None, pinned=True):
         """The grid as key-ordered lists (CamToCel, steps, blockLevels).
 
@@ -298,6 +302,98 @@ class Grid:
         if h is not None and getattr(self, "_own", False):
             try:
                 L.lib().bt_grid_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
+class GridSet:
+    """A set of grids of one size built together (bt_batch): grid k for
+    cameras[k] and spins[k].  The reference builds its grids one by one
+    (BT/BlackTracer.cpp:220-262); here all levels of all grids share launches
+    and one persistent ray-tracing queue.  ``grids[k]`` are Grid views of the
+    members (query, export and map as any Grid; released with the set)."""
+
+    def __init__(self, maxLevelPrec: int, startLevel: int, angle: bool, count: int,
+                 opts=None, stream=None):
+        self.MAXLEVEL = int(maxLevelPrec)
+        self.STARTLVL = int(startLevel)
+        self.equafactor = 1 if angle else 0
+        self.count = int(count)
+        self.opts = _opts(opts)
+        self._stream = stream
+        h = C.c_void_p()
+        L.check(L.lib().bt_batch_create(self.MAXLEVEL, self.equafactor, self.count,
+                                        C.byref(h)))
+        self._h = h
+        N, M = grid_dims(self.MAXLEVEL, angle)
+        sN, sM = grid_dims(self.STARTLVL, angle)
+        self.grids = []
+        for k in range(self.count):
+            g = Grid.__new__(Grid)
+            g.MAXLEVEL, g.STARTLVL, g.equafactor = self.MAXLEVEL, self.STARTLVL, self.equafactor
+            g.N, g.M, g.STARTN, g.STARTM = N, M, sN, sM
+            g.cam, g.a, g.opts, g._stream = None, None, self.opts, stream
+            g._own, g._info, g._map, g._set = False, None, None, self
+            g._h = C.c_void_p(L.lib().bt_batch_grid(h, k))
+            self.grids.append(g)
+        self._info = None
+
+    def _arrays(self, cameras, spins):
+        if len(cameras) != self.count or len(spins) != self.count:
+            raise ValueError(f"need {self.count} cameras and spins")
+        cams = (L.bt_camera * self.count)(*[c._c for c in cameras])
+        a = (C.c_double * self.count)(*[float(x) for x in spins])
+        return cams, a
+
+    def build(self, cameras, spins):
+        cams, a = self._arrays(cameras, spins)
+        L.check(L.lib().bt_batch_build(self._h, cams, a, self.STARTLVL, self.opts.ref,
+                                       _stream_ptr(self._stream)))
+        for g, c, s in zip(self.grids, cameras, spins):
+            g.cam, g.a, g._info, g._map = c, float(s), None, None
+        self._info = None
+
+    def info(self) -> L.bt_batch_info:
+        if self._info is None:
+            inf = L.bt_batch_info()
+            L.check(L.lib().bt_batch_query(self._h, C.byref(inf), _stream_ptr(self._stream)))
+            self._info = inf
+        return self._info
+
+    @property
+    def traced(self) -> int:
+        return int(self.info().traced)
+
+    def set_graph(self, on=True):
+        L.check(L.lib().bt_batch_set_graph(self._h, 1 if on else 0))
+
+    def set_timing(self, on=True):
+        L.check(L.lib().bt_batch_set_timing(self._h, 1 if on else 0))
+
+    def set_shape(self, threads=128, blocks_per_sm=0):
+        s = L.bt_trace_shape(threads, blocks_per_sm)
+        L.check(L.lib().bt_batch_set_shape(self._h, C.byref(s)))
+
+    def autotune(self, cameras, spins, repeats=2):
+        """Times the candidate trace launch shapes on these cameras, keeps
+        the fastest; returns ((threads, blocks_per_sm), ms per build)."""
+        cams, a = self._arrays(cameras, spins)
+        best = L.bt_trace_shape()
+        ms = C.c_float()
+        L.check(L.lib().bt_batch_autotune(self._h, cams, a, self.STARTLVL, self.opts.ref,
+                                          int(repeats), C.byref(best), C.byref(ms),
+                                          _stream_ptr(self._stream)))
+        for g in self.grids:
+            g._info, g._map = None, None
+        self._info = None
+        return (best.threads, best.blocks_per_sm), ms.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None:
+            try:
+                L.lib().bt_batch_destroy(h)
             except Exception:
                 pass
             self._h = None

@@ -169,8 +169,13 @@ typedef struct bt_grid_info {
 } bt_grid_info;
 
 /* Records CUDA events around the ray-tracing launches of later builds
- * (reported by bt_grid_query as trace_ms). */
+ * (reported by bt_grid_query as trace_ms; eager builds only). */
 int bt_grid_set_timing(bt_grid* g, int on);
+
+/* on = 1: later builds are captured once into a CUDA graph (per start
+ * level, precision and trace launch shape) and replayed.  No counterpart in
+ * the reference (its build is host-driven). */
+int bt_grid_set_graph(bt_grid* g, int on);
 
 /* Synchronises `stream` and reports the build.  Returns BT_ERR_NUMERIC when
  * a bounded loop (T-vertex fixed point) gave up. */
@@ -213,6 +218,61 @@ int bt_grid_export(bt_grid* g, bt_grid_export_t* out, void* stream);
  * (rows = 2N-1).  Returns a device pointer owned by the grid. */
 int bt_grid_map_export(bt_grid* g, const float** grid_out, int32_t* rows,
                        int32_t* cols, int32_t* sym, void* stream);
+
+/* ------------------------------------------------------------ grid sets */
+
+/* A set of `count` grids of the same (maxlevel, angle), each built for its
+ * own camera and spin, together: the reference builds its grids one after
+ * the other (BT/BlackTracer.cpp:220-262, one Grid per camera of `cams`);
+ * here every level of all grids is refined by one launch and traced by one
+ * persistent launch with a shared work queue, so the long rays of one grid
+ * overlap the work of the others.  Members are bt_grid handles for
+ * bt_grid_query / export / map_export; they are released with the set
+ * (bt_grid_destroy on a member does nothing, bt_grid_build on a member
+ * returns BT_ERR_ARG).  Builds of one set must be ordered on one stream. */
+typedef struct bt_batch bt_batch;
+
+int bt_batch_create(int maxlevel, int angle, int count, bt_batch** out);
+void bt_batch_destroy(bt_batch* b);
+
+/* Builds all grids: grid k from cams[k] with spin spins[k] (count each),
+ * from `startlevel`, options o for all.  Asynchronous on `stream`. */
+int bt_batch_build(bt_batch* b, const bt_camera* cams, const double* spins,
+                   int startlevel, const bt_integ_opts* o, void* stream);
+
+/* Member k (0 <= k < count), or NULL. */
+bt_grid* bt_batch_grid(bt_batch* b, int k);
+
+/* As bt_grid_set_graph / bt_grid_set_timing, for the whole set. */
+int bt_batch_set_graph(bt_batch* b, int on);
+int bt_batch_set_timing(bt_batch* b, int on);
+
+/* Launch shape of the persistent ray-tracing kernel: threads per block
+ * (64, 128 or 256) and resident blocks per SM (0 = as many as fit). */
+typedef struct bt_trace_shape {
+  int32_t threads;
+  int32_t blocks_per_sm;
+} bt_trace_shape;
+int bt_batch_set_shape(bt_batch* b, const bt_trace_shape* shape);
+
+typedef struct bt_batch_info {
+  int32_t count;
+  int64_t traced;          /* rays integrated by the last build, all grids */
+  uint32_t flags;          /* OR of the members' flags                     */
+  float trace_ms;          /* with timing on, eager builds                 */
+  int32_t trace_launches;
+  int32_t launches;        /* kernels per build                            */
+  int32_t graph;           /* builds replay a CUDA graph                   */
+  bt_trace_shape shape;
+} bt_batch_info;
+int bt_batch_query(bt_batch* b, bt_batch_info* info, void* stream);
+
+/* Autotuner: times `repeats` builds of these cameras for each candidate
+ * trace launch shape, keeps the fastest in the set and reports it (best,
+ * best_ms may be NULL).  Synchronises `stream`. */
+int bt_batch_autotune(bt_batch* b, const bt_camera* cams, const double* spins,
+                      int startlevel, const bt_integ_opts* o, int repeats,
+                      bt_trace_shape* best, float* best_ms, void* stream);
 
 /* ------------------------------------------------------- per-pixel map */
 

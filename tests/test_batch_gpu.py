@@ -1,0 +1,120 @@
+"""Grid sets (bt_batch): G grids with their own cameras and spins built
+together must give, grid by grid, exactly what a lone build of the same
+camera and spin gives -- the set only shares launches and the ray queue --
+in eager mode, replayed from a CUDA graph, after the autotuner, and in the
+mixed form.  One member is also checked against the oracle."""
+import math
+
+import numpy as np
+import pytest
+
+from test_grid_gpu import compare
+
+pytestmark = pytest.mark.gpu
+
+POSES = [  # (theta, phi, r, motion, a)
+    (math.pi / 2, 0.0, 5.0, (0.0, 0.0, 1.0), 0.999),   # circular orbit
+    (1.2, 0.0, 8.0, (0.0,), 0.99),                     # static
+    (math.pi / 2, 0.0, 30.0, (0.0,), 0.6),             # static, far
+    (0.5, 0.0, 12.0, (0.0,), 0.3),                     # static, high latitude
+]
+ML, SL = 8, 5
+
+
+def cameras(bt, poses):
+    return [bt.Camera(t, p, r, *mv, a=a) for t, p, r, mv, a in poses], [p[4] for p in poses]
+
+
+def dense(g):
+    return {k: v.cpu().numpy() for k, v in g.dense().items()}
+
+
+def alone(bt, cam, a, prec="plain"):
+    g = bt.Grid(ML, SL, True, cam, opts=prec)
+    return dense(g), g.traced
+
+
+def assert_same(a, b, label):
+    for k in ("exists", "blevel", "steps", "status"):
+        assert np.array_equal(a[k], b[k]), f"{label}: {k} differs"
+    e = a["exists"] == 1
+    for k in ("theta", "phi"):
+        assert np.array_equal(a[k][e], b[k][e]), f"{label}: {k} differs"
+
+
+@pytest.mark.parametrize("prec", ["plain", "mixed"])
+def test_set_members_equal_lone_builds(bt, cuda, prec):
+    cams, spins = cameras(bt, POSES)
+    S = bt.GridSet(ML, SL, True, len(cams), opts=prec)
+    S.build(cams, spins)
+    total = 0
+    for k, (c, a) in enumerate(zip(cams, spins)):
+        ref, traced = alone(bt, c, a, prec)
+        assert_same(dense(S.grids[k]), ref, f"{prec} member {k}")
+        assert S.grids[k].traced == traced
+        total += traced
+    assert S.traced == total
+    assert S.info().flags == 0
+
+
+def test_set_member_vs_oracle(bt, cuda, oracle_mod):
+    cams, spins = cameras(bt, POSES)
+    S = bt.GridSet(ML, SL, True, len(cams))
+    S.build(cams, spins)
+    for k in (0, 3):
+        cam12 = cams[k].as_array()
+        ref = oracle_mod.grid_build(ML, SL, True, cam12, spins[k], tfix=1)
+        compare(dense(S.grids[k]), ref, f"member {k}")
+
+
+def test_set_graph_replay_equals_eager(bt, cuda):
+    cams, spins = cameras(bt, POSES)
+    eager = bt.GridSet(ML, SL, True, len(cams))
+    eager.build(cams, spins)
+    ref = [dense(g) for g in eager.grids]
+    S = bt.GridSet(ML, SL, True, len(cams))
+    S.set_graph(True)
+    order = [2, 0, 3, 1]
+    S.build([cams[k] for k in order], [spins[k] for k in order])  # captures
+    S.build(cams, spins)                                          # replays
+    assert S.info().graph == 1
+    for k in range(len(cams)):
+        assert_same(dense(S.grids[k]), ref[k], f"graph member {k}")
+    S.build([cams[k] for k in order], [spins[k] for k in order])
+    for slot, k in enumerate(order):
+        assert_same(dense(S.grids[slot]), ref[k], f"graph permuted {slot}")
+
+
+def test_autotune_keeps_results(bt, cuda):
+    cams, spins = cameras(bt, POSES)
+    S = bt.GridSet(ML, SL, True, len(cams))
+    S.build(cams, spins)
+    ref = [dense(g) for g in S.grids]
+    (threads, per_sm), ms = S.autotune(cams, spins, repeats=1)
+    assert threads in (64, 128, 256) and 0 <= per_sm <= 32 and ms > 0
+    assert (S.info().shape.threads, S.info().shape.blocks_per_sm) == (threads, per_sm)
+    S.build(cams, spins)
+    for k in range(len(cams)):
+        assert_same(dense(S.grids[k]), ref[k], f"tuned member {k}")
+
+
+def test_lone_grid_graph_replay(bt, cuda):
+    cams, spins = cameras(bt, POSES)
+    ref, _ = alone(bt, cams[1], spins[1])
+    g = bt.Grid(ML, SL, True, cams[0], opts="plain")
+    g.set_graph(True)
+    g.build(cams[1], spins[1])
+    g.build(cams[1], spins[1])
+    assert_same(dense(g), ref, "lone graph")
+
+
+def test_member_misuse(bt, cuda):
+    cams, spins = cameras(bt, POSES[:2])
+    S = bt.GridSet(ML, SL, True, 2)
+    with pytest.raises(ValueError):
+        S.build(cams[:1], spins[:1])
+    S.build(cams, spins)
+    with pytest.raises(bt.BtError):
+        S.grids[0].build(cams[0], spins[0])
+    bt.lib().bt_grid_destroy(S.grids[1]._h)  # ignored for members
+    assert S.grids[1].traced > 0
