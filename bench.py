@@ -5,11 +5,14 @@ Headline (value): geodesics/s of building the adaptive camera-sky grid of the
 "single large adaptive grid" configuration -- Kerr a/M = 0.999, camera on a
 circular equatorial orbit at r = 5M boosted at Keplerian velocity, adaptive
 refinement from level 6 (64x128) to level 11 (2048x4096 equivalent) --
-through the C ABI (bt_grid_build), plain FP64 form (the form that reproduces
-the reference integrator; the mixed form is reported beside it).  One step =
-one complete grid build (all levels + T-vertex fix).  Also reported: 4K
-frames (3840x1920 BGRA8 from an 8192x4096 environment map and 10^6 stars,
-lensing + redshift on) per second and p50/p99 frame latency.
+through the C ABI (bt_grid_build), in the fast FP64 form by default (the
+reference's method with its equations of motion reassociated: same grid
+topology, p99 ~1e-13 rad against the plain form); the plain form (the
+reference's operation order) and the FP32-bulk mixed form are reported beside
+it, each with its error against plain.  One step = one complete grid build
+(all levels + T-vertex fix).  Also reported: 4K frames (3840x1920 BGRA8 from
+an 8192x4096 environment map and 10^6 stars, lensing + redshift on) per
+second and p50/p99 frame latency, and the 64-pose batched grid set.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -40,6 +43,11 @@ F_COMBINE = 270      # the Cash-Karp stage combinations of one attempt
 F_CONTROL = 45       # scale, error norm, step-size update
 F_ATTEMPT = 6 * F_EOM + F_COMBINE + F_CONTROL
 F_SETUP = 1000       # ray set-up + capture test (Newton + golden section), approx.
+# The fast form's equations of motion (kerr_fast.cuh), counted the same way:
+# 104 flops (3 reciprocals instead of 16 divisions); FMA = 2 flops.
+F_EOM_FAST = 104
+F_ATTEMPT_FORM = {"plain": F_ATTEMPT, "mixed": F_ATTEMPT,
+                  "fast": 6 * F_EOM_FAST + F_COMBINE + F_CONTROL}
 WORKLOAD = dict(maxlevel=11, startlevel=6, a=0.999, r=5.0, theta=np.pi / 2)
 
 
@@ -240,6 +248,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--frames", type=int, default=20, help="4K frames to time (0 = skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fast", choices=["fast", "plain", "mixed"],
+                    help="integrator form of the headline value")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the 64-pose batched-grid measurement")
     args = ap.parse_args()
@@ -274,7 +284,8 @@ def main():
 
     stream = torch.cuda.current_stream()
     cam = c2_camera(bt)
-    opts = bt.IntegOpts("plain")
+    prec_main = args.precision
+    opts = bt.IntegOpts(prec_main)
     grid = bt.Grid(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam, opts=opts)
     grid.set_timing(True)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # > L2 (126 MB)
@@ -286,7 +297,8 @@ def main():
     st_all = d["steps"].to(torch.int64)
     integrated = (d["exists"] == 1) & (d["status"] != 1)
     traced = int(grid.info().traced)
-    flops_build = float(((st_all[integrated] + 1).sum().item()) * F_ATTEMPT + traced * F_SETUP)
+    flops_build = float(((st_all[integrated] + 1).sum().item()) * F_ATTEMPT_FORM[prec_main] +
+                        traced * F_SETUP)
     del d, steps, st_all, integrated
 
     for _ in range(args.warmup):
@@ -315,31 +327,47 @@ def main():
     max_ms = allmax(total_ms)
     value = traced * args.steps * world / (max_ms / 1e3)
 
-    # mixed form, same workload (reported beside the headline)
-    gm = bt.Grid(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam, opts="mixed")
-    for _ in range(3):
-        gm.build()
-    torch.cuda.synchronize()
-    t_mixed = 0.0
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        gm.build()
-        e1.record(stream)
+    # the other two forms, same workload (reported beside the headline), with
+    # their error against the plain form
+    other = {}
+    ref_dense = None
+    for prec in [p_ for p_ in ("plain", "fast", "mixed") if p_ != prec_main]:
+        gm = bt.Grid(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam, opts=prec)
+        for _ in range(3):
+            gm.build()
         torch.cuda.synchronize()
-        t_mixed += e0.elapsed_time(e1)
-    mixed_value = int(gm.info().traced) * args.steps / (t_mixed / 1e3)
-    dp = grid.dense()
-    dm = gm.dense()
-    both = (dp["exists"] == 1) & (dm["exists"] == 1) & (dp["theta"] >= 0) & (dm["theta"] >= 0)
-    dth = (dp["theta"][both] - dm["theta"][both]).abs()
-    dph = (dp["phi"][both] - dm["phi"][both] + np.pi).remainder(2 * np.pi) - np.pi
-    err = torch.maximum(dth, dph.abs())
-    mixed_p99 = float(torch.quantile(err.float().cpu(), 0.99).item()) if err.numel() else None
-    mixed_topo = bool(torch.equal(dp["exists"], dm["exists"]) and torch.equal(dp["blevel"], dm["blevel"]))
-    del dp, dm, gm
+        t_o = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            gm.build()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_o += e0.elapsed_time(e1)
+        o_value = int(gm.info().traced) * args.steps / (t_o / 1e3)
+        if prec == "plain":
+            ref_dense = gm.dense()
+        dp = ref_dense if ref_dense is not None else grid.dense()
+        dm = gm.dense() if prec != "plain" else grid.dense()
+        both = (dp["exists"] == 1) & (dm["exists"] == 1) & (dp["theta"] >= 0) & (dm["theta"] >= 0)
+        dth = (dp["theta"][both] - dm["theta"][both]).abs()
+        dph = (dp["phi"][both] - dm["phi"][both] + np.pi).remainder(2 * np.pi) - np.pi
+        err = torch.maximum(dth, dph.abs()).float().cpu()
+        other[prec] = {
+            "value": o_value, "unit": "geodesics/s",
+            "ratio_to_headline": o_value / (traced * args.steps / (total_ms / 1e3)),
+            "p99_rad_vs_plain": float(torch.quantile(err, 0.99)) if err.numel() else None,
+            "max_rad_vs_plain": float(err.max()) if err.numel() else None,
+            "topology_exact": bool(torch.equal(dp["exists"], dm["exists"]) and
+                                   torch.equal(dp["blevel"], dm["blevel"]))}
+        if prec != "plain":
+            other[prec]["error_vs"] = "plain"
+        else:
+            other[prec]["error_vs"] = prec_main + " (the headline form)"
+        del dp, dm, gm
+    del ref_dense
 
     # end to end through the C ABI with host buffers: build + compact export
     # (CamToCel / steps / blockLevels) into pinned host memory every step
@@ -369,7 +397,7 @@ def main():
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
                 "traffic": traffic_from_profiles(),
-                "kernel": "k_trace_lattice<PlainPolicy>",
+                "kernel": "k_trace_lattice<%sPolicy>" % prec_main.capitalize(),
                 "peak_source": "measured in this run: independent-chain DFMA probe "
                                "(bt_probe_fp64_tflops); MEASURED_PEAKS.json has no FP64 entry",
                 "flops_per_build": flops_build, "trace_ms_per_build": trace_ms / args.steps,
@@ -424,7 +452,7 @@ def main():
         cams_b, spins_b = batch_poses(bt)
         res = {}
         sets = {}
-        for prec in ("plain", "mixed"):
+        for prec in ("plain", "fast", "mixed"):
             Sb = bt.GridSet(BATCH["maxlevel"], BATCH["startlevel"], True, BATCH["count"],
                             opts=prec)
             shape, _ = Sb.autotune(cams_b, spins_b, repeats=1)
@@ -446,19 +474,34 @@ def main():
                          "ms_per_set": ms, "rays_per_set": rays,
                          "trace_shape": {"threads": shape[0], "blocks_per_sm": shape[1]},
                          "launches_per_set": int(Sb.info().launches)}
+            if prec != "mixed":
+                # FP64 work of the set per build over the whole build time
+                attempts = 0
+                for gq in Sb.grids:
+                    dq = gq.dense()
+                    live = (dq["exists"] == 1) & (dq["status"] != 1)
+                    attempts += int((dq["steps"][live].to(torch.int64) + 1).sum().item())
+                    del dq
+                fl = float(attempts * F_ATTEMPT_FORM[prec] + rays * F_SETUP)
+                ach = fl / (ms / 1e3) / 1e12
+                res[prec]["roofline"] = {
+                    "bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                    "frac": ach / peak if peak else None, "flops_per_set": fl,
+                    "note": "whole set build time (all kernels), FP64 peak as the headline's"}
             sets[prec] = Sb
-        p99, mx, topo = set_error_vs(sets["plain"], sets["mixed"])
-        res["mixed"].update({"p99_rad_vs_plain": p99, "max_rad_vs_plain": mx,
-                             "topology_exact": topo})
-        plain_single = traced * args.steps / (total_ms / 1e3)
+        for prec in ("fast", "mixed"):
+            p99, mx, topo = set_error_vs(sets["plain"], sets[prec])
+            res[prec].update({"p99_rad_vs_plain": p99, "max_rad_vs_plain": mx,
+                              "topology_exact": topo})
+        plain_single = (other["plain"]["value"] if prec_main != "plain"
+                        else traced * args.steps / (total_ms / 1e3))
         batched = {"workload": f"{BATCH['count']} poses, adaptive L6->L9 (512x1024 "
                                "equivalent), static cameras r in [4M,40M], theta in "
                                "[0.1, pi-0.1], a in [0, 0.999], seeded; one set per step, "
                                "CUDA graph replay, launch shape from the autotuner",
-                   "plain": res["plain"], "mixed": res["mixed"],
+                   "plain": res["plain"], "fast": res["fast"], "mixed": res["mixed"],
                    "speedup_vs_single_grid_plain": {
-                       "plain": res["plain"]["value"] / plain_single,
-                       "mixed": res["mixed"]["value"] / plain_single}}
+                       k: res[k]["value"] / plain_single for k in ("plain", "fast", "mixed")}}
         del sets, Sb
 
     # CPU baseline: the reference's own Grid constructor, one thread, full workload
@@ -482,7 +525,12 @@ def main():
             "data": "synthetic",
             "config": {"workload": "adaptive grid L6->L11 (64x128 -> 2048x4096 equivalent), "
                                    "Kerr a=0.999, camera r=5M theta=pi/2 Keplerian orbit; "
-                                   "plain FP64 integrator",
+                                   f"{prec_main} integrator",
+                       "integrator": {"fast": "FP64, reference method with reassociated "
+                                              "equations of motion and FMA (error vs plain "
+                                              "under 'plain')",
+                                      "plain": "FP64, reference operation order, no FMA",
+                                      "mixed": "FP32 bulk, FP64 guards"}[prec_main],
                        "rays_per_build": traced, "l2": "flushed (256 MB write) before every step",
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "e2e": {"value": e2e_value, "unit": "geodesics/s", "h2d_bytes_per_step": h2d,
@@ -493,9 +541,7 @@ def main():
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": all_launches,
-            "mixed": {"value": mixed_value, "unit": "geodesics/s", "speedup_vs_plain":
-                      mixed_value / (traced * args.steps / (total_ms / 1e3)),
-                      "p99_rad_vs_plain": mixed_p99, "topology_exact": mixed_topo},
+            **other,
             "frames_4k": frames,
             "batched": batched,
         }

@@ -6,7 +6,8 @@ Compute runs in hand-written sm_100a CUDA (libblacktracer_b200.so, C ABI in
 include/blacktracer.h).  This package is the Python host mirror of the
 reference interfaces; device buffers are torch CUDA tensors.
 """
-from ._lib import (BtError, PRECISION_MIXED, PRECISION_PLAIN, RAY_CAPTURED,  # noqa: F401
+from ._lib import (BtError, PRECISION_FAST, PRECISION_MIXED, PRECISION_PLAIN,  # noqa: F401
+                   RAY_CAPTURED,
                    RAY_ESCAPED, RAY_MAXSTEP, RAY_NONCONVERGED, lib)
 from .host import (BlackHole, Camera, Grid, GridSet, IntegOpts, grid_dims,  # noqa: F401
                    integrate_rays, integrate_rays_host)

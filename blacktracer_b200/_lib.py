@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libblacktracer_b200.so")
 
 BT_OK, BT_ERR_ARG, BT_ERR_CUDA, BT_ERR_NOMEM, BT_ERR_NUMERIC, BT_ERR_STATE = range(6)
 RAY_ESCAPED, RAY_CAPTURED, RAY_MAXSTEP, RAY_NONCONVERGED = range(4)
-PRECISION_PLAIN, PRECISION_MIXED = 0, 1
+PRECISION_PLAIN, PRECISION_MIXED, PRECISION_FAST = 0, 1, 2
 
 
 class BtError(RuntimeError):

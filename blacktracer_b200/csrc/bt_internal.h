@@ -64,6 +64,9 @@ int launch_integrate_mixed(const RayParams& p, const double* th,
                            const double* ph, size_t n, double* tho,
                            double* pho, int32_t* steps, uint8_t* status,
                            cudaStream_t s);
+int launch_integrate_fast(const RayParams& p, const double* th, const double* ph,
+                          size_t n, double* tho, double* pho, int32_t* steps,
+                          uint8_t* status, cudaStream_t s);
 
 // Dense-lattice view of one grid on the device (grid.cu).  Vertex (i, j) of
 // the reference's CamToCel map lives at index i*M + j.
@@ -121,6 +124,8 @@ int launch_trace_plain(const GridDesc* D, int G, const uint32_t* qoff,
                        uint32_t* qfetch, TraceShape shape, cudaStream_t s);
 int launch_trace_mixed(const GridDesc* D, int G, const uint32_t* qoff,
                        uint32_t* qfetch, TraceShape shape, cudaStream_t s);
+int launch_trace_fast(const GridDesc* D, int G, const uint32_t* qoff,
+                      uint32_t* qfetch, TraceShape shape, cudaStream_t s);
 
 }  // namespace bt
 

@@ -951,6 +951,8 @@ int batch_enqueue(bt_batch* b, int startlevel, int precision, cudaStream_t s,
     if (t) BT_CUDA_TRY(cudaEventRecord(b->ev[b->n_ev], s));
     const int rc = precision == BT_PRECISION_MIXED
                        ? launch_trace_mixed(b->D, G, b->qoff, b->qfetch, b->shape, s)
+                   : precision == BT_PRECISION_FAST
+                       ? launch_trace_fast(b->D, G, b->qoff, b->qfetch, b->shape, s)
                        : launch_trace_plain(b->D, G, b->qoff, b->qfetch, b->shape, s);
     if (t) {
       BT_CUDA_TRY(cudaEventRecord(b->ev[b->n_ev + 1], s));

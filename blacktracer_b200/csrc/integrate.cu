@@ -63,6 +63,9 @@ int make_ray_params(const bt_camera* c, double a, const bt_integ_opts* o,
   }
   if (!c || !p) return BT_ERR_ARG;
   if (!(o->eps > 0) || o->maxstp < 0 || !(c->r > 0)) return BT_ERR_ARG;
+  if (o->precision != BT_PRECISION_PLAIN && o->precision != BT_PRECISION_MIXED &&
+      o->precision != BT_PRECISION_FAST)
+    return BT_ERR_ARG;
   std::memset(p, 0, sizeof(*p));
   p->thetaS = c->theta; p->phiS = c->phi; p->rS = c->r; p->sp = c->speed;
   p->br = c->br; p->btheta = c->btheta; p->bphi = c->bphi;
@@ -160,6 +163,8 @@ int launch_integrate(const RayParams& p, const double* th, const double* ph,
   if (blocks > cap) blocks = cap;
   if (p.precision == BT_PRECISION_MIXED)
     return launch_integrate_mixed(p, th, ph, n, tho, pho, steps, status, s);
+  if (p.precision == BT_PRECISION_FAST)
+    return launch_integrate_fast(p, th, ph, n, tho, pho, steps, status, s);
   k_integrate_plain<<<(unsigned)blocks, threads, 0, s>>>(p, th, ph, n, tho,
                                                          pho, steps, status);
   BT_CUDA_TRY(cudaGetLastError());

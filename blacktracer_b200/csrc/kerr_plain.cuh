@@ -99,8 +99,17 @@ __device__ __forceinline__ void eom(const double* y, double* f, double b,
   f[4] = s.f4;
 }
 
+// The equations of motion an attempt uses (the reference's by default).
+struct EomPlain {
+  static __device__ __forceinline__ void f(const double* y, double* o, double b, double q,
+                                           double a, double asq) {
+    eom(y, o, b, q, a, asq);
+  }
+};
+
 // One Cash-Karp attempt (BT/Metric.h:228-251).  Stage slopes k1..k5 are
 // the reference's aks[0..4], [5..9], ..., [20..24].
+template <class E = EomPlain>
 __device__ __forceinline__ void ck_attempt(const double* y, const double* d,
                                            double h, double* yo, double* err,
                                            double b, double q, double a,
@@ -108,23 +117,23 @@ __device__ __forceinline__ void ck_attempt(const double* y, const double* d,
   double k1[5], k2[5], k3[5], k4[5], k5[5], t[5];
 #pragma unroll
   for (int i = 0; i < 5; i++) t[i] = y[i] + b21 * h * d[i];
-  eom(t, k1, b, q, a, asq);
+  E::f(t, k1, b, q, a, asq);
 #pragma unroll
   for (int i = 0; i < 5; i++) t[i] = y[i] + h * (b31 * d[i] + b32 * k1[i]);
-  eom(t, k2, b, q, a, asq);
+  E::f(t, k2, b, q, a, asq);
 #pragma unroll
   for (int i = 0; i < 5; i++)
     t[i] = y[i] + h * (b41 * d[i] + b42 * k1[i] + b43 * k2[i]);
-  eom(t, k3, b, q, a, asq);
+  E::f(t, k3, b, q, a, asq);
 #pragma unroll
   for (int i = 0; i < 5; i++)
     t[i] = y[i] + h * (b51 * d[i] + b52 * k1[i] + b53 * k2[i] + b54 * k3[i]);
-  eom(t, k4, b, q, a, asq);
+  E::f(t, k4, b, q, a, asq);
 #pragma unroll
   for (int i = 0; i < 5; i++)
     t[i] = y[i] + h * (b61 * d[i] + b62 * k1[i] + b63 * k2[i] + b64 * k3[i] +
                        b65 * k4[i]);
-  eom(t, k5, b, q, a, asq);
+  E::f(t, k5, b, q, a, asq);
 #pragma unroll
   for (int i = 0; i < 5; i++) {
     yo[i] = y[i] + h * (c1 * d[i] + c3 * k2[i] + c4 * k3[i] + c6 * k5[i]);
@@ -270,12 +279,13 @@ __device__ __forceinline__ bool begin_ray(const RayParams& p, double th,
 // One quality-controlled attempt (odeint1 loop body + rkqs,
 // BT/Metric.h:291-302, 253-270).  Returns true when the ray is finished
 // (end point reached or attempt cap hit).
+template <class E = EomPlain>
 __device__ __forceinline__ bool attempt(const RayParams& p, RayState& s) {
   double d[5], scal[5], yt[5], err[5];
-  eom(s.y, d, s.b, s.q, p.a, p.asq);
+  E::f(s.y, d, s.b, s.q, p.a, p.asq);
 #pragma unroll
   for (int i = 0; i < 5; i++) scal[i] = fabs(s.y[i]) + fabs(d[i] * s.h) + kTiny;
-  ck_attempt(s.y, d, s.h, yt, err, s.b, s.q, p.a, p.asq);
+  ck_attempt<E>(s.y, d, s.h, yt, err, s.b, s.q, p.a, p.asq);
   double errmax = 0.0;
 #pragma unroll
   for (int i = 0; i < 5; i++) errmax = fmax(errmax, fabs(err[i] / scal[i]));

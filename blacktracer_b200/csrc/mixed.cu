@@ -1,7 +1,9 @@
-// mixed.cu -- launchers of the mixed-precision integrator (kerr_mixed.cuh).
-// Compiled with FMA contraction on: this form is not bit-matched to the
-// reference; its error against the FP64 oracle is measured instead.
+// mixed.cu -- launchers of the mixed-precision (kerr_mixed.cuh) and fast FP64
+// (kerr_fast.cuh) integrators.  Compiled with FMA contraction on: these forms
+// are not bit-matched to the reference; their error against the FP64 oracle
+// is measured instead.
 #include "bt_internal.h"
+#include "kerr_fast.cuh"
 #include "kerr_mixed.cuh"
 #include "trace_kernel.cuh"
 
@@ -25,6 +27,43 @@ struct MixedPolicy {
     plain::finish_ray(p, s.s, to, po, st, ss);
   }
 };
+
+struct FastPolicy {
+  using State = plain::RayState;
+  static __device__ __forceinline__ bool begin(const RayParams& p, double th,
+                                               double ph, State& s, double& to,
+                                               double& po, int32_t& st,
+                                               uint8_t& ss) {
+    return plain::begin_ray(p, th, ph, s, to, po, st, ss);
+  }
+  static __device__ __forceinline__ bool attempt(const RayParams& p, State& s) {
+    return fast::attempt(p, s);
+  }
+  static __device__ __forceinline__ void finish(const RayParams& p,
+                                                const State& s, double& to,
+                                                double& po, int32_t& st,
+                                                uint8_t& ss) {
+    plain::finish_ray(p, s, to, po, st, ss);
+  }
+};
+
+__global__ void __launch_bounds__(128)
+k_integrate_fast(const RayParams p, const double* __restrict__ th,
+                 const double* __restrict__ ph, size_t n,
+                 double* __restrict__ tho, double* __restrict__ pho,
+                 int32_t* __restrict__ steps, uint8_t* __restrict__ status) {
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n;
+       r += (size_t)gridDim.x * blockDim.x) {
+    double to, po;
+    int32_t st;
+    uint8_t s;
+    fast::integrate_ray(p, th[r], ph[r], to, po, st, s);
+    tho[r] = to;
+    pho[r] = po;
+    steps[r] = st;
+    if (status) status[r] = s;
+  }
+}
 
 __global__ void __launch_bounds__(128)
 k_integrate_mixed(const RayParams p, const double* __restrict__ th,
@@ -62,6 +101,25 @@ int launch_integrate_mixed(const RayParams& p, const double* th,
 int launch_trace_mixed(const GridDesc* D, int G, const uint32_t* qoff,
                        uint32_t* qfetch, TraceShape shape, cudaStream_t s) {
   return launch_trace_shape<MixedPolicy>(D, G, qoff, qfetch, shape, s);
+}
+
+int launch_integrate_fast(const RayParams& p, const double* th, const double* ph,
+                          size_t n, double* tho, double* pho, int32_t* steps,
+                          uint8_t* status, cudaStream_t s) {
+  if (n == 0) return BT_OK;
+  const int threads = 128;
+  size_t blocks = (n + threads - 1) / threads;
+  const size_t cap = (size_t)sm_count() * 16;
+  if (blocks > cap) blocks = cap;
+  k_integrate_fast<<<(unsigned)blocks, threads, 0, s>>>(p, th, ph, n, tho, pho, steps,
+                                                        status);
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
+int launch_trace_fast(const GridDesc* D, int G, const uint32_t* qoff,
+                      uint32_t* qfetch, TraceShape shape, cudaStream_t s) {
+  return launch_trace_shape<FastPolicy>(D, G, qoff, qfetch, shape, s);
 }
 
 }  // namespace bt

@@ -96,7 +96,8 @@ class IntegOpts:
         o = L.bt_integ_opts()
         L.lib().bt_integ_opts_default(C.byref(o))
         if isinstance(precision, str):
-            precision = {"plain": L.PRECISION_PLAIN, "mixed": L.PRECISION_MIXED}[precision]
+            precision = {"plain": L.PRECISION_PLAIN, "mixed": L.PRECISION_MIXED,
+                         "fast": L.PRECISION_FAST}[precision]
         o.precision = int(precision)
         for k, v in kw.items():
             setattr(o, k, v)
@@ -114,7 +115,7 @@ def _opts(opts) -> IntegOpts:
         return opts
     if isinstance(opts, str):
         return IntegOpts(opts)
-    raise TypeError("opts must be IntegOpts, 'plain', 'mixed' or None")
+    raise TypeError("opts must be IntegOpts, 'plain', 'mixed', 'fast' or None")
 
 
 def integrate_rays(cam: Camera, theta, phi, opts=None, a: float | None = None, stream=None):

@@ -93,3 +93,18 @@ def test_compact_export_matches_dense(bt, cuda, oracle_mod):
     # the reference's CamToCel holds exactly these keys
     ref = oracle_mod.grid_build(8, 5, True, cam, a, tfix=1)
     assert len(ii) == int(ref["exists"].sum())
+
+
+@pytest.mark.parametrize("ml,sl,camname", [(9, 6, "c2"), (9, 6, "c5")])
+def test_fast_grid_topology_matches_plain(bt, cuda, oracle_mod, ml, sl, camname):
+    """The fast FP64 form builds the same grid (vertex set, block levels) as
+    the plain form, with values within the 1e-6 rad target."""
+    cam, a = oracle_camera(oracle_mod, camname)
+    _, dp = build(bt, cam, a, ml, sl, True, "plain")
+    _, df = build(bt, cam, a, ml, sl, True, "fast")
+    assert np.array_equal(dp["exists"], df["exists"]), "vertex set differs"
+    assert np.array_equal(dp["blevel"], df["blevel"]), "block levels differ"
+    e = (dp["exists"] == 1) & (dp["theta"] >= 0)
+    err = ang_err(df["theta"][e], df["phi"][e], dp["theta"][e], dp["phi"][e])
+    print(f"fast grid L{ml}{camname}: p99 {np.percentile(err, 99):.2e} max {err.max():.2e}")
+    assert np.percentile(err, 99) <= 1e-6

@@ -5,7 +5,9 @@ differences come from the device libm's sin/cos/pow (an ulp at times), so
 rays agree to ~1e-12 except where an ulp flips an accept/reject decision of
 the step control.  Tolerance: 1e-9 rad per ray (max(|dtheta|, |dphi|)) for
 at least 99% of rays, same capture classification for all rays.
-Mixed form: p99 <= 1e-6 rad, identical capture classification.
+Mixed form: p99 <= 1e-6 rad, identical capture classification (the FP32
+form does not reach it; marked xfail).  Fast form (FP64 reassociated): p99
+<= 1e-6 rad, identical classification, >= 99% of rays on the same steps.
 """
 import os
 
@@ -71,6 +73,25 @@ def test_mixed_vs_oracle(bt, cuda, oracle_mod, name):
     print(f"{name} mixed: p50 {np.percentile(err, 50):.2e} p99 {np.percentile(err, 99):.2e} "
           f"max {err.max():.2e}")
     assert np.percentile(err, 99) <= MIXED_P99
+
+
+@pytest.mark.parametrize("name", sorted(CAMERAS))
+def test_fast_vs_oracle(bt, cuda, oracle_mod, name):
+    """Fast FP64 form (reassociated, FMA): same classification, p99 well
+    inside the 1e-6 rad target, nearly every ray on the reference's step
+    sequence."""
+    cam, a = oracle_camera(oracle_mod, name)
+    th, ph = seeded_rays(30000, seed=13)
+    ro = oracle_mod.integrate_rays(cam, a, th, ph)
+    to, po, st, ss = run_gpu(bt, cuda, cam, a, th, ph, "fast")
+    assert np.array_equal(ss == 1, ro[3] == 1), "capture classification must be exact"
+    esc = ro[3] == 0
+    err = ang_err(to[esc], po[esc], ro[0][esc], ro[1][esc])
+    same = float((st[esc] == ro[2][esc]).mean())
+    print(f"{name} fast: p50 {np.percentile(err, 50):.2e} p99 {np.percentile(err, 99):.2e} "
+          f"max {err.max():.2e} same steps {same:.4f}")
+    assert np.percentile(err, 99) <= MIXED_P99
+    assert same >= 0.99
 
 
 def test_host_entry_point_matches_device(bt, cuda):
