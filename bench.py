@@ -176,10 +176,10 @@ def synthetic_stars(n, seed, tmin=3000.0, tmax=30000.0):
     return [x.astype(np.float32) for x in (theta, phi, mag, bv)]
 
 
-def traffic_from_profiles():
-    """Per-launch DRAM bytes of the trace kernel from the committed ncu
-    summary (profiles/), or None."""
-    path = os.path.join(ROOT, "profiles", "k_trace_lattice_plain_c2.txt")
+def traffic_from_profiles(prec="plain"):
+    """Per-launch DRAM bytes of the trace kernel of form `prec` from the
+    committed ncu summary (profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", f"k_trace_lattice_{prec}_c2.txt")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -396,7 +396,7 @@ def main():
     achieved = flops_build / (trace_ms / args.steps / 1e3) / 1e12
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
-                "traffic": traffic_from_profiles(),
+                "traffic": traffic_from_profiles(prec_main),
                 "kernel": "k_trace_lattice<%sPolicy>" % prec_main.capitalize(),
                 "peak_source": "measured in this run: independent-chain DFMA probe "
                                "(bt_probe_fp64_tflops); MEASURED_PEAKS.json has no FP64 entry",
