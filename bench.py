@@ -191,6 +191,94 @@ def traffic_from_profiles(prec="plain"):
     return None
 
 
+SERVE = dict(rates=(30.0, 60.0, 120.0), sizes=((512, 256), (1920, 960), (3840, 1920)),
+             repeat=0.3, recent=10, seed=20261207, r=5.0, maxlevel=11, startlevel=6)
+
+
+def serve_rates(bt, torch, env, sp, n):
+    """The serving configuration: n frame requests per arrival rate, Poisson
+    arrivals (seeded), resolution uniform over SERVE['sizes'], spin uniform in
+    [0, 0.999], camera on the circular equatorial Keplerian orbit at r = 5M at a
+    uniform orbital phase; 30% of requests repeat one of the 10 most recent
+    poses.  Grid cache 40 GB, 10^6 resident stars.  Latency = completion -
+    submission (the generator submits at the scheduled arrival times)."""
+    out = {"workload": f"{n} requests per rate, Poisson arrivals, resolutions "
+                       "512x256 / 1920x960 / 3840x1920, a in [0, 0.999], Keplerian orbit "
+                       "r=5M at a uniform phase, 30% repeats of the 10 most recent poses; "
+                       "grids L6->L11 fast FP64, 40 GB grid cache, 1e6 stars, 8192x4096 env",
+           "rates": []}
+    pools = {sz: [] for sz in SERVE["sizes"]}
+    for rate in SERVE["rates"]:
+        rng = np.random.default_rng(SERVE["seed"] + int(rate))
+        t_arr = np.cumsum(rng.exponential(1.0 / rate, n))
+        poses, recent = [], []
+        for k in range(n):
+            if recent and rng.uniform() < SERVE["repeat"]:
+                poses.append(recent[rng.integers(len(recent))])
+            else:
+                p = (float(rng.uniform(0, 2 * np.pi)), float(rng.uniform(0.0, 0.999)))
+                poses.append(p)
+                recent = (recent + [p])[-SERVE["recent"]:]
+        sizes = [SERVE["sizes"][i] for i in rng.integers(0, len(SERVE["sizes"]), n)]
+        cams = {}
+        S = bt.Server(env=env, stars=sp, maxlevel=SERVE["maxlevel"],
+                      startlevel=SERVE["startlevel"], precision="fast",
+                      grid_cache_bytes=40 << 30, render_bytes=40 << 30, max_inflight=16)
+        # warm-up outside the timed schedule: render slots of every size (16 each)
+        # and the generator's pinned output buffers
+        wcam = bt.Camera(np.pi / 2, 0.0, SERVE["r"], 0.0, 0.0, 1.0, a=0.5)
+        for (W, H) in SERVE["sizes"]:
+            while len(pools[(W, H)]) < 32:
+                pools[(W, H)].append(torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True))
+            for q in range(16):
+                S.submit(10**9 + q, W, H, wcam, 0.5, pools[(W, H)][q])
+            got = 0
+            while got < 16:
+                got += len(S.poll(wait_ms=50))
+        st0 = S.stats()
+        used = {}
+        lat, done = {}, 0
+        t0 = time.perf_counter()
+
+        def collect(wait_ms=0):
+            nonlocal done
+            for c in S.poll(wait_ms=wait_ms):
+                assert c["status"] == 0, c
+                lat[c["id"]] = (c["t_done"] - c["t_submit"], c["grid_reused"])
+                pools[used.pop(c["id"])[0]].append(used_buf.pop(c["id"]))
+                done += 1
+
+        used_buf = {}
+        for k in range(n):
+            while time.perf_counter() - t0 < t_arr[k]:
+                collect()
+                time.sleep(0.0002)
+            W, H = sizes[k]
+            ph, a = poses[k]
+            if poses[k] not in cams:
+                cams[poses[k]] = bt.Camera(np.pi / 2, ph, SERVE["r"], 0.0, 0.0, 1.0, a=a)
+            buf = pools[(W, H)].pop() if pools[(W, H)] else torch.empty(
+                (H, W, 4), dtype=torch.uint8, pin_memory=True)
+            used[k] = ((W, H),)
+            used_buf[k] = buf
+            S.submit(k, W, H, cams[poses[k]], a, buf)
+        while done < n:
+            collect(wait_ms=20)
+        wall = time.perf_counter() - t0
+        st = S.stats()
+        S.close()
+        L = np.array([lat[k][0] for k in range(n)]) * 1e3
+        out["rates"].append({
+            "rate_rps": rate, "requests": n, "throughput_rps": n / wall,
+            "p50_ms": float(np.percentile(L, 50)), "p99_ms": float(np.percentile(L, 99)),
+            "mean_ms": float(L.mean()),
+            "grid_hits": st["grid_hits"] - st0["grid_hits"],
+            "grid_misses": st["grid_misses"] - st0["grid_misses"],
+            "grid_sets_built": st["build_sets"] - st0["build_sets"],
+            "evictions": st["evictions"] - st0["evictions"], "wall_s": wall})
+    return out
+
+
 def cpu_reference_arm(args):
     """--impl reference: the reference's own CPU integrator
     (Grid::integration_wrapper, compiled in place into oracle/_ref) on all
@@ -252,6 +340,9 @@ def main():
                     help="integrator form of the headline value")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the 64-pose batched-grid measurement")
+    ap.add_argument("--serve-requests", type=int, default=300,
+                    help="requests per arrival rate of the serving measurement (0 = skip; "
+                         "the serving configuration has 2000)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -404,15 +495,19 @@ def main():
                 "launches_per_build": launches / args.steps,
                 "avg_launch_ms": per_launch_ms}
 
-    # 4K frames with resident grid, environment and stars
-    frames = None
-    if args.frames > 0:
-        W, H = 3840, 1920
+    # resident environment (8192x4096) and star set (10^6 stars, tree level 14)
+    env = sp = None
+    if args.frames > 0 or args.serve_requests > 0:
         bgr = value_noise_env(torch, 4096, 8192, seed=20261204)
         env = bt.Environment(bgr)
         del bgr
         stars = synthetic_stars(1_000_000, seed=20261205)
         sp = bt.StarProcessor(*stars, treeLevel=14)
+
+    # 4K frames with resident grid, environment and stars
+    frames = None
+    if args.frames > 0:
+        W, H = 3840, 1920
         viewer = bt.Viewer(np.pi / 2, 0.0, 0.0, W, H, True)
         R = bt.Renderer(W, H)
         out = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
@@ -504,6 +599,11 @@ def main():
                        k: res[k]["value"] / plain_single for k in ("plain", "fast", "mixed")}}
         del sets, Sb
 
+    # serving loop: Poisson arrivals at 30, 60 and 120 requests/s
+    serving = None
+    if args.serve_requests > 0 and rank == 0:
+        serving = serve_rates(bt, torch, env, sp, args.serve_requests)
+
     # CPU baseline: the reference's own Grid constructor, one thread, full workload
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -544,6 +644,7 @@ def main():
             **other,
             "frames_4k": frames,
             "batched": batched,
+            "serving": serving,
         }
         print(json.dumps(line))
     if world > 1:

@@ -13,7 +13,9 @@ from .host import (BlackHole, Camera, Grid, GridSet, IntegOpts, grid_dims,  # no
                    integrate_rays, integrate_rays_host)
 
 from .render import Environment, Renderer, StarProcessor, Viewer  # noqa: F401
+from .serve import Server  # noqa: F401
 
-__all__ = ["Environment", "Renderer", "StarProcessor", "Viewer", "BlackHole", "Camera", "Grid",
+__all__ = ["Environment", "Renderer", "Server", "StarProcessor", "Viewer", "BlackHole",
+           "Camera", "Grid",
            "GridSet", "IntegOpts", "grid_dims", "integrate_rays",
            "integrate_rays_host", "BtError", "lib"]

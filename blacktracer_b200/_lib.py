@@ -63,6 +63,31 @@ class bt_batch_info(C.Structure):
                 ("launches", C.c_int32), ("graph", C.c_int32), ("shape", bt_trace_shape)]
 
 
+class bt_server_config(C.Structure):
+    _fields_ = [("maxlevel", C.c_int32), ("startlevel", C.c_int32), ("angle", C.c_int32),
+                ("precision", C.c_int32), ("grid_cache_bytes", C.c_size_t),
+                ("render_bytes", C.c_size_t), ("max_inflight", C.c_int32),
+                ("max_build_batch", C.c_int32), ("env", C.c_void_p), ("stars", C.c_void_p),
+                ("step", C.c_int32), ("lr", C.c_int32)]
+
+
+class bt_request(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("width", C.c_int32), ("height", C.c_int32),
+                ("cam", bt_camera), ("a", C.c_double), ("out", C.c_void_p)]
+
+
+class bt_completion(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("status", C.c_int32), ("grid_reused", C.c_int32),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
+class bt_server_stats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in (
+        "submitted", "completed", "failed", "grid_hits", "grid_misses", "grids_built",
+        "build_sets", "evictions", "grids_resident")] + [
+        ("grid_cache_bytes_used", C.c_size_t), ("render_bytes_used", C.c_size_t)]
+
+
 class bt_frame(C.Structure):
     _fields_ = [("grid", C.c_void_p), ("grid_rows", C.c_int32), ("grid_cols", C.c_int32),
                 ("grid_level", C.c_int32), ("view", C.c_void_p), ("hor", C.c_float),
@@ -133,6 +158,16 @@ _SIGS = {
     "bt_map_destroy": (None, [_vp]),
     "bt_map_render": (C.c_int, [_vp, C.POINTER(bt_frame), _vp]),
     "bt_map_scratch": (C.c_int, [_vp, C.POINTER(bt_map_buffers)]),
+    "bt_batch_build_first": (C.c_int, [_vp, C.c_int, C.POINTER(bt_camera),
+                                       C.POINTER(C.c_double), C.c_int,
+                                       C.POINTER(bt_integ_opts), _vp]),
+    "bt_server_config_default": (None, [C.POINTER(bt_server_config)]),
+    "bt_server_create": (C.c_int, [C.POINTER(bt_server_config), C.POINTER(_vp)]),
+    "bt_server_submit": (C.c_int, [_vp, C.POINTER(bt_request)]),
+    "bt_server_poll": (C.c_int, [_vp, C.POINTER(bt_completion), C.c_int,
+                                 C.POINTER(C.c_int), C.c_int]),
+    "bt_server_stats_get": (C.c_int, [_vp, C.POINTER(bt_server_stats)]),
+    "bt_server_destroy": (None, [_vp]),
     "bt_last_error": (C.c_char_p, []),
     "bt_version": (C.c_char_p, []),
 }

@@ -33,6 +33,7 @@ UNITS = {
     "stars.cu": ["--fmad=false"],
     "map_api.cu": [],
     "noalloc.cu": [],
+    "server.cu": [],
 }
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
            if f.endswith((".h", ".cuh"))] + [os.path.join(ROOT, "include", "blacktracer.h")]

@@ -98,6 +98,7 @@ struct bt_batch {
   int startlevel, precision;
   int launches;           // kernels of the last build
   int built;
+  int built_n;            // members built by the last build (the first built_n)
   // timing of the trace launches (eager builds only)
   int timing;
   cudaEvent_t ev[2 * 16];
@@ -106,7 +107,7 @@ struct bt_batch {
   int graph;
   cudaStream_t cap_stream;
   cudaGraphExec_t exec;
-  int exec_startlevel, exec_precision;
+  int exec_n, exec_startlevel, exec_precision;
   bt::TraceShape exec_shape;
 };
 
@@ -934,9 +935,9 @@ GridDesc member_desc(bt_batch* b, int g, int startlevel, const RayParams& p) {
 
 // The launch sequence of one build of the whole set (no host
 // synchronisation).  Returns the number of kernels launched in *launches.
-int batch_enqueue(bt_batch* b, int startlevel, int precision, cudaStream_t s,
+int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_t s,
                   bool timing, int* launches) {
-  const int G = b->G;
+  const int G = n;  // the first n members
   const size_t NM = b->NM;
   int nk = 0;
   BT_CUDA_TRY(cudaMemsetAsync(b->vflag, 0, G * NM + 4, s));
@@ -1004,13 +1005,14 @@ int batch_enqueue(bt_batch* b, int startlevel, int precision, cudaStream_t s,
   return BT_OK;
 }
 
-int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int startlevel,
-                const bt_integ_opts* o, cudaStream_t s) {
+int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int n,
+                int startlevel, const bt_integ_opts* o, cudaStream_t s) {
   BT_ARG_CHECK(cams && spins, "NULL cameras or spins");
+  BT_ARG_CHECK(n >= 1 && n <= b->G, "grid count out of [1, set size]");
   BT_ARG_CHECK(startlevel >= 1 && startlevel <= b->maxlevel,
                "startlevel out of [1, maxlevel]");
   BT_ARG_CHECK(b->maxlevel - startlevel <= 12, "maxlevel - startlevel > 12 is not supported");
-  const int G = b->G;
+  const int G = n;
   // descriptors into the next pinned staging slot, once its last copy ran
   const int slot = b->slot;
   b->slot = (slot + 1) % kParamSlots;
@@ -1037,7 +1039,7 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int sta
   BT_CUDA_TRY(cudaEventRecord(b->Dev[slot], s));
   int launches = 0;
   if (b->graph) {
-    const bool same = b->exec && b->exec_startlevel == startlevel &&
+    const bool same = b->exec && b->exec_n == G && b->exec_startlevel == startlevel &&
                       b->exec_precision == precision &&
                       b->exec_shape.threads == b->shape.threads &&
                       b->exec_shape.blocks_per_sm == b->shape.blocks_per_sm;
@@ -1047,7 +1049,7 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int sta
       if (!b->cap_stream)
         BT_CUDA_TRY(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking));
       BT_CUDA_TRY(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal));
-      int rc = batch_enqueue(b, startlevel, precision, b->cap_stream, false, &launches);
+      int rc = batch_enqueue(b, G, startlevel, precision, b->cap_stream, false, &launches);
       cudaGraph_t graph = nullptr;
       const cudaError_t e = cudaStreamEndCapture(b->cap_stream, &graph);
       if (rc == BT_OK && e != cudaSuccess) {
@@ -1064,6 +1066,7 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int sta
       }
       if (graph) cudaGraphDestroy(graph);
       if (rc) return rc;
+      b->exec_n = G;
       b->exec_startlevel = startlevel;
       b->exec_precision = precision;
       b->exec_shape = b->shape;
@@ -1072,13 +1075,14 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int sta
     BT_CUDA_TRY(cudaGraphLaunch(b->exec, s));
     b->n_ev = 0;
   } else {
-    if (int rc = batch_enqueue(b, startlevel, precision, s, true, &launches)) return rc;
+    if (int rc = batch_enqueue(b, G, startlevel, precision, s, true, &launches)) return rc;
     b->launches = launches;
   }
   b->startlevel = startlevel;
   b->precision = precision;
   b->built = 1;
-  for (int g = 0; g < G; g++) b->grids[g].built = 1;
+  b->built_n = G;
+  for (int g = 0; g < b->G; g++) b->grids[g].built = g < G ? 1 : 0;
   return BT_OK;
 }
 
@@ -1137,7 +1141,7 @@ int bt_grid_build(bt_grid* g, const bt_camera* cam, double a, int startlevel,
   clear_error();
   BT_ARG_CHECK(g && cam, "NULL pointer");
   BT_ARG_CHECK(g->set->standalone, "the grid belongs to a set: build the set (bt_batch_build)");
-  return batch_build(g->set, cam, &a, startlevel, o, (cudaStream_t)stream);
+  return batch_build(g->set, cam, &a, 1, startlevel, o, (cudaStream_t)stream);
 }
 
 int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream) {
@@ -1292,7 +1296,14 @@ int bt_batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int 
                    const bt_integ_opts* o, void* stream) {
   clear_error();
   BT_ARG_CHECK(b != nullptr, "NULL set");
-  return batch_build(b, cams, spins, startlevel, o, (cudaStream_t)stream);
+  return batch_build(b, cams, spins, b->G, startlevel, o, (cudaStream_t)stream);
+}
+
+int bt_batch_build_first(bt_batch* b, int n, const bt_camera* cams, const double* spins,
+                         int startlevel, const bt_integ_opts* o, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(b != nullptr, "NULL set");
+  return batch_build(b, cams, spins, n, startlevel, o, (cudaStream_t)stream);
 }
 
 bt_grid* bt_batch_grid(bt_batch* b, int k) {
@@ -1328,8 +1339,8 @@ int bt_batch_query(bt_batch* b, bt_batch_info* info, void* stream) {
   BT_ARG_CHECK(b->built, "set not built");
   BT_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
   std::memset(info, 0, sizeof(*info));
-  info->count = b->G;
-  for (int g = 0; g < b->G; g++) {
+  info->count = b->built_n;
+  for (int g = 0; g < b->built_n; g++) {
     const GridCounters& c = b->ctr_host[g];
     info->traced += ((int64_t)c.traced_hi << 32) | c.traced_lo;
     info->flags |= c.err | (c.overflow ? 4u : 0u);
@@ -1366,11 +1377,11 @@ int bt_batch_autotune(bt_batch* b, const bt_camera* cams, const double* spins, i
   int rc = BT_OK;
   for (const TraceShape& c : cand) {
     b->shape = c;
-    if ((rc = batch_build(b, cams, spins, startlevel, o, s))) break;  // warm-up
+    if ((rc = batch_build(b, cams, spins, b->G, startlevel, o, s))) break;  // warm-up
     float t_min = 3.4e38f;
     for (int r = 0; r < repeats && rc == BT_OK; r++) {
       cudaEventRecord(e0, s);
-      rc = batch_build(b, cams, spins, startlevel, o, s);
+      rc = batch_build(b, cams, spins, b->G, startlevel, o, s);
       cudaEventRecord(e1, s);
       if (cudaEventSynchronize(e1) != cudaSuccess) rc = BT_ERR_CUDA;
       float ms = 0.f;

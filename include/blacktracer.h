@@ -244,6 +244,13 @@ void bt_batch_destroy(bt_batch* b);
 int bt_batch_build(bt_batch* b, const bt_camera* cams, const double* spins,
                    int startlevel, const bt_integ_opts* o, void* stream);
 
+/* Builds only members 0..n-1 (1 <= n <= count) from cams[0..n-1] and
+ * spins[0..n-1]; the other members are left unbuilt.  For callers that
+ * gather a varying number of grids per build (a serving loop). */
+int bt_batch_build_first(bt_batch* b, int n, const bt_camera* cams,
+                         const double* spins, int startlevel,
+                         const bt_integ_opts* o, void* stream);
+
 /* Member k (0 <= k < count), or NULL. */
 bt_grid* bt_batch_grid(bt_batch* b, int k);
 
@@ -260,7 +267,7 @@ typedef struct bt_trace_shape {
 int bt_batch_set_shape(bt_batch* b, const bt_trace_shape* shape);
 
 typedef struct bt_batch_info {
-  int32_t count;
+  int32_t count;           /* members built by the last build              */
   int64_t traced;          /* rays integrated by the last build, all grids */
   uint32_t flags;          /* OR of the members' flags                     */
   float trace_ms;          /* with timing on, eager builds                 */
@@ -353,6 +360,67 @@ typedef struct bt_map_buffers {
   const uint8_t* env_img;
 } bt_map_buffers;
 int bt_map_scratch(const bt_map* m, bt_map_buffers* b);
+
+/* --------------------------------------------------------------- serving */
+
+/* A frame server: requests of any resolution, camera and spin are rendered
+ * (grid + per-pixel map, equirectangular sphere view) by a worker thread
+ * with continuous batching -- admission by HBM budget and in-flight slots,
+ * grids resident in a cache keyed by the exact camera and spin and reused,
+ * the grids missing at an admission round built together as one grid set,
+ * frames of different requests on their own streams, overlapping each other
+ * and the next grid build.  No counterpart in the reference (a single-scene
+ * host program, BT/BlackTracer.cpp). */
+typedef struct bt_server bt_server;
+
+typedef struct bt_server_config {
+  int32_t maxlevel, startlevel, angle;  /* grids built for requests         */
+  int32_t precision;                    /* BT_PRECISION_* of grid builds    */
+  size_t grid_cache_bytes;              /* HBM budget of resident grids     */
+  size_t render_bytes;                  /* HBM budget of render slots       */
+  int32_t max_inflight;                 /* frames admitted at once          */
+  int32_t max_build_batch;              /* grids built together (set size)  */
+  const bt_env* env;                    /* environment map, or NULL         */
+  const bt_stars* stars;                /* resident star set, or NULL       */
+  int32_t step, lr;                     /* splat radius, lensing + redshift */
+} bt_server_config;
+
+/* Defaults: L6 -> L11 full-sphere grids, fast FP64, 40 GB grid cache,
+ * 40 GB render slots, 16 frames in flight, sets of 8, step 1, lr on. */
+void bt_server_config_default(bt_server_config* c);
+
+typedef struct bt_request {
+  uint64_t id;            /* caller's tag, returned in the completion     */
+  int32_t width, height;
+  bt_camera cam;
+  double a;               /* spin                                         */
+  uint8_t* out;           /* width*height*4 BGRA8: pinned host or device  */
+} bt_request;
+
+typedef struct bt_completion {
+  uint64_t id;
+  int32_t status;         /* BT_OK or the error code                      */
+  int32_t grid_reused;    /* 1: the grid was resident                     */
+  double t_submit, t_admit, t_done;  /* seconds, steady clock             */
+} bt_completion;
+
+typedef struct bt_server_stats {
+  int64_t submitted, completed, failed;
+  int64_t grid_hits, grid_misses, grids_built, build_sets, evictions;
+  int64_t grids_resident;
+  size_t grid_cache_bytes_used, render_bytes_used;
+} bt_server_stats;
+
+/* The server uses the device current at creation; env and stars must
+ * outlive it. */
+int bt_server_create(const bt_server_config* cfg, bt_server** out);
+/* Thread-safe, non-blocking.  r->out must stay valid until completion. */
+int bt_server_submit(bt_server* s, const bt_request* r);
+/* Up to cap completions; waits up to wait_ms for the first one. */
+int bt_server_poll(bt_server* s, bt_completion* out, int cap, int* n, int wait_ms);
+int bt_server_stats_get(bt_server* s, bt_server_stats* st);
+/* Finishes every submitted request, then releases the server. */
+void bt_server_destroy(bt_server* s);
 
 /* FP64 FMA throughput of the current device, TFLOP/s (2 flops per FMA),
  * from an independent-chain DFMA kernel timed with CUDA events: the peak
