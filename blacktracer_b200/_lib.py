@@ -94,12 +94,12 @@ class bt_frame(C.Structure):
                 ("ver", C.c_float), ("cam", C.c_float * 7), ("env", C.c_void_p),
                 ("stars", C.c_void_p), ("map", C.c_int32), ("star", C.c_int32),
                 ("lr", C.c_int32), ("step", C.c_int32), ("diffraction", C.c_int32),
-                ("out", C.c_void_p)]
+                ("out", C.c_void_p), ("bb_table", C.c_int32), ("psf_scale", C.c_int32)]
 
 
 class bt_map_buffers(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("thphi", "gap", "bh", "area", "light",
-                                          "stars_img", "env_img")]
+                                          "stars_img", "env_img", "light_diffracted")]
 
 
 _vp = C.c_void_p
@@ -149,6 +149,7 @@ _SIGS = {
     "bt_env_destroy": (None, [_vp]),
     "bt_env_sat": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "bt_stars_tree_size": (C.c_int, [C.c_int]),
+    "bt_psf_airy": (C.c_int, [C.c_int, C.c_float, _vp]),
     "bt_stars_build_tree": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_float,
                                       _vp, _vp, _vp, C.POINTER(C.c_int)]),
     "bt_stars_create": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int,

@@ -164,6 +164,7 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
   BT_ARG_CHECK(!f->map || f->env, "map requested without an environment");
   BT_ARG_CHECK(!f->star || f->stars, "stars requested without a star set");
   BT_ARG_CHECK(f->step >= 0 && f->step <= 2, "step out of [0, 2]");
+  BT_ARG_CHECK(f->bb_table == 0 || f->bb_table == 1, "bb_table must be 0 or 1");
   cudaStream_t s = (cudaStream_t)stream;
   MapFrame F;
   F.grid = (const float2*)f->grid;
@@ -175,7 +176,9 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
   F.ver = f->ver;
   for (int q = 0; q < 7; q++) F.cam.v[q] = f->cam[q];
   F.env = f->env ? &f->env->e : nullptr;
-  F.stars = f->stars ? stars_internal(f->stars) : nullptr;
+  F.stars = f->stars;
+  F.bb_table = f->bb_table;
+  F.psf_scale = f->psf_scale;
   F.map = f->map;
   F.star = f->star;
   F.lr = f->lr;
@@ -203,6 +206,7 @@ int bt_map_scratch(const bt_map* m, bt_map_buffers* b) {
   b->light = m->S.light;
   b->stars_img = m->S.stars_img;
   b->env_img = m->tmp_img;
+  b->light_diffracted = m->S.light2;
   return BT_OK;
 }
 

@@ -50,8 +50,10 @@ struct MapFrame {
   float hor, ver;
   Cam7 cam;
   const EnvMap* env;
-  const StarSet* stars;
+  const bt_stars* stars;
   int map, star, lr, step, diffraction;
+  int bb_table;         // 0: the reference's 391-entry table, 1: 1024-entry FP32
+  int psf_scale;        // diffraction footprint scaled by sqrt(pixel magnification)
   uint8_t* out_bg;      // N*M*4 environment (or final) image
   uint8_t* out;         // N*M*4 final image
 };

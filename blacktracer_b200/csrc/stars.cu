@@ -23,6 +23,7 @@
 // Trails (addTrails, :98-174) are a multi-frame effect and are not part of
 // a single frame: on the first frame they leave the image unchanged.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <limits>
 #include <new>
@@ -42,13 +43,26 @@ struct bt_stars {
   float* mag;
   int* tree;
   float4* box;
-  float4* bb;  // 2 * kBlackbodyEntries: HSP, then RGB at unit brightness
+  float4* bb;    // 2 * kBlackbodyEntries: HSP, then RGB at unit brightness
+  float4* bb1k;  // the same for the 1024-entry FP32 table
   uchar3* psf;
 };
 
 namespace bt {
 
+constexpr int kBlackbody1k = 1024;
+
 const StarSet* stars_internal(const bt_stars* s) { return &s->s; }
+
+StarSet stars_for_frame(const bt_stars* s, int bb_table) {
+  StarSet o = s->s;
+  if (bb_table == 1) {
+    o.bb_hsp = s->bb1k;
+    o.bb_rgb = s->bb1k + kBlackbody1k;
+    o.bb_n = kBlackbody1k;
+  }
+  return o;
+}
 
 constexpr int TX = 32, TY = 8;
 static dim3 grid2(int w, int h) {
@@ -407,10 +421,30 @@ __global__ void k_blackbody_tables(float4* __restrict__ bb) {
   bb[kBlackbodyEntries + k] = make_float4(255.f * r, 255.f * g, 255.f * b, 0.f);
 }
 
+// The 1024-entry FP32 table: entry k lies at k * 390/1023 on the reference's
+// 100 K grid and is the linear interpolation of its two neighbouring entries.
+__global__ void k_blackbody_tables_1k(float4* __restrict__ bb) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= kBlackbody1k) return;
+  const float t = (float)k * ((float)(kBlackbodyEntries - 1) / (float)(kBlackbody1k - 1));
+  const int i0 = imin((int)t, kBlackbodyEntries - 2);
+  const float f = t - (float)i0;
+  float c[3];
+  for (int q = 0; q < 3; q++)
+    c[q] = ((1.f - f) * (float)blackbody(3 * i0 + q) + f * (float)blackbody(3 * i0 + 3 + q)) /
+           255.f;
+  float3 h;
+  rgb_to_hsp(c[0], c[1], c[2], h.x, h.y, h.z);
+  float r, g, b;
+  hsp_to_rgb(h.x, h.y, h.z, r, g, b);
+  bb[k] = make_float4(h.x, h.y, h.z, 0.f);
+  bb[kBlackbody1k + k] = make_float4(255.f * r, 255.f * g, 255.f * b, 0.f);
+}
+
 template <int kStep>
-void launch_heavy(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
+void launch_heavy(MapScratch& Sc, const MapFrame& F, const StarSet& SS, cudaStream_t s) {
   k_star_heavy<kStep><<<sm_count() * 2, kHeavyThreads, 0, s>>>(
-      Sc.thphi, Sc.bh, *F.stars, F.cam, Sc.M, Sc.N, F.view, F.lr, Sc.area, Sc.cells,
+      Sc.thphi, Sc.bh, SS, F.cam, Sc.M, Sc.N, F.view, F.lr, Sc.area, Sc.cells,
       Sc.flag, Sc.heavy_order, Sc.heavy_count, (uint32_t)((size_t)Sc.M * Sc.N));
 }
 
@@ -515,6 +549,57 @@ __global__ void k_diff_scatter(const float* __restrict__ light, float* acc,
   }
 }
 
+// Diffraction with the sprite's footprint scaled by s = sqrt(magnification)
+// of the bright pixel (magnification = the pixel's camera-sky area over its
+// celestial solid angle, as lensing uses), s clamped to [0.25, 4]: the
+// sprite is sampled bilinearly at (offset / s) and divided by s^2, so a
+// pixel's total diffracted light is the unscaled sprite's.  Otherwise as
+// k_diff_scatter (snapshot reads, the reference's amplitude and clamp).
+__global__ void k_diff_scatter_scaled(const float* __restrict__ light, float* acc,
+                                      const uint32_t* __restrict__ list, const uint32_t* count,
+                                      int M, int N, const uchar3* __restrict__ psf, int fs,
+                                      const float2* __restrict__ view,
+                                      const float* __restrict__ area) {
+  const uint32_t n = *count;
+  for (uint32_t b = blockIdx.x; b < n; b += gridDim.x) {
+    const uint32_t ij = list[b];
+    const int i = ij / M, j = ij % M;
+    const int M1 = M + 1, ind = i * M1 + j;
+    float ver4[4] = {view[ind].x, view[ind + 1].x, view[ind + M1 + 1].x, view[ind + M1].x};
+    float hor4[4] = {view[ind].y, view[ind + 1].y, view[ind + M1 + 1].y, view[ind + M1].y};
+    const float sa = area[ij];
+    const float mag = sa > 0.f ? calc_area(ver4, hor4) / sa : 1.f;
+    const float sc = fminf(4.f, fmaxf(0.25f, sqrtf(fmaxf(mag, 0.f))));
+    const int fe = 2 * (int)ceilf(0.5f * fs * sc) + 1;  // odd footprint
+    const int fh = fe / 2;
+    const float lx = light[3 * ij], ly = light[3 * ij + 1], lz = light[3 * ij + 2];
+    const float mxv = fmaxf(fmaxf(lx, ly), lz);
+    const float div = 10000 * powf(mxv, 0.6) * sc * sc;
+    const float c0 = 0.5f * (fs - 1);
+    for (int c = threadIdx.x; c < fe * fe; c += blockDim.x) {
+      const int q = c / fe, p = c % fe;
+      const int ti = i - fh + q;
+      if (ti < 0 || ti >= N) continue;
+      const float u = (q - fh) / sc + c0, v = (p - fh) / sc + c0;
+      if (u < 0.f || v < 0.f || u > fs - 1 || v > fs - 1) continue;
+      const int u0 = min((int)u, fs - 2), v0 = min((int)v, fs - 2);
+      const float fu = u - u0, fv = v - v0;
+      const uchar3 a00 = psf[u0 * fs + v0], a01 = psf[u0 * fs + v0 + 1];
+      const uchar3 a10 = psf[(u0 + 1) * fs + v0], a11 = psf[(u0 + 1) * fs + v0 + 1];
+      const float w00 = (1 - fu) * (1 - fv), w01 = (1 - fu) * fv, w10 = fu * (1 - fv),
+                  w11 = fu * fv;
+      const float dxs = w00 * a00.x + w01 * a01.x + w10 * a10.x + w11 * a11.x;
+      const float dys = w00 * a00.y + w01 * a01.y + w10 * a10.y + w11 * a11.y;
+      const float dzs = w00 * a00.z + w01 * a01.z + w10 * a10.z + w11 * a11.z;
+      const float dx = lx / div * dxs, dy = ly / div * dys, dz = lz / div * dzs;
+      const size_t t = (size_t)ti * M + (j - fh + p + 64 * (size_t)M) % M;
+      atomicAdd(&acc[3 * t], fminf(65025.f, dx * dx));
+      atomicAdd(&acc[3 * t + 1], fminf(65025.f, dy * dy));
+      atomicAdd(&acc[3 * t + 2], fminf(65025.f, dz * dz));
+    }
+  }
+}
+
 // makePix + composite from a light buffer (after diffraction).
 __global__ void k_makepix(const float* __restrict__ light, int M, int N,
                           const uchar4* __restrict__ bg, uchar4* __restrict__ out,
@@ -550,6 +635,7 @@ __global__ void k_makepix(const float* __restrict__ light, int M, int N,
 
 int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   const int M = Sc.M, N = Sc.N;
+  const StarSet SS = stars_for_frame(F.stars, F.bb_table);
   const int fw = 2 * F.step + 1;
   const size_t np = (size_t)M * N;
   if (!Sc.cells || Sc.cells_fw < fw) {
@@ -568,16 +654,16 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   }
   BT_CUDA_TRY(cudaMemsetAsync(Sc.heavy_count, 0, kHcWords * sizeof(uint32_t), s));
   k_star_cells<<<grid2(M, N), dim3(TX, TY), 0, s>>>(
-      Sc.thphi, Sc.bh, *F.stars, F.cam, M, N, F.step, F.view, F.lr, Sc.area,
+      Sc.thphi, Sc.bh, SS, F.cam, M, N, F.step, F.view, F.lr, Sc.area,
       Sc.cells, Sc.flag, Sc.heavy_list, Sc.heavy_count + kHcDeferred);
   k_heavy_plan<<<sm_count() * 2, 128, 0, s>>>(
-      Sc.thphi, Sc.bh, *F.stars, F.cam, M, F.step, F.view, F.lr, Sc.area, Sc.heavy_list,
+      Sc.thphi, Sc.bh, SS, F.cam, M, F.step, F.view, F.lr, Sc.area, Sc.heavy_list,
       Sc.heavy_count, Sc.heavy_order, (uint32_t)np);
-  if (F.step == 0) launch_heavy<0>(Sc, F, s);
-  else if (F.step == 1) launch_heavy<1>(Sc, F, s);
-  else launch_heavy<2>(Sc, F, s);
+  if (F.step == 0) launch_heavy<0>(Sc, F, SS, s);
+  else if (F.step == 1) launch_heavy<1>(Sc, F, SS, s);
+  else launch_heavy<2>(Sc, F, SS, s);
   BT_CUDA_TRY(cudaGetLastError());
-  const bool diff = F.diffraction && F.stars->psf && F.stars->psf_size > 0;
+  const bool diff = F.diffraction && SS.psf && SS.psf_size > 0;
   if (!diff) {
     k_star_gather<true><<<grid2(M, N), dim3(TX, TY), 0, s>>>(
         Sc.cells, Sc.flag, M, N, F.step, Sc.light, (const uchar4*)F.out_bg,
@@ -592,9 +678,13 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   BT_CUDA_TRY(cudaMemsetAsync(Sc.diff_count, 0, sizeof(uint32_t), s));
   k_diff_mark<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(Sc.light, (int)np,
                                                           Sc.diff_list, Sc.diff_count);
-  k_diff_scatter<<<sm_count() * 8, 256, 0, s>>>(Sc.light, Sc.light2, Sc.diff_list,
-                                                Sc.diff_count, M, N, F.stars->psf,
-                                                F.stars->psf_size);
+  if (F.psf_scale)
+    k_diff_scatter_scaled<<<sm_count() * 8, 256, 0, s>>>(Sc.light, Sc.light2, Sc.diff_list,
+                                                         Sc.diff_count, M, N, SS.psf,
+                                                         SS.psf_size, F.view, Sc.area);
+  else
+    k_diff_scatter<<<sm_count() * 8, 256, 0, s>>>(Sc.light, Sc.light2, Sc.diff_list,
+                                                  Sc.diff_count, M, N, SS.psf, SS.psf_size);
   k_makepix<<<grid2(M, N), dim3(TX, TY), 0, s>>>(Sc.light2, M, N,
                                                  (const uchar4*)F.out_bg,
                                                  (uchar4*)F.out, F.map);
@@ -696,6 +786,27 @@ extern "C" {
 
 int bt_stars_tree_size(int treeLevel) { return (1 << (treeLevel + 1)) - 1; }
 
+int bt_psf_airy(int size, float first_zero, uint8_t* rgb) {
+  clear_error();
+  BT_ARG_CHECK(rgb && size >= 3 && size <= 1025 && (size & 1) && first_zero > 0.f,
+               "invalid sprite arguments (odd size in [3, 1025], first_zero > 0)");
+  // first zero of J1 at x = 3.8317...; channel wavelengths relative to 550 nm
+  const double j1z = 3.8317059702075123, lam[3] = {610. / 550., 550. / 550., 465. / 550.};
+  const int h = size / 2;
+  for (int y = 0; y < size; y++)
+    for (int x = 0; x < size; x++) {
+      const double r = std::sqrt((double)(x - h) * (x - h) + (double)(y - h) * (y - h));
+      for (int c = 0; c < 3; c++) {
+        const double z = j1z * r / (first_zero * lam[c]);
+        const double I = z < 1e-9 ? 1.0 : std::pow(2.0 * std::cyl_bessel_j(1.0, z) / z, 2.0);
+        // RGB order, as the reference loads its sprite (stbi_load,
+        // BT/MakeImageKernel.cu:1281-1286): channel c scales star light c
+        rgb[((size_t)y * size + x) * 3 + c] = (uint8_t)std::lround(255.0 * I);
+      }
+    }
+  return BT_OK;
+}
+
 int bt_stars_build_tree(const float* theta, const float* phi, const float* mag,
                         const float* bv, int n, int treeLevel, float magnitude_cut,
                         float* star_pos, float* star_mag, int* tree, int* n_kept) {
@@ -747,8 +858,10 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   if (e == cudaSuccess) e = cudaMalloc((void**)&st->tree, tsize * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc((void**)&st->box, box.size() * sizeof(float4));
   if (e == cudaSuccess) e = cudaMalloc((void**)&st->bb, 2 * kBlackbodyEntries * sizeof(float4));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&st->bb1k, 2 * kBlackbody1k * sizeof(float4));
   if (e == cudaSuccess) {
     k_blackbody_tables<<<(kBlackbodyEntries + 127) / 128, 128, 0, s>>>(st->bb);
+    k_blackbody_tables_1k<<<kBlackbody1k / 128, 128, 0, s>>>(st->bb1k);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess && psf_size)
@@ -770,7 +883,7 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     cudaFree(st->pos); cudaFree(st->mag); cudaFree(st->tree); cudaFree(st->box);
-    cudaFree(st->bb); cudaFree(st->psf);
+    cudaFree(st->bb); cudaFree(st->bb1k); cudaFree(st->psf);
     delete st;
     set_error("star set upload failed: %s", cudaGetErrorString(e));
     return BT_ERR_CUDA;
@@ -783,6 +896,7 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   st->s.box = st->box;
   st->s.bb_hsp = st->bb;
   st->s.bb_rgb = st->bb + kBlackbodyEntries;
+  st->s.bb_n = kBlackbodyEntries;
   st->s.psf = st->psf;
   st->s.psf_size = psf_size;
   *out = st;
@@ -796,6 +910,7 @@ void bt_stars_destroy(bt_stars* st) {
   cudaFree(st->tree);
   cudaFree(st->box);
   cudaFree(st->bb);
+  cudaFree(st->bb1k);
   if (st->psf) cudaFree(st->psf);
   delete st;
 }

@@ -23,8 +23,12 @@ struct StarSet {
   int psf_size;
   // Per blackbody entry: RGBtoHSP of its colour (h, s, p) and
   // 255 * HSPtoRGB(h, s, p), computed once on the device by the same code.
+  // bb_n = 391: the reference's table (100 K steps, index floor(temp));
+  // bb_n = 1024: an FP32 table over the same 1000-40000 K range, linearly
+  // interpolated from the reference's entries (index round(temp * 1023/390)).
   const float4* bb_hsp;
   const float4* bb_rgb;
+  int bb_n;
   // Bounding box of each node's stars, (theta_min, phi_min, theta_max,
   // phi_max); min > max for a node without stars.  Not part of the
   // reference's layout: derived from pos and tree when the set is created.
@@ -254,7 +258,7 @@ struct StarHit {
 
 // Blackbody entry of a star of colour index bv seen with redshift factor
 // redshft (BT/MakeImageKernel.cu:294-297).
-BT_HD int blackbody_index(float bv, float redshft) {
+BT_HD int blackbody_index(float bv, float redshft, int n = kBlackbodyEntries) {
   const float temp = 46.f / redshft *
                          ((1.f / ((0.92f * bv) + 1.7f)) + (1.f / ((0.92f * bv) + 0.62f))) -
                      10.f;
@@ -262,7 +266,9 @@ BT_HD int blackbody_index(float bv, float redshft) {
   // the flattened table minus 3, then reads tempToRGB[3*index]: shifted
   // temperatures above 40000 K read past its 391 entries.  Clamped to the
   // last entry (40000 K) here.
-  return imax(0, imin((int)floorf(temp), kBlackbodyEntries - 1));
+  if (n == kBlackbodyEntries) return imax(0, imin((int)floorf(temp), kBlackbodyEntries - 1));
+  const float t = fminf(fmaxf(temp, 0.f), (float)(kBlackbodyEntries - 1));
+  return imin((int)rintf(t * ((float)(n - 1) / (float)(kBlackbodyEntries - 1))), n - 1);
 }
 
 // RGBtoHSP of blackbody entry k (BT/MakeImageKernel.cu:298-301).
@@ -296,7 +302,7 @@ BT_HD StarHit star_hit(const PixelStars& P, const StarSet& S, int q, float st,
   h.st = st;
   h.sp = sp;
   h.part = S.mag[2 * q] + P.red;
-  h.bb = blackbody_index(S.mag[2 * q + 1], P.redshft);
+  h.bb = blackbody_index(S.mag[2 * q + 1], P.redshft, S.bb_n);
   const float4 c = S.bb_hsp[h.bb];
   h.hsp = make_float3(c.x, c.y, c.z);
   return h;

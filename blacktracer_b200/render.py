@@ -86,6 +86,13 @@ def _device_view(ptr, shape, dtype):
     return torch.as_tensor(_Arr(), device="cuda")
 
 
+def psf_airy(size=33, first_zero=4.0):
+    """An Airy diffraction sprite (size, size, 3) uint8, RGB (bt_psf_airy)."""
+    out = np.empty((size, size, 3), dtype=np.uint8)
+    L.check(L.lib().bt_psf_airy(int(size), float(first_zero), out.ctypes.data))
+    return out
+
+
 class StarProcessor:
     """BT/StarProcessor.h: a star list arranged in the reference's binary
     tree (starPos, starMag, binaryStarTree) and uploaded to the device."""
@@ -143,28 +150,19 @@ class Renderer:
 
     def render(self, grid: Grid, viewer: Viewer, cam: Camera, env: Environment | None = None,
                stars: StarProcessor | None = None, lr=True, step=1, diffraction=False,
-               hor=0.0, ver=0.0, out=None, stream=None):
-        """Returns (or fills) an (H, W, 4) uint8 BGRA CUDA tensor."""
-        torch = _torch()
+               hor=0.0, ver=0.0, out=None, stream=None, bb_table=0, psf_scale=False):
+        """Returns (or fills) an (H, W, 4) uint8 BGRA CUDA tensor.  bb_table=1
+        selects the 1024-entry FP32 blackbody table, psf_scale scales the
+        diffraction footprint by sqrt(pixel magnification)."""
         gp, rows, cols, _ = grid.map_grid()
-        if out is None:
-            out = torch.empty((self.height, self.width, 4), dtype=torch.uint8, device="cuda")
-        f = L.bt_frame()
-        f.grid, f.grid_rows, f.grid_cols, f.grid_level = gp, rows, cols, grid.MAXLEVEL
-        f.view = viewer.viewMatrix.data_ptr()
-        f.hor, f.ver = hor, ver
-        f.cam[:] = [float(x) for x in cam.getParamArray()]
-        f.env = env._h if env is not None else None
-        f.stars = stars._h if stars is not None else None
-        f.map, f.star, f.lr = int(env is not None), int(stars is not None), int(bool(lr))
-        f.step, f.diffraction = int(step), int(bool(diffraction))
-        f.out = out.data_ptr()
-        L.check(L.lib().bt_map_render(self._h, C.byref(f), _stream_ptr(stream)))
-        return out
+        return self.render_raw(gp, rows, cols, grid.MAXLEVEL, viewer.viewMatrix,
+                               cam.getParamArray(), env=env, stars=stars, lr=lr, step=step,
+                               diffraction=diffraction, hor=hor, ver=ver, out=out,
+                               stream=stream, bb_table=bb_table, psf_scale=psf_scale)
 
     def render_raw(self, grid_ptr, grid_rows, grid_cols, grid_level, view, cam7, env=None,
                    stars=None, lr=True, step=1, diffraction=False, hor=0.0, ver=0.0,
-                   out=None, stream=None):
+                   out=None, stream=None, bb_table=0, psf_scale=False):
         """The same from a raw float2 grid (device pointer) and 7 camera floats."""
         torch = _torch()
         if out is None:
@@ -178,6 +176,7 @@ class Renderer:
         f.stars = stars._h if stars is not None else None
         f.map, f.star, f.lr = int(env is not None), int(stars is not None), int(bool(lr))
         f.step, f.diffraction = int(step), int(bool(diffraction))
+        f.bb_table, f.psf_scale = int(bb_table), int(bool(psf_scale))
         f.out = out.data_ptr()
         L.check(L.lib().bt_map_render(self._h, C.byref(f), _stream_ptr(stream)))
         return out
@@ -194,6 +193,7 @@ class Renderer:
             bh=_device_view(b.bh, (H * W,), torch.uint8),
             area=_device_view(b.area, (H * W,), torch.float32),
             light=_device_view(b.light, (H * W * 3,), torch.float32),
+            light_diffracted=_device_view(b.light_diffracted, (H * W * 3,), torch.float32),
             env_img=_device_view(b.env_img, (H * W * 4,), torch.uint8))
 
     def __del__(self):

@@ -344,7 +344,20 @@ typedef struct bt_frame {
   int32_t step;           /* splat half-width, 0..2 (the reference uses 1)  */
   int32_t diffraction;    /* scatter the sprite around saturated stars      */
   uint8_t* out;           /* H*W BGRA8                                      */
+  /* Extensions (0 = the reference's behaviour): */
+  int32_t bb_table;       /* 1: 1024-entry FP32 blackbody table (1000-40000 K,
+                             interpolated from the reference's 391 entries)  */
+  int32_t psf_scale;      /* 1: diffraction footprint scaled by the square
+                             root of the pixel's lensing magnification, total
+                             sprite energy kept                              */
 } bt_frame;
+
+/* An Airy diffraction sprite (size x size RGB8, the layout the reference
+ * loads its diffraction image in, BT/MakeImageKernel.cu:1281-1286):
+ * I = (2 J1(x)/x)^2 with the first dark ring at `first_zero` pixels for
+ * 550 nm, scaled per channel by wavelength (R 610, G 550, B 465 nm), 255 at
+ * the centre.  For bt_stars_create's psf_rgb. */
+int bt_psf_airy(int size, float first_zero, uint8_t* rgb);
 int bt_map_render(bt_map* m, const bt_frame* f, void* stream);
 
 /* Device pointers into a renderer's scratch after a frame (for tests and
@@ -358,6 +371,7 @@ typedef struct bt_map_buffers {
   const float* light;
   const uint8_t* stars_img;
   const uint8_t* env_img;
+  const float* light_diffracted;  /* star light after diffraction (3 floats) */
 } bt_map_buffers;
 int bt_map_scratch(const bt_map* m, bt_map_buffers* b);
 
