@@ -46,6 +46,11 @@ struct bt_stars {
   float4* bb;    // 2 * kBlackbodyEntries: HSP, then RGB at unit brightness
   float4* bb1k;  // the same for the 1024-entry FP32 table
   uchar3* psf;
+  short2* psf_nzoff;
+  float4* psf_nzval;
+  short2* psf_lvoff;
+  float4* psf_lvval;
+  int* psf_lvstart;
 };
 
 namespace bt {
@@ -549,55 +554,126 @@ __global__ void k_diff_scatter(const float* __restrict__ light, float* acc,
   }
 }
 
-// Diffraction with the sprite's footprint scaled by s = sqrt(magnification)
-// of the bright pixel (magnification = the pixel's camera-sky area over its
-// celestial solid angle, as lensing uses), s clamped to [0.25, 4]: the
-// sprite is sampled bilinearly at (offset / s) and divided by s^2, so a
-// pixel's total diffracted light is the unscaled sprite's.  Otherwise as
-// k_diff_scatter (snapshot reads, the reference's amplitude and clamp).
-__global__ void k_diff_scatter_scaled(const float* __restrict__ light, float* acc,
-                                      const uint32_t* __restrict__ list, const uint32_t* count,
-                                      int M, int N, const uchar3* __restrict__ psf, int fs,
-                                      const float2* __restrict__ view,
-                                      const float* __restrict__ area) {
-  const uint32_t n = *count;
-  for (uint32_t b = blockIdx.x; b < n; b += gridDim.x) {
-    const uint32_t ij = list[b];
-    const int i = ij / M, j = ij % M;
-    const int M1 = M + 1, ind = i * M1 + j;
-    float ver4[4] = {view[ind].x, view[ind + 1].x, view[ind + M1 + 1].x, view[ind + M1].x};
-    float hor4[4] = {view[ind].y, view[ind + 1].y, view[ind + M1 + 1].y, view[ind + M1].y};
-    const float sa = area[ij];
-    const float mag = sa > 0.f ? calc_area(ver4, hor4) / sa : 1.f;
-    const float sc = fminf(4.f, fmaxf(0.25f, sqrtf(fmaxf(mag, 0.f))));
-    const int fe = 2 * (int)ceilf(0.5f * fs * sc) + 1;  // odd footprint
-    const int fh = fe / 2;
-    const float lx = light[3 * ij], ly = light[3 * ij + 1], lz = light[3 * ij + 2];
-    const float mxv = fmaxf(fmaxf(lx, ly), lz);
-    const float div = 10000 * powf(mxv, 0.6) * sc * sc;
-    const float c0 = 0.5f * (fs - 1);
-    for (int c = threadIdx.x; c < fe * fe; c += blockDim.x) {
-      const int q = c / fe, p = c % fe;
-      const int ti = i - fh + q;
-      if (ti < 0 || ti >= N) continue;
-      const float u = (q - fh) / sc + c0, v = (p - fh) / sc + c0;
-      if (u < 0.f || v < 0.f || u > fs - 1 || v > fs - 1) continue;
-      const int u0 = min((int)u, fs - 2), v0 = min((int)v, fs - 2);
-      const float fu = u - u0, fv = v - v0;
-      const uchar3 a00 = psf[u0 * fs + v0], a01 = psf[u0 * fs + v0 + 1];
-      const uchar3 a10 = psf[(u0 + 1) * fs + v0], a11 = psf[(u0 + 1) * fs + v0 + 1];
-      const float w00 = (1 - fu) * (1 - fv), w01 = (1 - fu) * fv, w10 = fu * (1 - fv),
-                  w11 = fu * fv;
-      const float dxs = w00 * a00.x + w01 * a01.x + w10 * a10.x + w11 * a11.x;
-      const float dys = w00 * a00.y + w01 * a01.y + w10 * a10.y + w11 * a11.y;
-      const float dzs = w00 * a00.z + w01 * a01.z + w10 * a10.z + w11 * a11.z;
-      const float dx = lx / div * dxs, dy = ly / div * dys, dz = lz / div * dzs;
-      const size_t t = (size_t)ti * M + (j - fh + p + 64 * (size_t)M) % M;
-      atomicAdd(&acc[3 * t], fminf(65025.f, dx * dx));
-      atomicAdd(&acc[3 * t + 1], fminf(65025.f, dy * dy));
-      atomicAdd(&acc[3 * t + 2], fminf(65025.f, dz * dz));
-    }
+// Diffraction as a gather (addDiffraction, BT/MakeImageKernel.cu:775-800,
+// with snapshot reads).  A bright pixel (any channel of its summed star light
+// above 65025) adds min(65025, (light / (10000 max^0.6) * sprite)^2) per
+// channel around itself; written from the receiving side, pixel t gathers
+// that term from every bright pixel t - o for the sprite's non-zero offsets
+// o.  Pass 1 stores each pixel's coefficient light / (10000 max^0.6) (zero
+// for the others); pass 2 reads a tile of coefficients with its halo from
+// shared memory.  No atomics: the frame is deterministic.  The reference's
+// arithmetic per term is kept (coefficient times sprite value, squared,
+// clamped); only the summation order differs.
+__global__ void k_diff_coef(const float* __restrict__ light, int n, float3* __restrict__ coef) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const float lx = light[3 * q], ly = light[3 * q + 1], lz = light[3 * q + 2];
+  const float m = fmaxf(fmaxf(lx, ly), lz);
+  float3 c = make_float3(0.f, 0.f, 0.f);
+  if (m > 65025.f) {
+    const float div = 10000 * powf(m, 0.6);
+    c = make_float3(lx / div, ly / div, lz / div);
   }
+  coef[q] = c;
+}
+
+constexpr int kDiffTX = 32, kDiffTY = 8;
+
+// Loads the coefficient tile of a kDiffTX x kDiffTY output tile with a halo
+// of H on every side into shared memory (rows outside the image: zero;
+// columns wrap around the sphere).
+__device__ __forceinline__ void load_coef_tile(const float3* __restrict__ coef, int M, int N,
+                                               int i0, int j0, int H, float3* tile,
+                                               int ty = kDiffTY) {
+  const int TW = kDiffTX + 2 * H, TH = ty + 2 * H;
+  const int tid = threadIdx.y * kDiffTX + threadIdx.x;
+  for (int k = tid; k < TW * TH; k += kDiffTX * ty) {
+    const int r = k / TW, c = k % TW;
+    const int i = i0 - H + r;
+    const int j = ((j0 - H + c) % M + M) % M;
+    tile[k] = (i >= 0 && i < N) ? coef[(size_t)i * M + j] : make_float3(0.f, 0.f, 0.f);
+  }
+}
+
+__global__ void __launch_bounds__(kDiffTX * kDiffTY)
+k_diff_gather(const float3* __restrict__ coef, const float* __restrict__ light,
+              float* __restrict__ out, int M, int N, const short2* __restrict__ nzoff,
+              const float4* __restrict__ nzval, int nnz, int H) {
+  extern __shared__ float3 tile[];
+  const int i0 = blockIdx.y * kDiffTY, j0 = blockIdx.x * kDiffTX;
+  load_coef_tile(coef, M, N, i0, j0, H, tile);
+  __syncthreads();
+  const int ti = i0 + threadIdx.y, tj = j0 + threadIdx.x;
+  if (ti >= N || tj >= M) return;
+  const int TW = kDiffTX + 2 * H;
+  const int base = (threadIdx.y + H) * TW + threadIdx.x + H;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  for (int k = 0; k < nnz; k++) {
+    const short2 o = nzoff[k];  // source = target - offset
+    const float3 c = tile[base - o.x * TW - o.y];
+    if (c.x == 0.f && c.y == 0.f && c.z == 0.f) continue;
+    const float4 v = nzval[k];
+    const float dx = c.x * v.x, dy = c.y * v.y, dz = c.z * v.z;
+    ax += fminf(65025.f, dx * dx);
+    ay += fminf(65025.f, dy * dy);
+    az += fminf(65025.f, dz * dz);
+  }
+  const size_t t = (size_t)ti * M + tj;
+  out[3 * t] = light[3 * t] + ax;
+  out[3 * t + 1] = light[3 * t + 1] + ay;
+  out[3 * t + 2] = light[3 * t + 2] + az;
+}
+
+// Footprint scale levels of the scaled gather: s_k = 0.25 * 2^(k/8).
+constexpr int kPsfLevels = 33;
+// Its output tiles are 32 x 32 (1024 threads): the halo of the largest
+// footprints (~45 pixels) is shared by four times the pixels of a 32 x 8
+// tile, and an SM keeps 32 warps resident.
+constexpr int kDiffTYS = 32;
+
+// The same with the sprite's footprint scaled at the receiving pixel by
+// s = sqrt(magnification) (its camera-sky area over its celestial solid
+// angle, as lensing uses), s clamped to [0.25, 4] and rounded to the nearest
+// level s_k (9% steps): the term from offset o is the sprite sampled
+// bilinearly at (centre + o / s_k) divided by s_k^2 -- a scale keeps the
+// sprite's total light -- read from the level's precomputed entries.
+__global__ void __launch_bounds__(kDiffTX * kDiffTYS)
+k_diff_gather_scaled(const float3* __restrict__ coef, const float* __restrict__ light,
+                     float* __restrict__ out, int M, int N, const short2* __restrict__ lvoff,
+                     const float4* __restrict__ lvval, const int* __restrict__ lvstart,
+                     int maxlevel, int H, const float2* __restrict__ view,
+                     const float* __restrict__ area) {
+  extern __shared__ float3 tile[];
+  const int i0 = blockIdx.y * kDiffTYS, j0 = blockIdx.x * kDiffTX;
+  load_coef_tile(coef, M, N, i0, j0, H, tile, kDiffTYS);
+  __syncthreads();
+  const int ti = i0 + threadIdx.y, tj = j0 + threadIdx.x;
+  if (ti >= N || tj >= M) return;
+  const size_t t = (size_t)ti * M + tj;
+  const int M1 = M + 1, ind = ti * M1 + tj;
+  float ver4[4] = {view[ind].x, view[ind + 1].x, view[ind + M1 + 1].x, view[ind + M1].x};
+  float hor4[4] = {view[ind].y, view[ind + 1].y, view[ind + M1 + 1].y, view[ind + M1].y};
+  const float sa = area[t];
+  const float mag = sa > 0.f ? calc_area(ver4, hor4) / sa : 1.f;
+  // level of s = sqrt(mag): k = 8 log2(s / 0.25) = 4 log2(mag) + 16
+  const float kf = mag > 0.f ? 4.f * log2f(mag) + 16.f : 0.f;
+  const int k = imin(maxlevel, imax(0, (int)rintf(kf == kf ? kf : 16.f)));
+  const int TW = kDiffTX + 2 * H;
+  const int base = (threadIdx.y + H) * TW + threadIdx.x + H;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  for (int e = lvstart[k]; e < lvstart[k + 1]; e++) {
+    const short2 o = lvoff[e];
+    const float3 c = tile[base - o.x * TW - o.y];
+    if (c.x == 0.f && c.y == 0.f && c.z == 0.f) continue;
+    const float4 v = lvval[e];
+    const float dx = c.x * v.x, dy = c.y * v.y, dz = c.z * v.z;
+    ax += fminf(65025.f, dx * dx);
+    ay += fminf(65025.f, dy * dy);
+    az += fminf(65025.f, dz * dz);
+  }
+  out[3 * t] = light[3 * t] + ax;
+  out[3 * t + 1] = light[3 * t + 1] + ay;
+  out[3 * t + 2] = light[3 * t + 2] + az;
 }
 
 // makePix + composite from a light buffer (after diffraction).
@@ -673,18 +749,46 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   }
   k_star_gather<false><<<grid2(M, N), dim3(TX, TY), 0, s>>>(
       Sc.cells, Sc.flag, M, N, F.step, Sc.light, nullptr, nullptr, F.map);
-  BT_CUDA_TRY(cudaMemcpyAsync(Sc.light2, Sc.light, np * 3 * sizeof(float),
-                              cudaMemcpyDeviceToDevice, s));
-  BT_CUDA_TRY(cudaMemsetAsync(Sc.diff_count, 0, sizeof(uint32_t), s));
-  k_diff_mark<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(Sc.light, (int)np,
-                                                          Sc.diff_list, Sc.diff_count);
-  if (F.psf_scale)
-    k_diff_scatter_scaled<<<sm_count() * 8, 256, 0, s>>>(Sc.light, Sc.light2, Sc.diff_list,
-                                                         Sc.diff_count, M, N, SS.psf,
-                                                         SS.psf_size, F.view, Sc.area);
-  else
+  // the star cells are consumed: their buffer holds the coefficients
+  float3* coef = Sc.cells;
+  k_diff_coef<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(Sc.light, (int)np, coef);
+  const dim3 dgrid((unsigned)((M + kDiffTX - 1) / kDiffTX), (unsigned)((N + kDiffTY - 1) / kDiffTY));
+  const dim3 dblock(kDiffTX, kDiffTY);
+  constexpr int kMaxHalo = 52;  // (8 + 104) x (32 + 104) float3 = 183 KB of shared memory
+  auto tile_bytes = [](int H, int ty = kDiffTY) {
+    return (size_t)(kDiffTX + 2 * H) * (ty + 2 * H) * sizeof(float3);
+  };
+  if (F.psf_scale && SS.psf_lvstart) {
+    // the highest level whose footprint fits the shared-memory halo
+    int maxlevel = kPsfLevels - 1;
+    while (maxlevel > 0 &&
+           (int)ceilf(imax(1, SS.psf_rnz) * 0.25f * exp2f(maxlevel / 8.f)) + 1 > kMaxHalo)
+      maxlevel--;
+    const int H = imin(kMaxHalo, (int)ceilf(imax(1, SS.psf_rnz) * 0.25f * exp2f(maxlevel / 8.f)) + 1);
+    BT_CUDA_TRY(cudaFuncSetAttribute(k_diff_gather_scaled,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tile_bytes(H, kDiffTYS)));
+    const dim3 sgrid((unsigned)((M + kDiffTX - 1) / kDiffTX),
+                     (unsigned)((N + kDiffTYS - 1) / kDiffTYS));
+    k_diff_gather_scaled<<<sgrid, dim3(kDiffTX, kDiffTYS), tile_bytes(H, kDiffTYS), s>>>(
+        coef, Sc.light, Sc.light2, M, N, SS.psf_lvoff, SS.psf_lvval, SS.psf_lvstart, maxlevel,
+        H, F.view, Sc.area);
+  } else if (SS.psf_rnz <= kMaxHalo) {
+    const int H = imax(1, SS.psf_rnz);
+    BT_CUDA_TRY(cudaFuncSetAttribute(k_diff_gather, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tile_bytes(kMaxHalo)));
+    k_diff_gather<<<dgrid, dblock, tile_bytes(H), s>>>(coef, Sc.light, Sc.light2, M, N,
+                                                       SS.psf_nzoff, SS.psf_nzval, SS.psf_nnz, H);
+  } else {
+    // sprites wider than the shared-memory halo: scatter with atomics
+    BT_CUDA_TRY(cudaMemcpyAsync(Sc.light2, Sc.light, np * 3 * sizeof(float),
+                                cudaMemcpyDeviceToDevice, s));
+    BT_CUDA_TRY(cudaMemsetAsync(Sc.diff_count, 0, sizeof(uint32_t), s));
+    k_diff_mark<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(Sc.light, (int)np, Sc.diff_list,
+                                                            Sc.diff_count);
     k_diff_scatter<<<sm_count() * 8, 256, 0, s>>>(Sc.light, Sc.light2, Sc.diff_list,
                                                   Sc.diff_count, M, N, SS.psf, SS.psf_size);
+  }
   k_makepix<<<grid2(M, N), dim3(TX, TY), 0, s>>>(Sc.light2, M, N,
                                                  (const uchar4*)F.out_bg,
                                                  (uchar4*)F.out, F.map);
@@ -864,8 +968,75 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
     k_blackbody_tables_1k<<<kBlackbody1k / 128, 128, 0, s>>>(st->bb1k);
     e = cudaGetLastError();
   }
+  // the sprite's non-zero entries, offsets from its centre (index size/2)
+  std::vector<short2> nzoff;
+  std::vector<float4> nzval;
+  int rnz = 0;
+  for (int q = 0; q < psf_size; q++)
+    for (int p = 0; p < psf_size; p++) {
+      const uint8_t* v = psf_rgb + ((size_t)q * psf_size + p) * 3;
+      if (!v[0] && !v[1] && !v[2]) continue;
+      const int dq = q - psf_size / 2, dp = p - psf_size / 2;
+      nzoff.push_back(make_short2((short)dq, (short)dp));
+      nzval.push_back(make_float4((float)v[0], (float)v[1], (float)v[2], 0.f));
+      rnz = std::max(rnz, std::max(std::abs(dq), std::abs(dp)));
+    }
+  // resampled levels for the magnification-scaled footprint
+  std::vector<short2> lvoff;
+  std::vector<float4> lvval;
+  std::vector<int> lvstart(1, 0);
+  if (psf_size >= 2) {
+    const float c0 = (float)(psf_size / 2);
+    auto px = [&](int q, int p, int ch) {
+      return (float)psf_rgb[((size_t)q * psf_size + p) * 3 + ch];
+    };
+    for (int k = 0; k < kPsfLevels; k++) {
+      const float sc = 0.25f * std::exp2((float)k / 8.f), is = 1.f / sc;
+      const int R = (int)std::ceil(std::max(1, rnz) * sc) + 1;
+      for (int dq = -R; dq <= R; dq++)
+        for (int dp = -R; dp <= R; dp++) {
+          const float u = c0 + dq * is, v = c0 + dp * is;
+          if (u < 0.f || v < 0.f || u > psf_size - 1 || v > psf_size - 1) continue;
+          const int u0 = std::min((int)u, psf_size - 2), v0 = std::min((int)v, psf_size - 2);
+          const float fu = u - u0, fv = v - v0;
+          float val[3];
+          for (int ch = 0; ch < 3; ch++)
+            val[ch] = ((1 - fu) * (1 - fv) * px(u0, v0, ch) + (1 - fu) * fv * px(u0, v0 + 1, ch) +
+                       fu * (1 - fv) * px(u0 + 1, v0, ch) + fu * fv * px(u0 + 1, v0 + 1, ch)) *
+                      is * is;
+          if (val[0] == 0.f && val[1] == 0.f && val[2] == 0.f) continue;
+          lvoff.push_back(make_short2((short)dq, (short)dp));
+          lvval.push_back(make_float4(val[0], val[1], val[2], 0.f));
+        }
+      lvstart.push_back((int)lvoff.size());
+    }
+  }
   if (e == cudaSuccess && psf_size)
     e = cudaMalloc((void**)&st->psf, (size_t)psf_size * psf_size * 3);
+  if (e == cudaSuccess && !lvoff.empty()) {
+    e = cudaMalloc((void**)&st->psf_lvoff, lvoff.size() * sizeof(short2));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&st->psf_lvval, lvval.size() * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&st->psf_lvstart, lvstart.size() * sizeof(int));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(st->psf_lvoff, lvoff.data(), lvoff.size() * sizeof(short2),
+                          cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(st->psf_lvval, lvval.data(), lvval.size() * sizeof(float4),
+                          cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(st->psf_lvstart, lvstart.data(), lvstart.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, s);
+  }
+  if (e == cudaSuccess && !nzoff.empty())
+    e = cudaMalloc((void**)&st->psf_nzoff, nzoff.size() * sizeof(short2));
+  if (e == cudaSuccess && !nzoff.empty())
+    e = cudaMalloc((void**)&st->psf_nzval, nzval.size() * sizeof(float4));
+  if (e == cudaSuccess && !nzoff.empty())
+    e = cudaMemcpyAsync(st->psf_nzoff, nzoff.data(), nzoff.size() * sizeof(short2),
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !nzoff.empty())
+    e = cudaMemcpyAsync(st->psf_nzval, nzval.data(), nzval.size() * sizeof(float4),
+                        cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(st->box, box.data(), box.size() * sizeof(float4),
                         cudaMemcpyHostToDevice, s);
@@ -884,6 +1055,8 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   if (e != cudaSuccess) {
     cudaFree(st->pos); cudaFree(st->mag); cudaFree(st->tree); cudaFree(st->box);
     cudaFree(st->bb); cudaFree(st->bb1k); cudaFree(st->psf);
+    cudaFree(st->psf_nzoff); cudaFree(st->psf_nzval);
+    cudaFree(st->psf_lvoff); cudaFree(st->psf_lvval); cudaFree(st->psf_lvstart);
     delete st;
     set_error("star set upload failed: %s", cudaGetErrorString(e));
     return BT_ERR_CUDA;
@@ -899,6 +1072,13 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   st->s.bb_n = kBlackbodyEntries;
   st->s.psf = st->psf;
   st->s.psf_size = psf_size;
+  st->s.psf_nzoff = st->psf_nzoff;
+  st->s.psf_nzval = st->psf_nzval;
+  st->s.psf_nnz = (int)nzoff.size();
+  st->s.psf_rnz = rnz;
+  st->s.psf_lvoff = st->psf_lvoff;
+  st->s.psf_lvval = st->psf_lvval;
+  st->s.psf_lvstart = st->psf_lvstart;
   *out = st;
   return BT_OK;
 }
@@ -912,6 +1092,11 @@ void bt_stars_destroy(bt_stars* st) {
   cudaFree(st->bb);
   cudaFree(st->bb1k);
   if (st->psf) cudaFree(st->psf);
+  cudaFree(st->psf_nzoff);
+  cudaFree(st->psf_nzval);
+  cudaFree(st->psf_lvoff);
+  cudaFree(st->psf_lvval);
+  cudaFree(st->psf_lvstart);
   delete st;
 }
 

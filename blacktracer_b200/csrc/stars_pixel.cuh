@@ -21,6 +21,17 @@ struct StarSet {
   const int* tree;   // 2^(treeLevel+1)-1 cumulative counts
   const uchar3* psf; // diffraction sprite, psf_size^2 (may be NULL)
   int psf_size;
+  // The sprite's non-zero entries: offsets from its centre (row, column)
+  // and values, in row-major order; psf_rnz = their largest |offset|.
+  const short2* psf_nzoff;
+  const float4* psf_nzval;
+  int psf_nnz, psf_rnz;
+  // The sprite resampled at footprint scales s_k = 0.25 * 2^(k/8), k = 0..32:
+  // entry values = bilinear sample at (centre + offset / s_k) / s_k^2, non-zero
+  // entries only, level k at [lvl_start[k], lvl_start[k + 1]).
+  const short2* psf_lvoff;
+  const float4* psf_lvval;
+  const int* psf_lvstart;
   // Per blackbody entry: RGBtoHSP of its colour (h, s, p) and
   // 255 * HSPtoRGB(h, s, p), computed once on the device by the same code.
   // bb_n = 391: the reference's table (100 K steps, index floor(temp));
