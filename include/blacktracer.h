@@ -348,8 +348,9 @@ typedef struct bt_frame {
   int32_t bb_table;       /* 1: 1024-entry FP32 blackbody table (1000-40000 K,
                              interpolated from the reference's 391 entries)  */
   int32_t psf_scale;      /* 1: diffraction footprint scaled by the square
-                             root of the pixel's lensing magnification, total
-                             sprite energy kept                              */
+                             root of the lensing magnification at the
+                             receiving pixel (clamped to [0.25, 4], rounded
+                             to 33 levels 9% apart), total sprite light kept */
 } bt_frame;
 
 /* An Airy diffraction sprite (size x size RGB8, the layout the reference
