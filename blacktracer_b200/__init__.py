@@ -12,7 +12,7 @@ from ._lib import (BtError, PRECISION_FAST, PRECISION_MIXED, PRECISION_PLAIN,  #
 from .host import (BlackHole, Camera, Grid, GridSet, IntegOpts, grid_dims,  # noqa: F401
                    integrate_rays, integrate_rays_host)
 
-from .render import Environment, Renderer, StarProcessor, Viewer, psf_airy  # noqa: F401
+from .render import Blend, Environment, Renderer, StarProcessor, Viewer, psf_airy  # noqa: F401
 from .serve import Server  # noqa: F401
 
 __all__ = ["Environment", "Renderer", "Server", "StarProcessor", "Viewer", "BlackHole",

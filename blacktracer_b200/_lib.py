@@ -94,7 +94,9 @@ class bt_frame(C.Structure):
                 ("ver", C.c_float), ("cam", C.c_float * 7), ("env", C.c_void_p),
                 ("stars", C.c_void_p), ("map", C.c_int32), ("star", C.c_int32),
                 ("lr", C.c_int32), ("step", C.c_int32), ("diffraction", C.c_int32),
-                ("out", C.c_void_p), ("bb_table", C.c_int32), ("psf_scale", C.c_int32)]
+                ("out", C.c_void_p), ("bb_table", C.c_int32), ("psf_scale", C.c_int32),
+                ("grid2", C.c_void_p), ("alpha", C.c_float), ("cam2", C.c_float * 7),
+                ("blend", C.c_void_p)]
 
 
 class bt_map_buffers(C.Structure):
@@ -150,6 +152,11 @@ _SIGS = {
     "bt_env_sat": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "bt_stars_tree_size": (C.c_int, [C.c_int]),
     "bt_psf_airy": (C.c_int, [C.c_int, C.c_float, _vp]),
+    "bt_blend_create": (C.c_int, [C.POINTER(_vp)]),
+    "bt_blend_destroy": (None, [_vp]),
+    "bt_blend_prepare": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp]),
+    "bt_blend_info": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int32),
+                                C.POINTER(C.c_uint32)]),
     "bt_stars_build_tree": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, C.c_float,
                                       _vp, _vp, _vp, C.POINTER(C.c_int)]),
     "bt_stars_create": (C.c_int, [_vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int,

@@ -52,6 +52,157 @@ __global__ void k_pixinterp(const float2* __restrict__ view, int M, int N,
   gap[(size_t)i * M1 + j] = g;
 }
 
+// ---------------------------------------------------------- G = 2 blending
+// Interpolation between two grids computed for neighbouring camera poses
+// (the reference's movement between precomputed grids, BT/MakeImageKernel.cu
+// camUpdate / findBhCenter / findBhBorders / smoothBorder :386-456 and the
+// Gr > 1 branch of pixInterpolation :466-510).  The border of the black hole
+// is found in both grids along kBlendAngles directions from the centre of the
+// captured region; near the black hole each grid is read at a position
+// stretched towards its own border so that the shadow moves smoothly.
+
+// findBhCenter (:391-404): bounding box (in radians) of the captured
+// vertices of either grid.  box = {theta_min, theta_max}, {phi_min, phi_max};
+// the values are non-negative, so float order equals their bits' int order.
+__global__ void k_bh_center(const float2* __restrict__ ga, const float2* __restrict__ gb,
+                            int GM, int GN, float2* box) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  if (i >= GN || j >= GM) return;
+  const size_t q = (size_t)i * GM + j;
+  if (ga[q].x == -1.f || gb[q].x == -1.f) {
+    const float gridsize = PI / (1.f * GN);
+    atomicMin((int*)&box[0].x, __float_as_int(gridsize * (float)i));
+    atomicMax((int*)&box[0].y, __float_as_int(gridsize * (float)i));
+    atomicMin((int*)&box[1].x, __float_as_int(gridsize * (float)j));
+    atomicMax((int*)&box[1].y, __float_as_int(gridsize * (float)j));
+  }
+}
+
+// findBhBorders (:406-430): from the centre of the box, walk outwards in
+// lattice steps along direction k until a vertex with theta > 0 follows a
+// captured one (-1); thread 2k walks grid a, 2k+1 grid b.  The reference's
+// walk has no bound (and reads past the lattice when it misses the border);
+// here it stops at the lattice edge, and such walks are counted in *edge.
+__global__ void k_bh_borders(const float2* __restrict__ ga, const float2* __restrict__ gb,
+                             int GM, int GN, int nang, float2* border, uint32_t* edge) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nang * 2) return;
+  const int ii = i / 2;
+  const float2* g = (i % 2) ? gb : ga;
+  const float angle = PI2 / (1.f * nang) * 1.f * ii;
+  const float thetaChange = -sinf(angle);
+  const float phiChange = cosf(angle);
+  float2 pt = {.5f * border[0].x + .5f * border[0].y, .5f * border[1].x + .5f * border[1].y};
+  pt = {pt.x / PI2 * GM, pt.y / PI2 * GM};
+  float2 gridB = {-2, -2}, gridA = {-2, -2};
+  const int cap = 4 * (GM + GN);
+  int it = 0;
+  while (!(gridA.x > 0 && gridB.x == -1)) {
+    gridB = gridA;
+    pt.x += thetaChange;
+    pt.y += phiChange;
+    const int gx = int(pt.x), gy = int(pt.y);
+    if (gx < 0 || gy < 0 || gx >= GN || gy >= GM || ++it > cap) {
+      atomicAdd(edge, 1u);
+      break;
+    }
+    gridA = g[(size_t)gx * GM + gy];
+  }
+  border[2 + i] = {(pt.x - thetaChange) * PI2 / (1.f * GM), (pt.y - phiChange) * PI2 / (1.f * GM)};
+}
+
+// smoothBorder (:444-456): each border point averaged with its two
+// neighbours of the same grid.
+__global__ void k_smooth_border(const float2* __restrict__ in, float2* __restrict__ out, int nang) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nang * 2) return;
+  if (i == 0) {
+    out[0] = in[0];
+    out[1] = in[1];
+  }
+  const int prev = (i - 2 + 2 * nang) % (2 * nang);
+  const int next = (i + 2) % (2 * nang);
+  out[i + 2] = {1.f / 3.f * (in[prev + 2].x + in[i + 2].x + in[next + 2].x),
+                1.f / 3.f * (in[prev + 2].y + in[i + 2].y + in[next + 2].y)};
+}
+
+// pixInterpolation with Gr > 1 (:466-510): grid a weighted 1 - alpha, grid b
+// alpha; the block gap kept is grid b's (the reference's second call writes
+// it last).
+__global__ void k_pixinterp2(const float2* __restrict__ view, int M, int N, GridRef GA,
+                             GridRef GB, int gridlvl, float hor, float ver,
+                             const float2* __restrict__ bhBorder, int angleNum, float alpha,
+                             float2* __restrict__ thphi, int* __restrict__ gap) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  const int M1 = M + 1;
+  if (i > N || j > M) return;
+  const float2 v = view[(size_t)i * M1 + j];
+  const float theta = v.x + ver;
+  const float phi = fmodf(v.y + hor + PI2, PI2);
+  const size_t q = (size_t)i * M1 + j;
+  float2 A, B;
+  int ga = 0, gb = 0;
+  const float2 center = {.5f * bhBorder[0].x + .5f * bhBorder[0].y,
+                         .5f * bhBorder[1].x + .5f * bhBorder[1].y};
+  const float stretchRad =
+      fmaxf(bhBorder[0].y - bhBorder[0].x, bhBorder[1].x - bhBorder[1].y) * 0.75f;
+  const float centerdist =
+      (theta - center.x) * (theta - center.x) + (phi - center.y) * (phi - center.y);
+  if (centerdist < stretchRad * stretchRad) {
+    float angle = atan2f(center.x - theta, phi - center.y);
+    angle = fmodf(angle + PI2, PI2);
+    const int angleSlot = angle / PI2 * angleNum;
+    const float2 bA = bhBorder[2 * angleSlot + 2], bB = bhBorder[2 * angleSlot + 3];
+    const float2 bhBorderNew = {(1.f - alpha) * bA.x + alpha * bB.x,
+                                (1.f - alpha) * bA.y + alpha * bB.y};
+    if (centerdist <= (bhBorderNew.x - center.x) * (bhBorderNew.x - center.x) +
+                          (bhBorderNew.y - center.y) * (bhBorderNew.y - center.y)) {
+      thphi[q] = {-1, -1};
+      return;
+    }
+    const float tStoB = (center.x - stretchRad * sinf(angle) - bhBorderNew.x);
+    const float pStoB = (center.y + stretchRad * cosf(angle) - bhBorderNew.y);
+    const float thetaPerc = fabsf(tStoB) < 1E-5 ? 0 : 1.f - (theta - bhBorderNew.x) / tStoB;
+    const float phiPerc = fabsf(pStoB) < 1E-5 ? 0 : 1.f - (phi - bhBorderNew.y) / pStoB;
+    const float thetaA = theta - thetaPerc * (bhBorderNew.x - bA.x);
+    const float phiA = phi - phiPerc * (bhBorderNew.y - bA.y);
+    const float thetaB = theta - thetaPerc * (bhBorderNew.x - bB.x);
+    const float phiB = phi - phiPerc * (bhBorderNew.y - bB.y);
+    A = interpolate_pix(GA, thetaA, phiA, gridlvl, ga);
+    B = interpolate_pix(GB, thetaB, phiB, gridlvl, gb);
+  } else {
+    A = interpolate_pix(GA, theta, phi, gridlvl, ga);
+    B = interpolate_pix(GB, theta, phi, gridlvl, gb);
+  }
+  gap[q] = gb;
+  if (A.x == -1 || B.x == -1) {
+    thphi[q] = {-1, -1};
+  } else {
+    if (A.y < .2f * PI2 && B.y > .8f * PI2) A.y += PI2;
+    if (B.y < .2f * PI2 && A.y > .8f * PI2) B.y += PI2;
+    thphi[q] = {(1.f - alpha) * A.x + alpha * B.x, fmodf((1.f - alpha) * A.y + alpha * B.y, PI2)};
+  }
+}
+
+int blend_prepare(const float2* ga, const float2* gb, int GN, int GM, float2* border,
+                  float2* border2, int nang, uint32_t* edge, cudaStream_t s) {
+  // {100, 0} per axis, as the reference initialises its box (:1308-1310)
+  const float2 init[2] = {{100.f, 0.f}, {100.f, 0.f}};
+  BT_CUDA_TRY(cudaMemcpyAsync(border, init, sizeof(init), cudaMemcpyHostToDevice, s));
+  BT_CUDA_TRY(cudaMemsetAsync(edge, 0, sizeof(uint32_t), s));
+  k_bh_center<<<grid2(GM, GN), dim3(TX, TY), 0, s>>>(ga, gb, GM, GN, border);
+  const unsigned nb = (unsigned)((2 * nang + 255) / 256);
+  k_bh_borders<<<nb, 256, 0, s>>>(ga, gb, GM, GN, nang, border, edge);
+  for (int r = 0; r < 2; r++) {
+    k_smooth_border<<<nb, 256, 0, s>>>(border, border2, nang);
+    k_smooth_border<<<nb, 256, 0, s>>>(border2, border, nang);
+  }
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
 // findBlackPixels + findArea (BT/MakeImageKernel.cu:539-568), fused.
 __global__ void k_bh_area(const float2* __restrict__ thphi, int M, int N,
                           uint8_t* __restrict__ bh, float* __restrict__ area) {
@@ -401,8 +552,15 @@ __global__ void k_env_wide(const float2* __restrict__ thphi, uchar4* __restrict_
 int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s) {
   const int M = S.M, N = S.N;
   GridRef G{F.grid, F.GM, F.GN};
-  k_pixinterp<<<grid2(M + 1, N + 1), dim3(TX, TY), 0, s>>>(
-      F.view, M, N, G, F.gridlvl, F.hor, F.ver, S.thphi, S.gap);
+  if (F.grid2) {
+    GridRef G2{F.grid2, F.GM, F.GN};
+    k_pixinterp2<<<grid2(M + 1, N + 1), dim3(TX, TY), 0, s>>>(
+        F.view, M, N, G, G2, F.gridlvl, F.hor, F.ver, F.blend_border, F.blend_angles, F.alpha,
+        S.thphi, S.gap);
+  } else {
+    k_pixinterp<<<grid2(M + 1, N + 1), dim3(TX, TY), 0, s>>>(
+        F.view, M, N, G, F.gridlvl, F.hor, F.ver, S.thphi, S.gap);
+  }
   k_bh_area<<<grid2(M, N), dim3(TX, TY), 0, s>>>(S.thphi, M, N, S.bh, S.area);
   k_smooth_h<<<grid2(M, N), dim3(TX, TY), 0, s>>>(S.area_tmp, S.area, S.bh, S.gap, M, N);
   k_smooth_v<<<grid2(M, N), dim3(TX, TY), 0, s>>>(S.area_tmp, S.area, S.bh, S.gap, M, N);

@@ -97,6 +97,74 @@ int bt_env_sat(const bt_env* e, const float** sat, int32_t* rows, int32_t* cols)
   return BT_OK;
 }
 
+struct bt_blend {
+  float2* border;   // 2 + 2 * nang: the box, then (grid a, grid b) per direction
+  float2* border2;
+  uint32_t* edge;
+  uint32_t* edge_host;
+  int nang;
+  int rows, cols;
+  int ready;
+};
+
+int bt_blend_create(bt_blend** out) {
+  clear_error();
+  BT_ARG_CHECK(out != nullptr, "NULL pointer");
+  *out = nullptr;
+  bt_blend* b = new (std::nothrow) bt_blend;
+  if (!b) return BT_ERR_NOMEM;
+  std::memset(b, 0, sizeof(*b));
+  b->nang = 1000;  // angleNum, BT/MakeImageKernel.cu:1257
+  const size_t bytes = (size_t)(2 + 2 * b->nang) * sizeof(float2);
+  cudaError_t e = cudaMalloc((void**)&b->border, bytes);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->border2, bytes);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&b->edge, sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&b->edge_host, sizeof(uint32_t));
+  if (e != cudaSuccess) {
+    cudaFree(b->border); cudaFree(b->border2); cudaFree(b->edge);
+    delete b;
+    set_error("blend allocation failed: %s", cudaGetErrorString(e));
+    return BT_ERR_NOMEM;
+  }
+  *out = b;
+  return BT_OK;
+}
+
+void bt_blend_destroy(bt_blend* b) {
+  if (!b) return;
+  cudaFree(b->border);
+  cudaFree(b->border2);
+  cudaFree(b->edge);
+  if (b->edge_host) cudaFreeHost(b->edge_host);
+  delete b;
+}
+
+int bt_blend_prepare(bt_blend* b, const float* grid_a, const float* grid_b, int rows, int cols,
+                     void* stream) {
+  clear_error();
+  BT_ARG_CHECK(b && grid_a && grid_b, "NULL pointer");
+  BT_ARG_CHECK(rows > 1 && cols > 1, "invalid grid shape");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (int rc = blend_prepare((const float2*)grid_a, (const float2*)grid_b, rows, cols,
+                             b->border, b->border2, b->nang, b->edge, s))
+    return rc;
+  BT_CUDA_TRY(cudaMemcpyAsync(b->edge_host, b->edge, sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, s));
+  b->rows = rows;
+  b->cols = cols;
+  b->ready = 1;
+  return BT_OK;
+}
+
+int bt_blend_info(const bt_blend* b, const float** border, int32_t* angles,
+                  uint32_t* walks_at_edge) {
+  BT_ARG_CHECK(b != nullptr, "NULL pointer");
+  if (border) *border = (const float*)b->border;
+  if (angles) *angles = b->nang;
+  if (walks_at_edge) *walks_at_edge = b->edge_host ? *b->edge_host : 0;
+  return BT_OK;
+}
+
 int bt_map_create(int width, int height, bt_map** out) {
   clear_error();
   BT_ARG_CHECK(out != nullptr, "NULL pointer");
@@ -165,6 +233,9 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
   BT_ARG_CHECK(!f->star || f->stars, "stars requested without a star set");
   BT_ARG_CHECK(f->step >= 0 && f->step <= 2, "step out of [0, 2]");
   BT_ARG_CHECK(f->bb_table == 0 || f->bb_table == 1, "bb_table must be 0 or 1");
+  BT_ARG_CHECK(!f->grid2 || (f->blend && f->blend->ready && f->blend->rows == f->grid_rows &&
+                             f->blend->cols == f->grid_cols),
+               "a second grid needs a blend prepared on grids of the same shape");
   cudaStream_t s = (cudaStream_t)stream;
   MapFrame F;
   F.grid = (const float2*)f->grid;
@@ -179,6 +250,16 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
   F.stars = f->stars;
   F.bb_table = f->bb_table;
   F.psf_scale = f->psf_scale;
+  F.grid2 = (const float2*)f->grid2;
+  F.blend_border = nullptr;
+  F.blend_angles = 0;
+  F.alpha = f->alpha;
+  if (f->grid2) {
+    // camUpdate (BT/MakeImageKernel.cu:386-389): the camera between the two
+    for (int q = 0; q < 7; q++) F.cam.v[q] = (1.f - f->alpha) * f->cam[q] + f->alpha * f->cam2[q];
+    F.blend_border = f->blend->border;
+    F.blend_angles = f->blend->nang;
+  }
   F.map = f->map;
   F.star = f->star;
   F.lr = f->lr;

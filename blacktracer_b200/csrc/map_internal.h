@@ -52,6 +52,10 @@ struct MapFrame {
   const EnvMap* env;
   const bt_stars* stars;
   int map, star, lr, step, diffraction;
+  const float2* grid2;  // second grid (G = 2 blending) or NULL
+  const float2* blend_border;  // bhBorder of the blend
+  int blend_angles;
+  float alpha;
   int bb_table;         // 0: the reference's 391-entry table, 1: 1024-entry FP32
   int psf_scale;        // diffraction footprint scaled by sqrt(pixel magnification)
   uint8_t* out_bg;      // N*M*4 environment (or final) image
@@ -59,6 +63,8 @@ struct MapFrame {
 };
 
 int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s);
+int blend_prepare(const float2* ga, const float2* gb, int GN, int GM, float2* border,
+                  float2* border2, int nang, uint32_t* edge, cudaStream_t s);
 int map_run_stars(MapScratch& S, const MapFrame& F, cudaStream_t s);
 int launch_view_sphere(float2* view, int W, int H, cudaStream_t s);
 int launch_sat(const uint8_t* bgr, int rows, int cols, float4* sat, cudaStream_t s);

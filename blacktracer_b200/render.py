@@ -93,6 +93,44 @@ def psf_airy(size=33, first_zero=4.0):
     return out
 
 
+class Blend:
+    """Blending between two grids of neighbouring camera poses (bt_blend):
+    prepare(grid_a, grid_b) finds the black hole's border in both; a frame
+    rendered with grid2 / alpha / cam2 / blend then mixes them."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        L.check(L.lib().bt_blend_create(C.byref(h)))
+        self._h = h
+
+    def prepare(self, grid_a, grid_b, stream=None):
+        pa, rows, cols, _ = grid_a.map_grid()
+        pb, rows_b, cols_b, _ = grid_b.map_grid()
+        if (rows, cols) != (rows_b, cols_b):
+            raise ValueError("grids of different shapes")
+        L.check(L.lib().bt_blend_prepare(self._h, pa, pb, rows, cols, _stream_ptr(stream)))
+
+    def info(self):
+        """(border as an (2 + 2*angles, 2) CUDA tensor view, angles, walks
+        that reached the lattice edge); synchronises the device first."""
+        torch = _torch()
+        torch.cuda.synchronize()
+        p = C.c_void_p()
+        n = C.c_int32()
+        e = C.c_uint32()
+        L.check(L.lib().bt_blend_info(self._h, C.byref(p), C.byref(n), C.byref(e)))
+        return _device_view(p.value, (2 + 2 * n.value, 2), torch.float32), n.value, e.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None:
+            try:
+                L.lib().bt_blend_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
 class StarProcessor:
     """BT/StarProcessor.h: a star list arranged in the reference's binary
     tree (starPos, starMag, binaryStarTree) and uploaded to the device."""
@@ -150,19 +188,26 @@ class Renderer:
 
     def render(self, grid: Grid, viewer: Viewer, cam: Camera, env: Environment | None = None,
                stars: StarProcessor | None = None, lr=True, step=1, diffraction=False,
-               hor=0.0, ver=0.0, out=None, stream=None, bb_table=0, psf_scale=False):
+               hor=0.0, ver=0.0, out=None, stream=None, bb_table=0, psf_scale=False,
+               grid2=None, cam2=None, alpha=0.0, blend=None):
         """Returns (or fills) an (H, W, 4) uint8 BGRA CUDA tensor.  bb_table=1
         selects the 1024-entry FP32 blackbody table, psf_scale scales the
-        diffraction footprint by sqrt(pixel magnification)."""
+        diffraction footprint by sqrt(pixel magnification); grid2 / cam2 /
+        alpha / blend (a prepared Blend) mix a second grid in."""
         gp, rows, cols, _ = grid.map_grid()
+        extra = {}
+        if grid2 is not None:
+            extra = dict(grid2=grid2.map_grid()[0], cam2=cam2.getParamArray(), alpha=alpha,
+                         blend=blend)
         return self.render_raw(gp, rows, cols, grid.MAXLEVEL, viewer.viewMatrix,
                                cam.getParamArray(), env=env, stars=stars, lr=lr, step=step,
                                diffraction=diffraction, hor=hor, ver=ver, out=out,
-                               stream=stream, bb_table=bb_table, psf_scale=psf_scale)
+                               stream=stream, bb_table=bb_table, psf_scale=psf_scale, **extra)
 
     def render_raw(self, grid_ptr, grid_rows, grid_cols, grid_level, view, cam7, env=None,
                    stars=None, lr=True, step=1, diffraction=False, hor=0.0, ver=0.0,
-                   out=None, stream=None, bb_table=0, psf_scale=False):
+                   out=None, stream=None, bb_table=0, psf_scale=False, grid2=None,
+                   cam2=None, alpha=0.0, blend=None):
         """The same from a raw float2 grid (device pointer) and 7 camera floats."""
         torch = _torch()
         if out is None:
@@ -177,6 +222,9 @@ class Renderer:
         f.map, f.star, f.lr = int(env is not None), int(stars is not None), int(bool(lr))
         f.step, f.diffraction = int(step), int(bool(diffraction))
         f.bb_table, f.psf_scale = int(bb_table), int(bool(psf_scale))
+        if grid2 is not None:
+            f.grid2, f.alpha, f.blend = grid2, float(alpha), blend._h
+            f.cam2[:] = [float(x) for x in cam2]
         f.out = out.data_ptr()
         L.check(L.lib().bt_map_render(self._h, C.byref(f), _stream_ptr(stream)))
         return out

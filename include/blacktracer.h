@@ -351,7 +351,34 @@ typedef struct bt_frame {
                              root of the lensing magnification at the
                              receiving pixel (clamped to [0.25, 4], rounded
                              to 33 levels 9% apart), total sprite light kept */
+  /* Blending between two grids (the reference's Gr > 1 path): NULL grid2
+   * renders `grid` alone. */
+  const float* grid2;     /* second map grid, same shape as grid            */
+  float alpha;            /* weight of grid2, in [0, 1]                     */
+  float cam2[7];          /* getParamArray of grid2's camera: the frame uses
+                             (1 - alpha) cam + alpha cam2 (camUpdate)       */
+  const struct bt_blend* blend;  /* prepared on (grid, grid2)               */
 } bt_frame;
+
+/* Blending between two grids computed for neighbouring camera poses (the
+ * reference's movement between precomputed grids, BT/MakeImageKernel.cu
+ * camUpdate / findBhCenter / findBhBorders / smoothBorder :386-456 and the
+ * Gr > 1 branch of pixInterpolation :466-510).  bt_blend_prepare finds the
+ * black hole's centre (box of the captured vertices of either grid) and its
+ * border along 1000 directions in each grid, smoothed 4 times; a frame with
+ * grid2 then blends the two grids, stretched towards their borders near the
+ * shadow.  The reference's border walk has no bound; here it stops at the
+ * lattice edge and bt_blend_info reports how many walks did. */
+typedef struct bt_blend bt_blend;
+int bt_blend_create(bt_blend** out);
+void bt_blend_destroy(bt_blend* b);
+int bt_blend_prepare(bt_blend* b, const float* grid_a, const float* grid_b, int rows,
+                     int cols, void* stream);
+/* Device pointer to the border (2 + 2*angles float2: the box, then per
+ * direction grid a's and grid b's point); walks_at_edge is valid once the
+ * prepare's stream has been synchronised. */
+int bt_blend_info(const bt_blend* b, const float** border, int32_t* angles,
+                  uint32_t* walks_at_edge);
 
 /* An Airy diffraction sprite (size x size RGB8, the layout the reference
  * loads its diffraction image in, BT/MakeImageKernel.cu:1281-1286):

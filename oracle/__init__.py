@@ -220,6 +220,9 @@ def _refmaplib():
                                         C.c_int, C.c_int, C.c_int, C.c_int, _f32p, C.c_int,
                                         _f32p, _f32p, _u8p, C.c_void_p]
         lib.btref_map_compose.argtypes = [_u8p, _u8p, _u8p, C.c_int, C.c_int]
+        lib.btref_map_pixinterp_blend.argtypes = [_f32p, C.c_int, C.c_int, _f32p, C.c_int,
+                                                  C.c_int, C.c_int, C.c_float, C.c_float,
+                                                  C.c_float, _f32p, _i32, _f32p]
         _refmap = lib
     return _refmap
 
@@ -236,6 +239,27 @@ def ref_star_tree(theta, phi, mag, bv, tree_level):
     tree = np.empty((1 << (tree_level + 1)) - 1, np.int32)
     lib.btref_star_tree(f(theta), f(phi), f(mag), f(bv), n, tree_level, pos, mg, tree)
     return pos, mg, tree
+
+
+def ref_map_blend(grid_a, grid_b, grid_rows, grid_cols, gridlvl, view, width, height, alpha,
+                  hor=0.0, ver=0.0):
+    """The reference's Gr = 2 corner interpolation (findBhCenter,
+    findBhBorders, smoothBorder x 4, pixInterpolation; BT/MakeImageKernel.cu
+    :391-510) on two map grids stored one after the other, as the reference
+    stores them.  Returns (thphi, gap, border).  Only for grids where every
+    border walk ends inside the lattice (the reference's walk has no bound):
+    check with the device's walk count first."""
+    lib = _refmaplib()
+    g = np.ascontiguousarray(np.concatenate([np.asarray(grid_a, np.float32).reshape(-1, 2),
+                                             np.asarray(grid_b, np.float32).reshape(-1, 2)]))
+    view = np.ascontiguousarray(view, dtype=np.float32)
+    M, N = width, height
+    thphi = np.zeros(((N + 1) * (M + 1), 2), np.float32)
+    gap = np.zeros((N + 1) * (M + 1), np.int32)
+    border = np.zeros((2 + 2 * 1000, 2), np.float32)
+    lib.btref_map_pixinterp_blend(view, M, N, g, grid_cols, grid_rows, gridlvl, hor, ver, alpha,
+                                  thphi, gap, border)
+    return thphi, gap, border
 
 
 def ref_map_frame(grid_f2, grid_rows, grid_cols, gridlvl, view, width, height, cam7,

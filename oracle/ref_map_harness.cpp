@@ -87,6 +87,48 @@ void btref_map_pixinterp(const float* view, int M, int N, const float* grid,
     }
 }
 
+// The Gr = 2 path: findBhCenter, findBhBorders, smoothBorder x 4
+// (BT/MakeImageKernel.cu:391-456, as the reference sequences them) on two
+// grids stored one after the other (2 x GN1 x GM float2), then
+// pixInterpolation with Gr = 2 for every corner.  border: (2 + 2*angleNum)
+// float2 out.  Only for grids where every border walk ends inside the
+// lattice (the reference's walk has no bound).
+void btref_map_pixinterp_blend(const float* view, int M, int N, const float* grid2,
+                               int GM, int GN1, int gridlvl, float hor, float ver,
+                               float alpha, float* thphi, int* gap, float* border_out) {
+  const int angleNum = 1000;
+  std::vector<float2> b1((size_t)(angleNum + 1) * 2), b2((size_t)(angleNum + 1) * 2);
+  b1[0] = {100, 0};
+  b1[1] = {100, 0};
+  const float2* g = (const float2*)grid2;
+  for (int i = 0; i < GN1; i++)
+    for (int j = 0; j < GM; j++) {
+      at(i, j);
+      findBhCenter(GM, GN1, g, b1.data());
+    }
+  for (int i = 0; i < angleNum * 2; i++) {
+    at(i, 0);
+    findBhBorders(GM, GN1, g, angleNum, b1.data());
+  }
+  for (int r = 0; r < 2; r++) {
+    for (int i = 0; i < angleNum * 2; i++) {
+      at(i, 0);
+      smoothBorder(b1.data(), b2.data(), angleNum);
+    }
+    for (int i = 0; i < angleNum * 2; i++) {
+      at(i, 0);
+      smoothBorder(b2.data(), b1.data(), angleNum);
+    }
+  }
+  for (int i = 0; i <= N; i++)
+    for (int j = 0; j <= M; j++) {
+      at(i, j);
+      pixInterpolation((const float2*)view, M, N, 2, (float2*)thphi, g, GM, GN1, hor, ver,
+                       gap, gridlvl, b1.data(), angleNum, alpha);
+    }
+  memcpy(border_out, b1.data(), (size_t)(2 + 2 * angleNum) * sizeof(float2));
+}
+
 // findBlackPixels + findArea for every pixel.
 void btref_map_bh_area(const float* thphi, int M, int N, unsigned char* bh,
                        float* area) {
