@@ -14,8 +14,12 @@ from .host import (BlackHole, Camera, Grid, GridSet, IntegOpts, grid_dims,  # no
 
 from .render import Blend, Environment, Renderer, StarProcessor, Viewer, psf_airy  # noqa: F401
 from .serve import Server  # noqa: F401
+from .cache import (GridFile, psh_build, read_grid_file, read_star_file,  # noqa: F401
+                    write_grid_file, write_star_file)
 
-__all__ = ["Environment", "Renderer", "Server", "StarProcessor", "Viewer", "BlackHole",
+__all__ = ["Environment", "GridFile", "Renderer", "Server", "StarProcessor", "Viewer",
+           "BlackHole", "psh_build", "read_grid_file", "write_grid_file", "read_star_file",
+           "write_star_file",
            "Camera", "Grid",
            "GridSet", "IntegOpts", "grid_dims", "integrate_rays",
            "integrate_rays_host", "BtError", "lib"]

@@ -99,6 +99,13 @@ class bt_frame(C.Structure):
                 ("blend", C.c_void_p)]
 
 
+class bt_psh(C.Structure):
+    _fields_ = [("hash_table", C.c_void_p), ("pos_tag", C.c_void_p),
+                ("offset_table", C.c_void_p), ("cap_hash", C.c_size_t),
+                ("cap_offset", C.c_size_t), ("hash_width", C.c_int32),
+                ("offset_width", C.c_int32)]
+
+
 class bt_map_buffers(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("thphi", "gap", "bh", "area", "light",
                                           "stars_img", "env_img", "light_diffracted")]
@@ -176,6 +183,23 @@ _SIGS = {
                                  C.POINTER(C.c_int), C.c_int]),
     "bt_server_stats_get": (C.c_int, [_vp, C.POINTER(bt_server_stats)]),
     "bt_server_destroy": (None, [_vp]),
+    "bt_psh_build": (C.c_int, [_vp, _vp, C.c_size_t, C.POINTER(bt_psh)]),
+    "bt_grid_map_from_psh": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       _vp, C.c_int, _vp]),
+    "bt_grid_file_write": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int,
+                                     C.POINTER(bt_psh)]),
+    "bt_grid_file_read": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_int32), C.POINTER(bt_psh)]),
+    "bt_grid_save": (C.c_int, [_vp, C.c_char_p, _vp]),
+    "bt_grid_file_map_shape": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_int32)]),
+    "bt_grid_file_load_map": (C.c_int, [C.c_char_p, _vp, C.c_int, C.c_int, _vp]),
+    "bt_stars_file_write": (C.c_int, [C.c_char_p, _vp, _vp, C.c_int, _vp, C.c_int]),
+    "bt_stars_file_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "bt_stars_file_read": (C.c_int, [C.c_char_p, _vp, _vp, C.c_int, _vp, C.c_int]),
+    "bt_view_camera": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                 _vp]),
     "bt_last_error": (C.c_char_p, []),
     "bt_version": (C.c_char_p, []),
 }

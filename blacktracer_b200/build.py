@@ -34,6 +34,7 @@ UNITS = {
     "map_api.cu": [],
     "noalloc.cu": [],
     "server.cu": [],
+    "cache.cu": [],
 }
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
            if f.endswith((".h", ".cuh"))] + [os.path.join(ROOT, "include", "blacktracer.h")]

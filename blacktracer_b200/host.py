@@ -278,6 +278,14 @@ class Grid:
         self._map = (p.value, rows.value, cols.value, sym.value)
         return self._map
 
+    def save(self, path):
+        """Writes the reference's grid cache file (write, BT/BlackTracer.cpp
+        :26-33): MAXLEVEL, N, M and the vertices in a perfect spatial hash,
+        which the reference loads in place of computing the grid."""
+        import os
+        L.check(L.lib().bt_grid_save(self._h, os.fsencode(os.fspath(path)),
+                                     _stream_ptr(self._stream)))
+
     # --- reference-shaped host views (slow; for compatibility and tests) ---
     @property
     def CamToCel(self) -> dict:

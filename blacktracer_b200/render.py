@@ -18,21 +18,26 @@ from .host import Camera, Grid, _stream_ptr, _torch
 
 
 class Viewer:
-    """Camera-sky corner directions of the output pixels (BT/Viewer.h).
-
-    Only the equirectangular sphere view (makeSphereView) is implemented on
-    the device; viewMatrix is a ((pixh+1)*(pixw+1), 2) float32 CUDA tensor."""
+    """Camera-sky corner directions of the output pixels (BT/Viewer.h:20-33):
+    the equirectangular sphere view (makeSphereView) or, with sphere=False,
+    the perspective view of horizontal angle `viewangle` turned by offUp and
+    offRight (makeCameraView).  viewMatrix is a ((pixh+1)*(pixw+1), 2)
+    float32 CUDA tensor."""
 
     def __init__(self, viewangle, offUp, offRight, pixw, pixh, sphere=True, stream=None):
-        if not sphere:
-            raise NotImplementedError("perspective camera view: not built")
         torch = _torch()
         self.pixelwidth, self.pixelheight = int(pixw), int(pixh)
         self.viewAngleWide = float(viewangle)
         self.viewMatrix = torch.empty(((pixh + 1) * (pixw + 1), 2), dtype=torch.float32,
                                       device="cuda")
-        L.check(L.lib().bt_view_sphere(self.viewMatrix.data_ptr(), self.pixelwidth,
-                                       self.pixelheight, _stream_ptr(stream)))
+        if sphere:
+            L.check(L.lib().bt_view_sphere(self.viewMatrix.data_ptr(), self.pixelwidth,
+                                           self.pixelheight, _stream_ptr(stream)))
+        else:
+            self.viewAngleUp = self.pixelheight * self.viewAngleWide / self.pixelwidth
+            L.check(L.lib().bt_view_camera(self.viewMatrix.data_ptr(), self.pixelwidth,
+                                           self.pixelheight, self.viewAngleWide, float(offUp),
+                                           float(offRight), _stream_ptr(stream)))
 
 
 class Environment:
@@ -157,6 +162,36 @@ class StarProcessor:
         self.starSize = kept.value
         self.starPos = self.starPos[: 2 * self.starSize].copy()
         self.starMag = self.starMag[: 2 * self.starSize].copy()
+        self._upload(psf, stream)
+
+    @classmethod
+    def from_tree(cls, starPos, starMag, binaryStarTree, treeLevel, psf=None, stream=None):
+        """A star set already arranged in the reference's tree (a StarProcessor
+        of the reference, or a .star file)."""
+        self = cls.__new__(cls)
+        self.treeLevel = int(treeLevel)
+        self.starPos = np.ascontiguousarray(starPos, dtype=np.float32)
+        self.starMag = np.ascontiguousarray(starMag, dtype=np.float32)
+        self.binaryStarTree = np.ascontiguousarray(binaryStarTree, dtype=np.int32)
+        self.starSize = self.starPos.size // 2
+        self._upload(psf, stream)
+        return self
+
+    @classmethod
+    def load(cls, path, psf=None, stream=None):
+        """A star cache file of the reference (BT/BlackTracer.cpp:326-331)."""
+        from .cache import read_star_file
+        pos, mag, tree, level = read_star_file(path)
+        return cls.from_tree(pos, mag, tree, level, psf=psf, stream=stream)
+
+    def save(self, path):
+        """Writes the reference's star cache file (writeStars,
+        BT/BlackTracer.cpp:40-46)."""
+        from .cache import write_star_file
+        write_star_file(path, self.starPos, self.starMag, self.binaryStarTree, self.treeLevel)
+
+    def _upload(self, psf, stream):
+        lib = L.lib()
         self.psf = None if psf is None else np.ascontiguousarray(psf, dtype=np.uint8)
         h = C.c_void_p()
         L.check(lib.bt_stars_create(self.starPos.ctypes.data, self.starMag.ctypes.data,

@@ -403,6 +403,107 @@ typedef struct bt_map_buffers {
 } bt_map_buffers;
 int bt_map_scratch(const bt_map* m, bt_map_buffers* b);
 
+/* ----------------------------------------------------------- cache files */
+
+/* The reference's grid and star cache files (cereal binary archives,
+ * written by write / writeStars, BT/BlackTracer.cpp:26-46, and loaded at
+ * :226-258 and :306-335), read and written without cereal:
+ * little-endian, each vector as a uint64 element count followed by its
+ * elements, each int as 4 bytes.
+ *   .grid  Grid::serialize (BT/Grid.h:36-39): int MAXLEVEL, N, M, then the
+ *          PSHOffsetTable (BT/PSHOffsetTable.h:46-48): vector<float>
+ *          hashTable (2 per slot), vector<int> offsetTable (2 per entry),
+ *          vector<int> hashPosTag (2 per slot), int hashTableWidth,
+ *          int offsetTableWidth.
+ *   .star  StarProcessor::serialize (BT/StarProcessor.h:21-23):
+ *          vector<int> binaryStarTree, vector<float> starPos,
+ *          vector<float> starMag, int starSize, treeSize, treeLevel. */
+
+/* A perfect spatial hash of lattice keys (i, j) -> (theta, phi): the
+ * reference's PSHOffsetTable (BT/PSHOffsetTable.h), as the reference's
+ * renderer consumes it (hashLookup, BT/kernel.cuh:713-733).  Buffers are
+ * the caller's (HOST); a call whose capacities are too small returns
+ * BT_ERR_ARG with the widths set, so the caller can size and call again. */
+typedef struct bt_psh {
+  float* hash_table;      /* 2 * hash_width^2: (theta, phi) per slot        */
+  int32_t* pos_tag;       /* 2 * hash_width^2: key (i, j) per slot          */
+  int32_t* offset_table;  /* 2 * offset_width^2                             */
+  size_t cap_hash;        /* capacity of hash_table and pos_tag, elements   */
+  size_t cap_offset;      /* capacity of offset_table, elements             */
+  int32_t hash_width;     /* out (in, for bt_grid_file_write)               */
+  int32_t offset_width;   /* out (in, for bt_grid_file_write)               */
+} bt_psh;
+
+/* Builds a table for n keys (2n ints, (i, j) >= 0, distinct) and values (2n
+ * floats): replaces saveAsGpuHash + PSHOffsetTable::PSHOffsetTable
+ * (BT/Grid.h:642-654, BT/PSHOffsetTable.h:350-370, widths :59-79).  Same table widths as
+ * the reference (hash width (int)(sqrt(1.1 n) + 1.1), offset width
+ * (int)(sqrt(n / 4) + 1.1) raised to be coprime with it) unless those fail
+ * a few times -- regular key sets such as a uniform lattice -- after which
+ * both widths grow.  Offsets are found by a deterministic search (the
+ * reference seeds rand() with the time), so the table is reproducible.
+ * HOST only.  BT_ERR_NUMERIC if no table was found after the bounded
+ * retries. */
+int bt_psh_build(const int32_t* keys, const float* values, size_t n, bt_psh* out);
+
+/* The float2 map grid of a PSH table: makeGrid (BT/MakeImageKernel.cu
+ * :369-384) -- every lattice vertex (i < N, j < M) looked up, (-2,-2) where
+ * absent; with sym (M / N > 3) the lower hemisphere is mirrored into rows
+ * 2N-1-i (rows = 2N-1).  Tables are DEVICE arrays; grid is a DEVICE array
+ * of rows * M float2.  Offsets outside the table wrap (the reference reads
+ * out of bounds there). */
+int bt_grid_map_from_psh(const float* hash_table, const int32_t* pos_tag,
+                         const int32_t* offset_table, int hash_width,
+                         int offset_width, int N, int M, float* grid, int rows,
+                         void* stream);
+
+/* Writes / reads a .grid file.  maxlevel, N and M as the reference's Grid
+ * holds them; tables as bt_psh (hash_width and offset_width are inputs for
+ * writing).  Reading checks every count against the file's size and the
+ * lattice shape against maxlevel; HOST only. */
+int bt_grid_file_write(const char* path, int maxlevel, int N, int M, const bt_psh* t);
+int bt_grid_file_read(const char* path, int32_t* maxlevel, int32_t* N, int32_t* M,
+                      bt_psh* t);
+
+/* A built grid to a .grid file the reference loads (BT/BlackTracer.cpp
+ * :236-242): compact export, bt_psh_build, bt_grid_file_write.  Synchronises
+ * `stream`.  The reference writes an empty table when startlevel ==
+ * maxlevel (BT/Grid.h:623); here the table always holds the vertices. */
+int bt_grid_save(bt_grid* g, const char* path, void* stream);
+
+/* Shape of a .grid file's map grid: rows (2N-1 when mirrored, else N),
+ * cols (M), sym (1 when mirrored); and the file's maxlevel (the map's grid
+ * level).  Any output may be NULL. */
+int bt_grid_file_map_shape(const char* path, int32_t* maxlevel, int32_t* rows,
+                           int32_t* cols, int32_t* sym);
+/* A .grid file straight to a DEVICE map grid (rows x cols float2, as
+ * bt_grid_map_export returns): read, upload (stream-ordered allocation,
+ * released on `stream`), bt_grid_map_from_psh. */
+int bt_grid_file_load_map(const char* path, float* grid, int rows, int cols,
+                          void* stream);
+
+/* .star files.  Write: the arrays of bt_stars_build_tree / bt_stars_create
+ * (star_pos, star_mag 2n each, tree bt_stars_tree_size(treeLevel)).  Read:
+ * bt_stars_file_info for the counts, then bt_stars_file_read into HOST
+ * arrays of those sizes. */
+int bt_stars_file_write(const char* path, const float* star_pos, const float* star_mag,
+                        int n, const int* tree, int treeLevel);
+int bt_stars_file_info(const char* path, int* n, int* treeLevel);
+int bt_stars_file_read(const char* path, float* star_pos, float* star_mag, int n_cap,
+                       int* tree, int tree_cap);
+
+/* ---------------------------------------------------------- camera view */
+
+/* Camera-sky corner directions of a perspective W x H view looking along
+ * the camera's forward direction, turned by offset_ver (up) and offset_hor
+ * (right): Viewer::makeCameraView (BT/Viewer.h:109-133), with the
+ * horizontal field of view view_angle (radians; the vertical one is
+ * H / W of it).  |offset_ver| must not exceed (pi - vertical angle) / 2
+ * (the reference prints an error and leaves the view unset).  view: DEVICE
+ * float2 array of (H+1)*(W+1) (theta, phi). */
+int bt_view_camera(float* view, int width, int height, double view_angle,
+                   double offset_ver, double offset_hor, void* stream);
+
 /* --------------------------------------------------------------- serving */
 
 /* A frame server: requests of any resolution, camera and spin are rendered

@@ -333,3 +333,95 @@ def ref_map_frame(grid_f2, grid_rows, grid_cols, gridlvl, view, width, height, c
             img = simg
     out["image"] = img
     return out
+
+
+# ---------------------------------------------------------------- cache files, view (reference)
+def _path(p) -> bytes:
+    return os.fsencode(os.fspath(p))
+
+
+def ref_grid_file_write(path, maxlevel, startlevel, angle, cam, a) -> int:
+    """The reference's Grid constructor (with its perfect hash) written
+    through cereal as the reference's app writes it.  Returns CamToCel's
+    size."""
+    lib = _reflib()
+    lib.btref_grid_file_write.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _dp,
+                                          C.c_double]
+    lib.btref_grid_file_write.restype = C.c_long
+    cam = np.ascontiguousarray(cam, dtype=np.float64)
+    return int(lib.btref_grid_file_write(_path(path), maxlevel, startlevel, 1 if angle else 0,
+                                         cam, a))
+
+
+def ref_grid_file_decode(path) -> dict:
+    """A .grid file read through cereal into the reference's Grid: its
+    tables, and every lattice vertex looked up with the reference's hash
+    (dense (N*M, 2) float32, -2 where absent)."""
+    lib = _reflib()
+    ip = C.POINTER(C.c_int)
+    lib.btref_grid_file_dims.argtypes = [C.c_char_p, ip, ip, ip, ip, ip]
+    lib.btref_grid_file_decode.argtypes = [C.c_char_p, _f32p, _i32, _i32, _f32p]
+    v = [C.c_int() for _ in range(5)]
+    if lib.btref_grid_file_dims(_path(path), *[C.byref(x) for x in v]) != 0:
+        raise FileNotFoundError(path)
+    ml, N, M, hw, ow = (x.value for x in v)
+    ht = np.empty(2 * hw * hw, np.float32)
+    ot = np.empty(2 * ow * ow, np.int32)
+    tag = np.empty(2 * hw * hw, np.int32)
+    dense = np.empty(2 * N * M, np.float32)
+    lib.btref_grid_file_decode(_path(path), ht, ot, tag, dense)
+    return dict(MAXLEVEL=ml, N=N, M=M, hash_width=hw, offset_width=ow,
+                hash_table=ht.reshape(-1, 2), offset_table=ot.reshape(-1, 2),
+                pos_tag=tag.reshape(-1, 2), dense=dense.reshape(-1, 2))
+
+
+def ref_psh_build(keys, values) -> dict:
+    """The reference's PSHOffsetTable from keys (n, 2) and values (n, 2)
+    (its offset search is seeded with the time: tables differ run to run)."""
+    lib = _reflib()
+    ip = C.POINTER(C.c_int)
+    lib.btref_psh_build.argtypes = [_i32, _f32p, C.c_int, ip, ip, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_long, C.c_long]
+    k = np.ascontiguousarray(keys, dtype=np.int32).reshape(-1)
+    v = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
+    hw, ow = C.c_int(), C.c_int()
+    lib.btref_psh_build(k, v, len(k) // 2, C.byref(hw), C.byref(ow), None, None, None, 0, 0)
+    return dict(hash_width=hw.value, offset_width=ow.value)
+
+
+def ref_stars_file_write(path, pos, mag, tree, tree_level) -> None:
+    lib = _reflib()
+    lib.btref_stars_file_write.argtypes = [C.c_char_p, _f32p, _f32p, C.c_int, _i32, C.c_int]
+    pos = np.ascontiguousarray(pos, np.float32)
+    lib.btref_stars_file_write(_path(path), pos, np.ascontiguousarray(mag, np.float32),
+                               pos.size // 2, np.ascontiguousarray(tree, np.int32), tree_level)
+
+
+def ref_stars_file_read(path):
+    """(pos, mag, tree, treeLevel) of a .star file read through cereal into
+    the reference's StarProcessor."""
+    lib = _reflib()
+    ip = C.POINTER(C.c_int)
+    lib.btref_stars_file_read.argtypes = [C.c_char_p, ip, ip, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_int, C.c_int]
+    n, lv = C.c_int(), C.c_int()
+    if lib.btref_stars_file_read(_path(path), C.byref(n), C.byref(lv), None, None, None,
+                                 -1, -1) != 0:
+        raise FileNotFoundError(path)
+    pos = np.empty(2 * n.value, np.float32)
+    mag = np.empty(2 * n.value, np.float32)
+    tree = np.empty((1 << (lv.value + 1)) - 1, np.int32)
+    lib.btref_stars_file_read(_path(path), C.byref(n), C.byref(lv), pos.ctypes.data,
+                              mag.ctypes.data, tree.ctypes.data, n.value, tree.size)
+    return pos, mag, tree, lv.value
+
+
+def ref_view_camera(view_angle, off_up, off_right, width, height):
+    """Viewer(viewangle, offUp, offRight, W, H, sphere = false).viewMatrix
+    (BT/Viewer.h:109-133) as ((H+1)*(W+1), 2) float32."""
+    lib = _reflib()
+    lib.btref_view_camera.argtypes = [C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                      _f32p]
+    out = np.zeros(2 * (height + 1) * (width + 1), np.float32)
+    lib.btref_view_camera(view_angle, off_up, off_right, width, height, out)
+    return out.reshape(-1, 2)

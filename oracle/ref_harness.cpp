@@ -6,7 +6,11 @@
 // repository; this file only calls the reference's classes:
 //   Camera (BT/Camera.h:27,40), BlackHole (BT/BlackHole.h:7),
 //   Grid::integration_wrapper (BT/Grid.h:514), Grid::raytrace (BT/Grid.h:291),
-//   Grid::fixTvertices (BT/Grid.h:103), Grid::Grid (BT/Grid.h:605-624).
+//   Grid::fixTvertices (BT/Grid.h:103), Grid::Grid (BT/Grid.h:605-624),
+//   PSHOffsetTable (BT/PSHOffsetTable.h), StarProcessor::makeTree and the
+//   cereal archives of Grid and StarProcessor (BT/Grid.h:36-39,
+//   BT/StarProcessor.h:21-23; cereal 1.2.2 as vendored with the reference),
+//   Viewer::makeCameraView (BT/Viewer.h:109-133).
 // It exposes them through a small extern "C" surface that oracle/__init__.py
 // loads with ctypes, so the plain-C restatement (oracle/bt_oracle.c) and the
 // GPU library can be pinned to the reference's own outputs.
@@ -41,6 +45,7 @@
 #define private public
 #include "Grid.h"
 #include "StarProcessor.h"
+#include "Viewer.h"
 #undef private
 
 // StarProcessor holds an (always empty) cv::Mat; its inline destructor
@@ -225,6 +230,143 @@ void btref_star_tree(const float* theta, const float* phi, const float* mag,
   std::copy(sp.starPos.begin(), sp.starPos.end(), star_pos);
   std::copy(sp.starMag.begin(), sp.starMag.end(), star_mag);
   std::copy(sp.binaryStarTree.begin(), sp.binaryStarTree.end(), tree);
+}
+
+// ---- cache files, through cereal (the reference's own archive code) ----
+
+// The reference's Grid constructor (with its perfect hash, BT/Grid.h:605-624)
+// written as BT/BlackTracer.cpp:26-33 writes it.  Returns CamToCel's size.
+long btref_grid_file_write(const char* path, int maxlevel, int startlevel, int angle,
+                           const double* cam12, double a) {
+  Quiet q;
+  BlackHole bh(a);
+  Camera cam = cam_from_array(cam12);
+  Grid g(maxlevel, startlevel, angle != 0, &cam, &bh);
+  {
+    std::ofstream ofs(path, std::ios::out | std::ios::binary);
+    cereal::BinaryOutputArchive oarch(ofs);
+    oarch(g);
+  }
+  return (long)g.CamToCel.size();
+}
+
+// A .grid file read as BT/BlackTracer.cpp:236-242 reads it; dims first.
+int btref_grid_file_dims(const char* path, int* maxlevel, int* N, int* M, int* hw, int* ow) {
+  Grid g;
+  std::ifstream ifs(path, std::ios::in | std::ios::binary);
+  if (!ifs.good()) return -1;
+  {
+    cereal::BinaryInputArchive iarch(ifs);
+    iarch(g);
+  }
+  *maxlevel = g.MAXLEVEL;
+  *N = g.N;
+  *M = g.M;
+  *hw = g.hasher.hashTableWidth;
+  *ow = g.hasher.offsetTableWidth;
+  return 0;
+}
+
+// The file's tables as the reference holds them, and every lattice vertex
+// looked up with the reference's hash (PSHOffsetTable::hashFunc plus the tag
+// test of hashLookup): dense N*M float2, (-2,-2) where absent.
+int btref_grid_file_decode(const char* path, float* hash_table, int* offset_table,
+                           int* pos_tag, float* dense) {
+  Grid g;
+  std::ifstream ifs(path, std::ios::in | std::ios::binary);
+  if (!ifs.good()) return -1;
+  {
+    cereal::BinaryInputArchive iarch(ifs);
+    iarch(g);
+  }
+  PSHOffsetTable& h = g.hasher;
+  std::copy(h.hashTable.begin(), h.hashTable.end(), hash_table);
+  std::copy(h.offsetTable.begin(), h.offsetTable.end(), offset_table);
+  std::copy(h.hashPosTag.begin(), h.hashPosTag.end(), pos_tag);
+  const int hw = h.hashTableWidth;
+  for (int i = 0; i < g.N; i++)
+    for (int j = 0; j < g.M; j++) {
+      int2 key = {i, j};
+      int2 s = h.hashFunc(key);
+      const int id = s.x * hw + s.y;
+      float* o = dense + 2 * ((size_t)i * g.M + j);
+      if (h.hashPosTag[2 * id] != i || h.hashPosTag[2 * id + 1] != j) {
+        o[0] = -2.f;
+        o[1] = -2.f;
+      } else {
+        o[0] = h.hashTable[2 * id];
+        o[1] = h.hashTable[2 * id + 1];
+      }
+    }
+  return 0;
+}
+
+// The reference's PSHOffsetTable built from keys / values (BT/PSHOffsetTable.h
+// :350-370); its widths, then its tables.
+void btref_psh_build(const int* keys, const float* vals, int n, int* hw, int* ow,
+                     float* hash_table, int* offset_table, int* pos_tag, long cap_hash,
+                     long cap_offset) {
+  Quiet q;
+  std::vector<int2> el(n);
+  std::vector<float2> dt(n);
+  for (int k = 0; k < n; k++) {
+    el[k] = {keys[2 * k], keys[2 * k + 1]};
+    dt[k] = {vals[2 * k], vals[2 * k + 1]};
+  }
+  PSHOffsetTable t(el, dt);
+  *hw = t.hashTableWidth;
+  *ow = t.offsetTableWidth;
+  if ((long)t.hashTable.size() <= cap_hash && (long)t.offsetTable.size() <= cap_offset) {
+    std::copy(t.hashTable.begin(), t.hashTable.end(), hash_table);
+    std::copy(t.offsetTable.begin(), t.offsetTable.end(), offset_table);
+    std::copy(t.hashPosTag.begin(), t.hashPosTag.end(), pos_tag);
+  }
+}
+
+// A StarProcessor with the given tree written / read through cereal
+// (BT/BlackTracer.cpp:40-46, :326-331).
+void btref_stars_file_write(const char* path, const float* pos, const float* mag, int n,
+                            const int* tree, int treeLevel) {
+  StarProcessor sp;
+  sp.starSize = n;
+  sp.treeLevel = treeLevel;
+  sp.treeSize = (1 << (treeLevel + 1)) - 1;
+  sp.starPos.assign(pos, pos + 2 * n);
+  sp.starMag.assign(mag, mag + 2 * n);
+  sp.binaryStarTree.assign(tree, tree + sp.treeSize);
+  std::ofstream ofs(path, std::ios::out | std::ios::binary);
+  cereal::BinaryOutputArchive oarch(ofs);
+  oarch(sp);
+}
+
+int btref_stars_file_read(const char* path, int* n, int* treeLevel, float* pos, float* mag,
+                          int* tree, int cap_n, int cap_tree) {
+  StarProcessor sp;
+  std::ifstream ifs(path, std::ios::in | std::ios::binary);
+  if (!ifs.good()) return -1;
+  {
+    cereal::BinaryInputArchive iarch(ifs);
+    iarch(sp);
+  }
+  *n = sp.starSize;
+  *treeLevel = sp.treeLevel;
+  if (sp.starSize <= cap_n && (int)sp.binaryStarTree.size() <= cap_tree) {
+    std::copy(sp.starPos.begin(), sp.starPos.end(), pos);
+    std::copy(sp.starMag.begin(), sp.starMag.end(), mag);
+    std::copy(sp.binaryStarTree.begin(), sp.binaryStarTree.end(), tree);
+  }
+  return 0;
+}
+
+// Viewer(viewangle, offUp, offRight, pixw, pixh, sphere = false): the
+// perspective view of BT/Viewer.h:20-33, 109-133.
+void btref_view_camera(double angle, double offUp, double offRight, int w, int h, float* out) {
+  Quiet q;
+  Viewer v(angle, offUp, offRight, w, h, false);
+  for (size_t k = 0; k < v.viewMatrix.size(); k++) {
+    out[2 * k] = v.viewMatrix[k].x;
+    out[2 * k + 1] = v.viewMatrix[k].y;
+  }
 }
 
 }  // extern "C"
