@@ -14,13 +14,16 @@
 // Differences, all deliberate:
 //   * No OpenCV: celestial points are Point2d {x = theta, y = phi}; images
 //     are BGR8 / BGRA8 byte buffers in cv::Mat's channel order.
-//   * No files: the star list and the environment image are passed in
-//     memory; Distorter renders into a caller buffer instead of a PNG.
+//   * No image files: the star list and the environment image are passed in
+//     memory; Distorter renders into a caller buffer instead of a PNG.  The
+//     grid and star cache files are the reference's (Grid::save / load,
+//     StarProcessor(file) / save).
 //   * Errors throw blacktracer::Error (the reference printed and carried on).
 //   * Grid keeps its lattice on the device; CamToCel / steps / blockLevels
 //     are host copies made on first access.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <stdexcept>
@@ -103,6 +106,36 @@ class Camera {
   }
 };
 
+// Device memory owned by the mirror classes.
+template <class T>
+class DeviceArray {
+ public:
+  DeviceArray() {}
+  explicit DeviceArray(size_t n) { resize(n); }
+  DeviceArray(const DeviceArray&) = delete;
+  DeviceArray& operator=(const DeviceArray&) = delete;
+  ~DeviceArray() {
+    if (p_) cudaFree(p_);
+  }
+  void resize(size_t n) {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = n;
+    if (n && cudaMalloc((void**)&p_, n * sizeof(T)) != cudaSuccess)
+      throw Error(BT_ERR_NOMEM, "device allocation failed");
+  }
+  T* get() const { return p_; }
+  size_t size() const { return n_; }
+  void swap(DeviceArray& o) noexcept {
+    std::swap(p_, o.p_);
+    std::swap(n_, o.n_);
+  }
+
+ private:
+  T* p_ = nullptr;
+  size_t n_ = 0;
+};
+
 struct Point2d {
   double x, y;  // theta, phi
 };
@@ -147,7 +180,49 @@ class Grid {
     block_levels_.swap(o.block_levels_);
     steps_.swap(o.steps_);
     exported_ = o.exported_;
+    file_map_.swap(o.file_map_);
+    std::swap(file_rows_, o.file_rows_);
+    std::swap(file_cols_, o.file_cols_);
     return *this;
+  }
+
+  // write(filename, grid), BT/BlackTracer.cpp:26-33: the reference's .grid
+  // cache file (MAXLEVEL, N, M and the vertices' perfect spatial hash).
+  void save(const std::string& path) {
+    if (!g_) throw Error(BT_ERR_STATE, "a grid loaded from a file is already a file");
+    check(bt_grid_save(g_, path.c_str(), stream_));
+  }
+
+  // The cereal load of BT/BlackTracer.cpp:236-242.  Like the reference's
+  // loaded Grid it holds MAXLEVEL, N and M and renders, but its CamToCel,
+  // steps and blockLevels are empty (they are not in the file).
+  static Grid load(const std::string& path, cudaStream_t stream = nullptr) {
+    Grid g;
+    g.stream_ = stream;
+    int32_t ml = 0, rows = 0, cols = 0, sym = 0;
+    check(bt_grid_file_map_shape(path.c_str(), &ml, &rows, &cols, &sym));
+    g.MAXLEVEL = ml;
+    g.M = cols;
+    g.N = sym ? (rows + 1) / 2 : rows;
+    g.equafactor = sym ? 0 : 1;
+    g.file_map_.resize((size_t)2 * rows * cols);
+    g.file_rows_ = rows;
+    g.file_cols_ = cols;
+    check(bt_grid_file_load_map(path.c_str(), g.file_map_.get(), rows, cols, stream));
+    g.exported_ = true;
+    return g;
+  }
+
+  // The float2 map grid the renderer reads (makeGrid's output).
+  void mapGrid(const float** grid, int32_t* rows, int32_t* cols) const {
+    if (!g_) {
+      *grid = file_map_.get();
+      *rows = file_rows_;
+      *cols = file_cols_;
+      return;
+    }
+    int32_t sym = 0;
+    check(bt_grid_map_export(g_, grid, rows, cols, &sym, stream_));
   }
   ~Grid() {
     if (g_) bt_grid_destroy(g_);
@@ -196,32 +271,8 @@ class Grid {
   std::unordered_map<uint64_t, int> block_levels_;
   std::vector<int> steps_;
   bool exported_ = false;
-};
-
-// Device memory owned by the mirror classes.
-template <class T>
-class DeviceArray {
- public:
-  DeviceArray() {}
-  explicit DeviceArray(size_t n) { resize(n); }
-  DeviceArray(const DeviceArray&) = delete;
-  DeviceArray& operator=(const DeviceArray&) = delete;
-  ~DeviceArray() {
-    if (p_) cudaFree(p_);
-  }
-  void resize(size_t n) {
-    if (p_) cudaFree(p_);
-    p_ = nullptr;
-    n_ = n;
-    if (n && cudaMalloc((void**)&p_, n * sizeof(T)) != cudaSuccess)
-      throw Error(BT_ERR_NOMEM, "device allocation failed");
-  }
-  T* get() const { return p_; }
-  size_t size() const { return n_; }
-
- private:
-  T* p_ = nullptr;
-  size_t n_ = 0;
+  DeviceArray<float> file_map_;  // a grid loaded from a file
+  int32_t file_rows_ = 0, file_cols_ = 0;
 };
 
 class Viewer {
@@ -232,14 +283,16 @@ class Viewer {
 
   Viewer(double viewangle, double offUp, double offRight, int pixw, int pixh,
          bool sphere, cudaStream_t stream = nullptr) {
-    (void)offUp;
-    (void)offRight;
-    if (!sphere) throw Error(BT_ERR_ARG, "perspective camera view: not built");
     pixelwidth = pixw;
     pixelheight = pixh;
-    viewAngleWide = viewangle;
     viewMatrix.resize((size_t)2 * (pixh + 1) * (pixw + 1));
-    check(bt_view_sphere(viewMatrix.get(), pixw, pixh, stream));
+    if (sphere) {
+      check(bt_view_sphere(viewMatrix.get(), pixw, pixh, stream));
+    } else {  // makeCameraView(offUp, offRight), BT/Viewer.h:109-133
+      viewAngleWide = viewangle;
+      viewAngleUp = 1. * pixh * viewAngleWide / (1. * pixw);
+      check(bt_view_camera(viewMatrix.get(), pixw, pixh, viewangle, offUp, offRight, stream));
+    }
   }
 };
 
@@ -279,6 +332,24 @@ class StarProcessor {
     check(bt_stars_create(starPos.data(), starMag.data(), starSize, binaryStarTree.data(),
                           treeLevel, psf_rgb, psf_size, &s_, stream));
   }
+  // The cereal load of a star cache file (BT/BlackTracer.cpp:326-331).
+  explicit StarProcessor(const std::string& starFile, const uint8_t* psf_rgb = nullptr,
+                         int psf_size = 0, cudaStream_t stream = nullptr) {
+    check(bt_stars_file_info(starFile.c_str(), &starSize, &treeLevel));
+    treeSize = bt_stars_tree_size(treeLevel);
+    starPos.resize((size_t)2 * starSize);
+    starMag.resize((size_t)2 * starSize);
+    binaryStarTree.resize(treeSize);
+    check(bt_stars_file_read(starFile.c_str(), starPos.data(), starMag.data(), starSize,
+                             binaryStarTree.data(), treeSize));
+    check(bt_stars_create(starPos.data(), starMag.data(), starSize, binaryStarTree.data(),
+                          treeLevel, psf_rgb, psf_size, &s_, stream));
+  }
+  // writeStars, BT/BlackTracer.cpp:40-46.
+  void save(const std::string& path) const {
+    check(bt_stars_file_write(path.c_str(), starPos.data(), starMag.data(), starSize,
+                              binaryStarTree.data(), treeLevel));
+  }
   StarProcessor(const StarProcessor&) = delete;
   StarProcessor& operator=(const StarProcessor&) = delete;
   ~StarProcessor() {
@@ -301,9 +372,17 @@ class Distorter {
             std::vector<Camera>* cams, const uint8_t* env_bgr, int env_rows,
             int env_cols, cudaStream_t stream = nullptr)
       : grids_(grids), view_(viewer), stars_(stars), cams_(cams), stream_(stream) {
-    if (grids->size() != 1)
-      throw Error(BT_ERR_ARG, "blending of several grids (G > 1) is not built");
+    if (grids->empty() || cams->size() != grids->size())
+      throw Error(BT_ERR_ARG, "one camera per grid is needed");
     check(bt_map_create(viewer->pixelwidth, viewer->pixelheight, &m_));
+    if (grids->size() > 1) {
+      int rc = bt_blend_create(&blend_);
+      if (rc) {
+        bt_map_destroy(m_);
+        m_ = nullptr;
+        check(rc);
+      }
+    }
     if (env_bgr) {
       int rc = bt_env_create(env_bgr, env_rows, env_cols, 0, &env_, stream_);
       if (rc) {
@@ -316,16 +395,31 @@ class Distorter {
   Distorter(const Distorter&) = delete;
   Distorter& operator=(const Distorter&) = delete;
   ~Distorter() {
+    if (blend_) bt_blend_destroy(blend_);
     if (env_) bt_env_destroy(env_);
     if (m_) bt_map_destroy(m_);
   }
 
-  // One frame into a device BGRA8 buffer of width*height*4 bytes.
-  void renderDevice(uint8_t* out_bgra, float hor = 0.f, float ver = 0.f) {
-    Grid& g = (*grids_)[0];
+  // One frame into a device BGRA8 buffer of width*height*4 bytes.  hor / ver
+  // are the look-around offsets the reference's arrow keys change
+  // (BT/MakeImageKernel.cu:1081-1102).  With several grids, prec selects the
+  // pair blended as the reference's '=' / '-' keys do (:990-1008): grids
+  // (int)p and (int)p + 1 with weight fmod(p, 1) of the second, p = fmod(prec,
+  // G - 1).
+  void renderDevice(uint8_t* out_bgra, float hor = 0.f, float ver = 0.f, float prec = 0.f) {
+    const int G = (int)grids_->size();
+    int gnr = 0;
+    float alpha = 0.f;
+    if (G > 1) {
+      const float p = std::fmod(prec, (float)G - 1.f);
+      alpha = std::fmod(p, 1.f);
+      gnr = (int)p;
+      if (gnr < 0 || gnr > G - 2) throw Error(BT_ERR_ARG, "prec must not be negative");
+    }
+    Grid& g = (*grids_)[gnr];
     const float* grid = nullptr;
-    int32_t rows = 0, cols = 0, sym = 0;
-    check(bt_grid_map_export(g.handle(), &grid, &rows, &cols, &sym, stream_));
+    int32_t rows = 0, cols = 0;
+    g.mapGrid(&grid, &rows, &cols);
     bt_frame f;
     std::memset(&f, 0, sizeof(f));
     f.grid = grid;
@@ -335,7 +429,7 @@ class Distorter {
     f.view = view_->viewMatrix.get();
     f.hor = hor;
     f.ver = ver;
-    const std::vector<float> c = (*cams_)[0].getParamArray();
+    const std::vector<float> c = (*cams_)[gnr].getParamArray();
     for (int q = 0; q < 7; q++) f.cam[q] = c[q];
     f.env = env_;
     f.stars = stars_ ? stars_->handle() : nullptr;
@@ -345,14 +439,29 @@ class Distorter {
     f.step = step;
     f.diffraction = diffraction ? 1 : 0;
     f.out = out_bgra;
+    if (G > 1) {
+      const float* grid2 = nullptr;
+      int32_t rows2 = 0, cols2 = 0;
+      (*grids_)[gnr + 1].mapGrid(&grid2, &rows2, &cols2);
+      if (rows2 != rows || cols2 != cols) throw Error(BT_ERR_ARG, "grids of different shapes");
+      if (gnr != prepared_) {  // findBhCenter / findBhBorders / smoothBorder
+        check(bt_blend_prepare(blend_, grid, grid2, rows, cols, stream_));
+        prepared_ = gnr;
+      }
+      const std::vector<float> c2 = (*cams_)[gnr + 1].getParamArray();
+      for (int q = 0; q < 7; q++) f.cam2[q] = c2[q];
+      f.grid2 = grid2;
+      f.alpha = alpha;
+      f.blend = blend_;
+    }
     check(bt_map_render(m_, &f, stream_));
   }
 
   // One frame into a host BGRA8 buffer (the reference wrote it to a PNG).
-  void render(uint8_t* host_bgra) {
+  void render(uint8_t* host_bgra, float hor = 0.f, float ver = 0.f, float prec = 0.f) {
     const size_t bytes = (size_t)view_->pixelwidth * view_->pixelheight * 4;
     if (out_.size() != bytes) out_.resize(bytes);
-    renderDevice(out_.get());
+    renderDevice(out_.get(), hor, ver, prec);
     if (cudaMemcpyAsync(host_bgra, out_.get(), bytes, cudaMemcpyDeviceToHost, stream_) !=
             cudaSuccess ||
         cudaStreamSynchronize(stream_) != cudaSuccess)
@@ -367,6 +476,8 @@ class Distorter {
   cudaStream_t stream_;
   bt_map* m_ = nullptr;
   bt_env* env_ = nullptr;
+  bt_blend* blend_ = nullptr;
+  int prepared_ = -1;  // grid pair the blend was prepared for
   DeviceArray<uint8_t> out_;
 };
 

@@ -60,3 +60,13 @@ def test_cpp_grid_matches_oracle(demo, oracle_mod, cuda):
 def test_cpp_frame_renders(demo, cuda):
     total, nstars = run(demo, "frame")[0].split()
     assert int(nstars) == 2000 and int(total) > 256 * 128 * 255  # alpha alone
+
+
+@pytest.mark.gpu
+def test_cpp_files_view_and_blend(demo, cuda, tmp_path):
+    out = subprocess.run([demo, "files", str(tmp_path)], check=True, capture_output=True,
+                         text=True).stdout
+    same, level, nstars, repeat, blended = out.split()
+    assert same == "1", "frame from the saved files differs"
+    assert int(level) == 7 and int(nstars) == 1500
+    assert repeat == "1" and blended == "1"
