@@ -12,12 +12,13 @@ from ._lib import (BtError, PRECISION_FAST, PRECISION_MIXED, PRECISION_PLAIN,  #
 from .host import (BlackHole, Camera, Grid, GridSet, IntegOpts, grid_dims,  # noqa: F401
                    integrate_rays, integrate_rays_host)
 
-from .render import Blend, Environment, Renderer, StarProcessor, Viewer, psf_airy  # noqa: F401
+from .render import (Blend, Environment, Renderer, StarProcessor, Trails,  # noqa: F401
+                     Viewer, psf_airy)
 from .serve import Server  # noqa: F401
 from .cache import (GridFile, psh_build, read_grid_file, read_star_file,  # noqa: F401
                     write_grid_file, write_star_file)
 
-__all__ = ["Environment", "GridFile", "Renderer", "Server", "StarProcessor", "Viewer",
+__all__ = ["Environment", "GridFile", "Trails", "Renderer", "Server", "StarProcessor", "Viewer",
            "BlackHole", "psh_build", "read_grid_file", "write_grid_file", "read_star_file",
            "write_star_file",
            "Camera", "Grid",

@@ -96,7 +96,12 @@ class bt_frame(C.Structure):
                 ("lr", C.c_int32), ("step", C.c_int32), ("diffraction", C.c_int32),
                 ("out", C.c_void_p), ("bb_table", C.c_int32), ("psf_scale", C.c_int32),
                 ("grid2", C.c_void_p), ("alpha", C.c_float), ("cam2", C.c_float * 7),
-                ("blend", C.c_void_p)]
+                ("blend", C.c_void_p), ("trails", C.c_void_p)]
+
+
+class bt_trails_info(C.Structure):
+    _fields_ = [("frame", C.c_int64), ("hits", C.c_uint32), ("dropped", C.c_uint32),
+                ("walks_cut", C.c_uint32), ("trail", C.c_void_p)]
 
 
 class bt_psh(C.Structure):
@@ -200,6 +205,11 @@ _SIGS = {
     "bt_stars_file_read": (C.c_int, [C.c_char_p, _vp, _vp, C.c_int, _vp, C.c_int]),
     "bt_view_camera": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                  _vp]),
+    "bt_trails_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t,
+                                   C.POINTER(_vp)]),
+    "bt_trails_destroy": (None, [_vp]),
+    "bt_trails_reset": (C.c_int, [_vp]),
+    "bt_trails_query": (C.c_int, [_vp, C.POINTER(bt_trails_info), _vp]),
     "bt_last_error": (C.c_char_p, []),
     "bt_version": (C.c_char_p, []),
 }

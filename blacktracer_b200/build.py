@@ -35,6 +35,7 @@ UNITS = {
     "noalloc.cu": [],
     "server.cu": [],
     "cache.cu": [],
+    "trails.cu": ["--fmad=false"],
 }
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC)
            if f.endswith((".h", ".cuh"))] + [os.path.join(ROOT, "include", "blacktracer.h")]

@@ -266,6 +266,7 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
   F.step = f->step;
   F.diffraction = f->diffraction;
   F.out = f->out;
+  F.trails = f->trails;
   // environment into the output directly, or into a temporary when stars
   // are composited on top (addStarsAndBackground)
   F.out_bg = (f->star && f->map) ? m->tmp_img : f->out;

@@ -60,12 +60,18 @@ struct MapFrame {
   int psf_scale;        // diffraction footprint scaled by sqrt(pixel magnification)
   uint8_t* out_bg;      // N*M*4 environment (or final) image
   uint8_t* out;         // N*M*4 final image
+  bt_trails* trails;    // star trails between frames, or NULL
 };
 
 int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s);
 int blend_prepare(const float2* ga, const float2* gb, int GN, int GM, float2* border,
                   float2* border2, int nang, uint32_t* edge, cudaStream_t s);
 int map_run_stars(MapScratch& S, const MapFrame& F, cudaStream_t s);
+StarSet stars_for_frame(const bt_stars* s, int bb_table);
+// Star trails of this frame into the trail buffer (trails.cu).
+int trails_run(bt_trails* t, MapScratch& Sc, const MapFrame& F, const StarSet& SS,
+               cudaStream_t s);
+const float* trails_buffer(const bt_trails* t);
 int launch_view_sphere(float2* view, int W, int H, cudaStream_t s);
 int launch_sat(const uint8_t* bgr, int rows, int cols, float4* sat, cudaStream_t s);
 

@@ -459,7 +459,8 @@ __global__ void k_star_gather(const float3* __restrict__ cells,
                               const uint8_t* __restrict__ flag, int M, int N,
                               int step, float* __restrict__ light,
                               const uchar4* __restrict__ bg,
-                              uchar4* __restrict__ out, int map) {
+                              uchar4* __restrict__ out, int map,
+                              const float* __restrict__ trail) {
   const int j = blockIdx.x * TX + threadIdx.x;
   const int i = blockIdx.y * TY + threadIdx.y;
   if (i >= N || j >= M) return;
@@ -479,6 +480,11 @@ __global__ void k_star_gather(const float3* __restrict__ cells,
       b.z += factor * c.z;
     }
   const size_t ij = (size_t)i * M + j;
+  if (trail) {  // factor2 = 1, BT/MakeImageKernel.cu:766-770
+    b.x += 1.f * trail[3 * ij];
+    b.y += 1.f * trail[3 * ij + 1];
+    b.z += 1.f * trail[3 * ij + 2];
+  }
   if (!kCompose) {
     light[3 * ij] = b.x;
     light[3 * ij + 1] = b.y;
@@ -739,16 +745,21 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   else if (F.step == 1) launch_heavy<1>(Sc, F, SS, s);
   else launch_heavy<2>(Sc, F, SS, s);
   BT_CUDA_TRY(cudaGetLastError());
+  const float* trail = nullptr;
+  if (F.trails) {
+    if (int rc = trails_run(F.trails, Sc, F, SS, s)) return rc;
+    trail = trails_buffer(F.trails);
+  }
   const bool diff = F.diffraction && SS.psf && SS.psf_size > 0;
   if (!diff) {
     k_star_gather<true><<<grid2(M, N), dim3(TX, TY), 0, s>>>(
         Sc.cells, Sc.flag, M, N, F.step, Sc.light, (const uchar4*)F.out_bg,
-        (uchar4*)F.out, F.map);
+        (uchar4*)F.out, F.map, trail);
     BT_CUDA_TRY(cudaGetLastError());
     return BT_OK;
   }
   k_star_gather<false><<<grid2(M, N), dim3(TX, TY), 0, s>>>(
-      Sc.cells, Sc.flag, M, N, F.step, Sc.light, nullptr, nullptr, F.map);
+      Sc.cells, Sc.flag, M, N, F.step, Sc.light, nullptr, nullptr, F.map, trail);
   // the star cells are consumed: their buffer holds the coefficients
   float3* coef = Sc.cells;
   k_diff_coef<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(Sc.light, (int)np, coef);

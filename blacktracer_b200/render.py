@@ -212,6 +212,41 @@ class StarProcessor:
             self._h = None
 
 
+class Trails:
+    """Star trails between consecutive frames rendered with this object
+    (addTrails / makeGradField / clearArrays, BT/MakeImageKernel.cu:98-174,
+    517-537, 618-629).  Made for one star set and one output size."""
+
+    def __init__(self, n_stars, width, height, trailnum=30, max_hits=0):
+        h = C.c_void_p()
+        L.check(L.lib().bt_trails_create(int(n_stars), int(width), int(height), int(trailnum),
+                                         int(max_hits), C.byref(h)))
+        self._h = h
+        self.width, self.height = int(width), int(height)
+
+    def reset(self):
+        """The next frame is a first frame again (no trails)."""
+        L.check(L.lib().bt_trails_reset(self._h))
+
+    def query(self, stream=None):
+        """dict(frame, hits, dropped, walks_cut, trail: (H*W, 3) float32 CUDA
+        view of the last frame's trail light); synchronises."""
+        torch = _torch()
+        i = L.bt_trails_info()
+        L.check(L.lib().bt_trails_query(self._h, C.byref(i), _stream_ptr(stream)))
+        return dict(frame=i.frame, hits=i.hits, dropped=i.dropped, walks_cut=i.walks_cut,
+                    trail=_device_view(i.trail, (self.width * self.height, 3), torch.float32))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None:
+            try:
+                L.lib().bt_trails_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+
 class Renderer:
     """Per-resolution device scratch + the frame call (makeImage, G = 1)."""
 
@@ -224,11 +259,12 @@ class Renderer:
     def render(self, grid: Grid, viewer: Viewer, cam: Camera, env: Environment | None = None,
                stars: StarProcessor | None = None, lr=True, step=1, diffraction=False,
                hor=0.0, ver=0.0, out=None, stream=None, bb_table=0, psf_scale=False,
-               grid2=None, cam2=None, alpha=0.0, blend=None):
+               grid2=None, cam2=None, alpha=0.0, blend=None, trails=None):
         """Returns (or fills) an (H, W, 4) uint8 BGRA CUDA tensor.  bb_table=1
         selects the 1024-entry FP32 blackbody table, psf_scale scales the
         diffraction footprint by sqrt(pixel magnification); grid2 / cam2 /
-        alpha / blend (a prepared Blend) mix a second grid in."""
+        alpha / blend (a prepared Blend) mix a second grid in; trails (a
+        Trails) adds star trails from the previous frame rendered with it."""
         gp, rows, cols, _ = grid.map_grid()
         extra = {}
         if grid2 is not None:
@@ -237,12 +273,13 @@ class Renderer:
         return self.render_raw(gp, rows, cols, grid.MAXLEVEL, viewer.viewMatrix,
                                cam.getParamArray(), env=env, stars=stars, lr=lr, step=step,
                                diffraction=diffraction, hor=hor, ver=ver, out=out,
-                               stream=stream, bb_table=bb_table, psf_scale=psf_scale, **extra)
+                               stream=stream, bb_table=bb_table, psf_scale=psf_scale,
+                               trails=trails, **extra)
 
     def render_raw(self, grid_ptr, grid_rows, grid_cols, grid_level, view, cam7, env=None,
                    stars=None, lr=True, step=1, diffraction=False, hor=0.0, ver=0.0,
                    out=None, stream=None, bb_table=0, psf_scale=False, grid2=None,
-                   cam2=None, alpha=0.0, blend=None):
+                   cam2=None, alpha=0.0, blend=None, trails=None):
         """The same from a raw float2 grid (device pointer) and 7 camera floats."""
         torch = _torch()
         if out is None:
@@ -261,6 +298,7 @@ class Renderer:
             f.grid2, f.alpha, f.blend = grid2, float(alpha), blend._h
             f.cam2[:] = [float(x) for x in cam2]
         f.out = out.data_ptr()
+        f.trails = trails._h if trails is not None else None
         L.check(L.lib().bt_map_render(self._h, C.byref(f), _stream_ptr(stream)))
         return out
 

@@ -358,6 +358,9 @@ typedef struct bt_frame {
   float cam2[7];          /* getParamArray of grid2's camera: the frame uses
                              (1 - alpha) cam + alpha cam2 (camUpdate)       */
   const struct bt_blend* blend;  /* prepared on (grid, grid2)               */
+  /* Star trails from the previous frame rendered with the same trails
+   * object (NULL: none, as in the reference's first frame). */
+  struct bt_trails* trails;
 } bt_frame;
 
 /* Blending between two grids computed for neighbouring camera poses (the
@@ -379,6 +382,34 @@ int bt_blend_prepare(bt_blend* b, const float* grid_a, const float* grid_b, int 
  * prepare's stream has been synchronised. */
 int bt_blend_info(const bt_blend* b, const float** border, int32_t* angles,
                   uint32_t* walks_at_edge);
+
+/* Star trails between consecutive frames: addTrails, makeGradField and
+ * clearArrays (BT/MakeImageKernel.cu:98-174, 517-537, 618-629).  A frame
+ * rendered with bt_frame.trails draws, for every star seen in a pixel whose
+ * kd-tree search holds fewer than n_stars / 100 stars, a fading line from
+ * the position in the previous frame (of the same trails object) that best
+ * follows the celestial gradient, within width / 25 pixels and 45 degrees;
+ * the line is added to the star light.  A star's positions are cached per
+ * frame in ascending pixel order, up to trailnum (the reference uses 30).
+ * The first frame after create / reset draws none.  The reference's line
+ * walk can step past its target and never end; here it stops there
+ * (walks_cut counts those), and crossing lines keep the brighter value per
+ * channel.  max_hits (0 = width * height) bounds the (pixel, star) pairs per
+ * frame; pairs past it draw no trail (dropped). */
+typedef struct bt_trails bt_trails;
+int bt_trails_create(int n_stars, int width, int height, int trailnum, size_t max_hits,
+                     bt_trails** out);
+void bt_trails_destroy(bt_trails* t);
+int bt_trails_reset(bt_trails* t);
+typedef struct bt_trails_info {
+  int64_t frame;        /* frames rendered since create / reset             */
+  uint32_t hits;        /* (pixel, star) pairs of the last frame            */
+  uint32_t dropped;     /* pairs beyond max_hits                            */
+  uint32_t walks_cut;   /* line walks stopped at their target               */
+  const float* trail;   /* DEVICE: the last frame's trail light, 3 per pixel */
+} bt_trails_info;
+/* Synchronises `stream` (the stream of the last frame). */
+int bt_trails_query(bt_trails* t, bt_trails_info* info, void* stream);
 
 /* An Airy diffraction sprite (size x size RGB8, the layout the reference
  * loads its diffraction image in, BT/MakeImageKernel.cu:1281-1286):

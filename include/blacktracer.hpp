@@ -366,6 +366,7 @@ class StarProcessor {
 class Distorter {
  public:
   bool star = true, map = true, lr = true, diffraction = false;
+  bool trails = false;  // star trails from the previous frame (addTrails)
   int step = 1;
 
   Distorter(std::vector<Grid>* grids, Viewer* viewer, StarProcessor* stars,
@@ -395,6 +396,7 @@ class Distorter {
   Distorter(const Distorter&) = delete;
   Distorter& operator=(const Distorter&) = delete;
   ~Distorter() {
+    if (trails_) bt_trails_destroy(trails_);
     if (blend_) bt_blend_destroy(blend_);
     if (env_) bt_env_destroy(env_);
     if (m_) bt_map_destroy(m_);
@@ -439,6 +441,12 @@ class Distorter {
     f.step = step;
     f.diffraction = diffraction ? 1 : 0;
     f.out = out_bgra;
+    if (trails && f.star) {
+      if (!trails_)
+        check(bt_trails_create(stars_->starSize, view_->pixelwidth, view_->pixelheight, 30, 0,
+                               &trails_));
+      f.trails = trails_;
+    }
     if (G > 1) {
       const float* grid2 = nullptr;
       int32_t rows2 = 0, cols2 = 0;
@@ -477,6 +485,7 @@ class Distorter {
   bt_map* m_ = nullptr;
   bt_env* env_ = nullptr;
   bt_blend* blend_ = nullptr;
+  bt_trails* trails_ = nullptr;
   int prepared_ = -1;  // grid pair the blend was prepared for
   DeviceArray<uint8_t> out_;
 };

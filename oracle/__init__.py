@@ -425,3 +425,65 @@ def ref_view_camera(view_angle, off_up, off_right, width, height):
     out = np.zeros(2 * (height + 1) * (width + 1), np.float32)
     lib.btref_view_camera(view_angle, off_up, off_right, width, height, out)
     return out.reshape(-1, 2)
+
+
+# ---------------------------------------------------------------- trails (reference)
+def ref_trail_cache(thphi, bh, area, cam7, stars, width, height, step, view, lr, trailnum=30):
+    """The star caches and hit counts the reference's frame-0 star pass
+    leaves (no line is drawn at frame 0).  stars = (pos, mag, tree, level).
+    Returns (cache (n, trailnum, 2) int32, counts (n,) int32)."""
+    lib = _refmaplib()
+    pos, mg, tree, tl = stars
+    n = len(pos) // 2
+    lib.btref_trail_cache.argtypes = [C.c_void_p, _u8p, _f32p, _i32, C.c_int, _f32p, _f32p,
+                                      C.c_int, C.c_int, C.c_int, C.c_int, _f32p, C.c_int,
+                                      _f32p, C.c_int, _i32, _i32]
+    M, N = width, height
+    th = _trail_corners(thphi, M, N)
+    cache = np.zeros(n * trailnum * 2, np.int32)
+    cnt = np.zeros(n, np.int32)
+    lib.btref_trail_cache(C.c_void_p(th.ctypes.data), np.ascontiguousarray(bh, np.uint8),
+                          np.ascontiguousarray(pos, np.float32),
+                          np.ascontiguousarray(tree, np.int32), n,
+                          np.ascontiguousarray(cam7, np.float32),
+                          np.ascontiguousarray(mg, np.float32), tl, M, N, step,
+                          np.ascontiguousarray(view, np.float32), int(lr),
+                          np.ascontiguousarray(area, np.float32), trailnum, cache, cnt)
+    return cache.reshape(n, trailnum, 2), cnt
+
+
+def _trail_corners(thphi, M, N):
+    # makeGradField reads one element past the corner array: an absent corner
+    th = np.full(((N + 1) * (M + 1) + 1) * 2, -2.0, np.float32)
+    th[:(N + 1) * (M + 1) * 2] = np.asarray(thphi, np.float32).reshape(-1)
+    return th
+
+
+def ref_trail_frames(f0, f1, stars, width, height, step, view, lr, trailnum=30):
+    """Frames 0 and 1 through the reference's trail code (clearArrays,
+    makeGradField, distortStarMap with addTrails, sumStarLight).  f0, f1 =
+    (thphi, bh, area, cam7).  Returns (trail of frame 1 (N*M, 3), light of
+    frame 1 (N*M, 3)).  Run only where oracle.trails.plan says every walk
+    ends."""
+    lib = _refmaplib()
+    pos, mg, tree, tl = stars
+    n = len(pos) // 2
+    M, N = width, height
+    lib.btref_trail_frames.argtypes = ([C.c_void_p, _u8p, _f32p, _f32p] * 2 +
+                                       [_f32p, _i32, C.c_int, _f32p, C.c_int, C.c_int, C.c_int,
+                                        C.c_int, _f32p, C.c_int, C.c_int, _f32p, _f32p])
+    keep = []
+    args = []
+    for (thphi, bh, area, cam7) in (f0, f1):
+        th = _trail_corners(thphi, M, N)
+        keep.append(th)
+        args += [C.c_void_p(th.ctypes.data), np.ascontiguousarray(bh, np.uint8),
+                 np.ascontiguousarray(area, np.float32), np.ascontiguousarray(cam7, np.float32)]
+    trail = np.zeros(N * M * 3, np.float32)
+    light = np.zeros(N * M * 3, np.float32)
+    lib.btref_trail_frames(*args, np.ascontiguousarray(pos, np.float32),
+                           np.ascontiguousarray(tree, np.int32), n,
+                           np.ascontiguousarray(mg, np.float32), tl, M, N, step,
+                           np.ascontiguousarray(view, np.float32), int(lr), trailnum, trail,
+                           light)
+    return trail.reshape(-1, 3), light.reshape(-1, 3)

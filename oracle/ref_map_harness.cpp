@@ -242,6 +242,108 @@ void btref_map_compose(const unsigned char* stars, const unsigned char* bg,
     }
 }
 
+// ---- trails (addTrails / makeGradField / clearArrays) ----
+// One frame's star pass as the reference's driver runs it
+// (BT/MakeImageKernel.cu:1481-1497): clearArrays, makeGradField,
+// distortStarMap, then sumStarLight (which adds and clears the trail buffer).
+// Pixels run in ascending order, so the per-star caches list pixels in that
+// order.  thphi is read one element past the corner array by makeGradField;
+// the caller pads it with an absent (-2) value.
+struct TrailRun {
+  int M, N, step, filterW, searchNr, trailnum, starSize;
+  std::vector<float3> scratch;
+  std::vector<int> search;
+  std::vector<int2> stCache;
+  std::vector<int> stnums;
+  std::vector<float3> trail;
+  std::vector<float2> grad;
+};
+
+static void trail_frame(TrailRun& R, int frame, const float* thphi, const unsigned char* bh,
+                        const float* stars, const int* tree, const float* cam7,
+                        const float* mag, int treeLevel, const float* view, int lr,
+                        const float* area, float* trail_out, float* light, int with_sum) {
+  const int M = R.M, N = R.N;
+  for (int q = 0; q < R.starSize; q++) {
+    at(q, 0);
+    clearArrays(R.stnums.data(), R.stCache.data(), frame, R.trailnum, R.starSize);
+  }
+  for (int i = 0; i <= N; i++)
+    for (int j = 0; j <= M; j++) {
+      at(i, j);
+      makeGradField((const float2*)thphi, M, N, R.grad.data());
+    }
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      distortStarMap(R.scratch.data(), (const float2*)thphi, bh, stars, tree, R.starSize, cam7,
+                     mag, treeLevel, M, N, R.step, 0.f, R.search.data(), R.searchNr,
+                     R.stCache.data(), R.stnums.data(), R.trail.data(), R.trailnum,
+                     R.grad.data(), frame, (const float2*)view, lr != 0, area);
+    }
+  if (trail_out) memcpy(trail_out, R.trail.data(), R.trail.size() * sizeof(float3));
+  if (!with_sum) return;
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      sumStarLight(R.scratch.data(), R.trail.data(), (float3*)light, R.step, M, N, R.filterW);
+    }
+}
+
+static void trail_init(TrailRun& R, int M, int N, int step, int treeLevel, int starSize,
+                       int trailnum) {
+  R.M = M; R.N = N; R.step = step; R.filterW = 2 * step + 1;
+  R.searchNr = (int)powf(2, treeLevel / 3 * 2);
+  R.trailnum = trailnum;
+  R.starSize = starSize;
+  R.scratch.assign((size_t)N * M * R.filterW * R.filterW, float3{0.f, 0.f, 0.f});
+  R.search.assign((size_t)N * M * R.searchNr + 64 * R.searchNr, 0);
+  R.stCache.assign((size_t)2 * starSize * trailnum, int2{-1, -1});
+  R.stnums.assign(starSize, 0);
+  R.trail.assign((size_t)N * M, float3{0.f, 0.f, 0.f});
+  R.grad.assign((size_t)(N + 1) * (M + 1), float2{0.f, 0.f});
+}
+
+// Frame 0 only (no line is drawn at frame 0): the star caches it leaves --
+// per star up to trailnum pixels (i, j) in ascending order -- and the number
+// of hits per star.  Safe to run on any input.
+void btref_trail_cache(const float* thphi, const unsigned char* bh, const float* stars,
+                       const int* tree, int starSize, const float* cam7, const float* mag,
+                       int treeLevel, int M, int N, int step, const float* view, int lr,
+                       const float* area, int trailnum, int* cache_out, int* stnums_out) {
+  TrailRun R;
+  trail_init(R, M, N, step, treeLevel, starSize, trailnum);
+  trail_frame(R, 0, thphi, bh, stars, tree, cam7, mag, treeLevel, view, lr, area, nullptr,
+              nullptr, 0);
+  for (int q = 0; q < starSize; q++) {
+    stnums_out[q] = R.stnums[q];
+    for (int w = 0; w < trailnum; w++) {
+      const int2 c = R.stCache[2 * (trailnum * q) + w];  // parity 0
+      cache_out[2 * (trailnum * q + w)] = c.x;
+      cache_out[2 * (trailnum * q + w) + 1] = c.y;
+    }
+  }
+}
+
+// Frames 0 and 1 in sequence; the trail buffer of frame 1 before
+// sumStarLight consumes it, and frame 1's summed star light.  Only for inputs
+// where every line walk of frame 1 ends (the reference's walk can run on
+// forever); the caller checks that first.
+void btref_trail_frames(const float* thphi0, const unsigned char* bh0, const float* area0,
+                        const float* cam0, const float* thphi1, const unsigned char* bh1,
+                        const float* area1, const float* cam1, const float* stars,
+                        const int* tree, int starSize, const float* mag, int treeLevel, int M,
+                        int N, int step, const float* view, int lr, int trailnum,
+                        float* trail_out, float* light_out) {
+  TrailRun R;
+  trail_init(R, M, N, step, treeLevel, starSize, trailnum);
+  std::vector<float> light((size_t)N * M * 3);
+  trail_frame(R, 0, thphi0, bh0, stars, tree, cam0, mag, treeLevel, view, lr, area0, nullptr,
+              light.data(), 1);
+  trail_frame(R, 1, thphi1, bh1, stars, tree, cam1, mag, treeLevel, view, lr, area1, trail_out,
+              light_out, 1);
+}
+
 // searchTree for one bounding box (picheck = 0, as distortStarMap calls it).
 int btref_search_tree(const int* tree, const float* mn, const float* mx,
                       int treeLevel, int* nodes, int cap) {
