@@ -51,6 +51,15 @@ F_ATTEMPT_FORM = {"plain": F_ATTEMPT, "mixed": F_ATTEMPT,
 WORKLOAD = dict(maxlevel=11, startlevel=6, a=0.999, r=5.0, theta=np.pi / 2)
 
 
+def hbm_peak():
+    """Measured copy bandwidth of this pool's B200s (GB/s), else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return 6650.0, "fallback (6.65 TB/s)"
+
+
 def c2_camera(bt):
     return bt.Camera(WORKLOAD["theta"], 0.0, WORKLOAD["r"], 0.0, 0.0, 1.0, a=WORKLOAD["a"])
 
@@ -339,6 +348,13 @@ def full_frame(bt, torch, n_frames):
            "frame_p99_ms": float(np.percentile(lat, 99)), "frames": n_frames,
            "frame_plus_grid_ms": float(np.percentile(lat, 50)) + build_ms,
            "setup_s": setup_s}
+    t0 = time.perf_counter()
+    cen = R.census()
+    res["star_census"] = {
+        "pixels": cen["star_pixels"],
+        "candidates_per_pixel_reference": cen["star_candidates_ref"] / max(1, cen["star_pixels"]),
+        "candidates_per_pixel": cen["star_candidates"] / max(1, cen["star_pixels"]),
+        "census_s": time.perf_counter() - t0}
     del R, out, sp, env, g
     torch.cuda.empty_cache()
     return res
@@ -600,13 +616,57 @@ def main():
             torch.cuda.synchronize()
             lat_e2e.append((time.perf_counter() - t0) * 1e3)
         lat = np.array(lat)
+        # map roofline: algorithmic bytes of the frame over its p50 time
+        cen = R.census()
+        gptr, grows, gcols, _ = grid.map_grid()
+        n_stars = int(sp.starSize)
+        algo = (8 * grows * gcols + 8 * (W + 1) * (H + 1) + 32 * cen["env_columns"] +
+                16 * n_stars + 4 * W * H)
+        hbm, hbm_src = hbm_peak()
+        ach = algo / (float(np.percentile(lat, 50)) / 1e3) / 1e9
+        map_roofline = {
+            "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+            "peak_source": hbm_src, "algorithmic_bytes": int(algo),
+            "bytes_formula": "8*GN*GM (map grid) + 8*(W+1)(H+1) (view) + 32*sum(pixNum+1) "
+                             "(summed-area pairs) + 16*N_stars + 4*W*H (BGRA8 out)",
+            "env_columns": cen["env_columns"], "note": "whole frame (every map kernel) at "
+                                                       "the p50 frame time"}
+        star_census = {
+            "pixels": cen["star_pixels"],
+            "candidates_per_pixel_reference": cen["star_candidates_ref"] / max(1, cen["star_pixels"]),
+            "candidates_per_pixel": cen["star_candidates"] / max(1, cen["star_pixels"]),
+            "note": "reference: stars of the kd-tree nodes its search emits (starsToCheck); "
+                    "this build: stars of the leaves left after node-box pruning"}
+        cpu_map = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            import oracle
+            if oracle.have_ref_map():
+                from blacktracer_b200.render import _device_view
+                gmap = _device_view(gptr, (grows * gcols, 2), torch.float32).cpu().numpy()
+                sat = env.sat().cpu().numpy()
+                cores = os.cpu_count() or 1
+                rt = oracle.ref_map_time(gmap, grows, gcols, grid.MAXLEVEL,
+                                         viewer.viewMatrix.cpu().numpy(), W, H,
+                                         cam.getParamArray(), sat, env.rows, env.cols,
+                                         (sp.starPos, sp.starMag, sp.binaryStarTree,
+                                          sp.treeLevel), row_stride=16, nthreads=cores)
+                del gmap, sat
+                cpu_map = {"value": 1.0 / rt["frame_s"], "unit": "frames/s", "cores": cores,
+                           "kind": "reference", "phases_s": rt,
+                           "sample": f"the reference's map kernels (BT/MakeImageKernel.cu) "
+                                     f"compiled for the host, OpenMP over rows: corners and "
+                                     f"areas over the whole 4K frame, environment and stars "
+                                     f"over every 16th row ({rt['rows_sampled']} rows) scaled "
+                                     f"to the frame; the per-pixel sums and the composite "
+                                     f"are not timed"}
         frames = {"fps": float(1e3 / lat.mean()), "p50_ms": float(np.percentile(lat, 50)),
                   "p99_ms": float(np.percentile(lat, 99)),
                   "e2e_fps": float(1e3 / np.mean(lat_e2e)),
                   "e2e_p99_ms": float(np.percentile(lat_e2e, 99)),
                   "d2h_bytes_per_frame": W * H * 4, "width": W, "height": H,
                   "env": "8192x4096 BGR8 value noise", "stars": 1_000_000, "tree_level": 14,
-                  "lensing_redshift": True}
+                  "lensing_redshift": True, "roofline": map_roofline,
+                  "star_census": star_census, "cpu_baseline": cpu_map}
 
     # batched grids (64 poses, L6 -> L9): one set, graph-captured, launch shape
     # from the autotuner; plain and mixed; the sets are larger than L2
@@ -690,6 +750,22 @@ def main():
             cpu = {"value": traced / secs, "unit": "geodesics/s", "cores": 1, "kind": "reference",
                    "sample": f"one full grid build (Grid::Grid, L6->L11, {traced} rays, "
                              f"{secs:.2f} s incl. its perfect hash) on one host thread"}
+            # 8-way: the grid's rays split into 8 disjoint slices, integration_wrapper
+            # on 8 threads (it only reads the camera and the spin)
+            d = grid.dense()
+            ii, jj = np.nonzero((d["exists"] == 1).cpu().numpy())
+            del d
+            keep = ~(((ii == 0) | (ii == grid.N - 1)) & (jj != 0))
+            th8 = ii[keep] / (grid.N - 1) * np.pi
+            ph8 = jj[keep] / grid.M * 2 * np.pi
+            t0 = time.perf_counter()
+            oracle.integrate_rays(camr, WORKLOAD["a"], th8, ph8, ref=True, nthreads=8)
+            s8 = time.perf_counter() - t0
+            cpu["eight_way"] = {"value": len(th8) / s8, "unit": "geodesics/s", "cores": 8,
+                                "kind": "reference",
+                                "sample": f"the grid's {len(th8)} traced rays through "
+                                          f"Grid::integration_wrapper on 8 threads "
+                                          f"({s8:.2f} s)"}
 
     if rank == 0:
         line = {

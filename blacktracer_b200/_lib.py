@@ -99,6 +99,11 @@ class bt_frame(C.Structure):
                 ("blend", C.c_void_p), ("trails", C.c_void_p)]
 
 
+class bt_map_census_t(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("env_columns", "env_pixels", "star_pixels",
+                                          "star_candidates_ref", "star_candidates")]
+
+
 class bt_trails_info(C.Structure):
     _fields_ = [("frame", C.c_int64), ("hits", C.c_uint32), ("dropped", C.c_uint32),
                 ("walks_cut", C.c_uint32), ("trail", C.c_void_p)]
@@ -210,6 +215,7 @@ _SIGS = {
     "bt_trails_destroy": (None, [_vp]),
     "bt_trails_reset": (C.c_int, [_vp]),
     "bt_trails_query": (C.c_int, [_vp, C.POINTER(bt_trails_info), _vp]),
+    "bt_map_census": (C.c_int, [_vp, C.POINTER(bt_frame), C.POINTER(bt_map_census_t), _vp]),
     "bt_last_error": (C.c_char_p, []),
     "bt_version": (C.c_char_p, []),
 }

@@ -578,6 +578,39 @@ int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s) {
   return BT_OK;
 }
 
+// Census of the environment pass of the last frame: per coloured pixel the
+// environment columns it spans (pixNum, BT/MakeImageKernel.cu:650-657);
+// sums pixNum + 1 and the pixels into out[0] and out[1].
+__global__ void k_env_census(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
+                             int rows, int M, int N, unsigned long long* out) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  unsigned long long cols = 0, px = 0;
+  if (i < N && j < M && bh[(size_t)i * M + j] == 0) {
+    float t[4], p[4];
+    bool picheck = false;
+    const int ind = i * (M + 1) + j;
+    if (pixel_corners(thphi, ind, M, t, p, picheck, 0.f) && ind > 0) {
+      cols = (unsigned long long)(env_span(p, rows).pixNum + 1);
+      px = 1;
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    cols += __shfl_down_sync(0xffffffffu, cols, o);
+    px += __shfl_down_sync(0xffffffffu, px, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (cols || px)) {
+    atomicAdd(out, cols);
+    atomicAdd(out + 1, px);
+  }
+}
+
+int map_env_census(const MapScratch& S, int env_rows, unsigned long long* out, cudaStream_t s) {
+  k_env_census<<<grid2(S.M, S.N), dim3(TX, TY), 0, s>>>(S.thphi, S.bh, env_rows, S.M, S.N, out);
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
 int launch_view_sphere(float2* view, int W, int H, cudaStream_t s) {
   k_view_sphere<<<grid2(W + 1, H + 1), dim3(TX, TY), 0, s>>>(view, W, H);
   BT_CUDA_TRY(cudaGetLastError());

@@ -11,6 +11,16 @@ struct bt_env {
   bt::EnvMap e;
 };
 
+struct bt_blend {
+  float2* border;   // 2 + 2 * nang: the box, then (grid a, grid b) per direction
+  float2* border2;
+  uint32_t* edge;
+  uint32_t* edge_host;
+  int nang;
+  int rows, cols;
+  int ready;
+};
+
 struct bt_map {
   bt::MapScratch S;
   uint8_t* tmp_img;  // env image when stars are composited on top
@@ -30,6 +40,43 @@ void map_free(bt_map* m) {
     if (p) cudaFree(p);
 }
 
+}  // namespace
+
+namespace {
+// The frame description of bt_frame for the map passes.
+MapFrame frame_of(const bt_frame* f) {
+  MapFrame F;
+  F.grid = (const float2*)f->grid;
+  F.GN = f->grid_rows;
+  F.GM = f->grid_cols;
+  F.gridlvl = f->grid_level;
+  F.view = (const float2*)f->view;
+  F.hor = f->hor;
+  F.ver = f->ver;
+  for (int q = 0; q < 7; q++) F.cam.v[q] = f->cam[q];
+  F.env = f->env ? &f->env->e : nullptr;
+  F.stars = f->stars;
+  F.bb_table = f->bb_table;
+  F.psf_scale = f->psf_scale;
+  F.grid2 = (const float2*)f->grid2;
+  F.blend_border = nullptr;
+  F.blend_angles = 0;
+  F.alpha = f->alpha;
+  if (f->grid2) {
+    // camUpdate (BT/MakeImageKernel.cu:386-389): the camera between the two
+    for (int q = 0; q < 7; q++) F.cam.v[q] = (1.f - f->alpha) * f->cam[q] + f->alpha * f->cam2[q];
+    F.blend_border = f->blend->border;
+    F.blend_angles = f->blend->nang;
+  }
+  F.map = f->map;
+  F.star = f->star;
+  F.lr = f->lr;
+  F.step = f->step;
+  F.diffraction = f->diffraction;
+  F.out = f->out;
+  F.trails = f->trails;
+  return F;
+}
 }  // namespace
 
 extern "C" {
@@ -96,16 +143,6 @@ int bt_env_sat(const bt_env* e, const float** sat, int32_t* rows, int32_t* cols)
   if (cols) *cols = e->e.cols;
   return BT_OK;
 }
-
-struct bt_blend {
-  float2* border;   // 2 + 2 * nang: the box, then (grid a, grid b) per direction
-  float2* border2;
-  uint32_t* edge;
-  uint32_t* edge_host;
-  int nang;
-  int rows, cols;
-  int ready;
-};
 
 int bt_blend_create(bt_blend** out) {
   clear_error();
@@ -237,36 +274,7 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
                              f->blend->cols == f->grid_cols),
                "a second grid needs a blend prepared on grids of the same shape");
   cudaStream_t s = (cudaStream_t)stream;
-  MapFrame F;
-  F.grid = (const float2*)f->grid;
-  F.GN = f->grid_rows;
-  F.GM = f->grid_cols;
-  F.gridlvl = f->grid_level;
-  F.view = (const float2*)f->view;
-  F.hor = f->hor;
-  F.ver = f->ver;
-  for (int q = 0; q < 7; q++) F.cam.v[q] = f->cam[q];
-  F.env = f->env ? &f->env->e : nullptr;
-  F.stars = f->stars;
-  F.bb_table = f->bb_table;
-  F.psf_scale = f->psf_scale;
-  F.grid2 = (const float2*)f->grid2;
-  F.blend_border = nullptr;
-  F.blend_angles = 0;
-  F.alpha = f->alpha;
-  if (f->grid2) {
-    // camUpdate (BT/MakeImageKernel.cu:386-389): the camera between the two
-    for (int q = 0; q < 7; q++) F.cam.v[q] = (1.f - f->alpha) * f->cam[q] + f->alpha * f->cam2[q];
-    F.blend_border = f->blend->border;
-    F.blend_angles = f->blend->nang;
-  }
-  F.map = f->map;
-  F.star = f->star;
-  F.lr = f->lr;
-  F.step = f->step;
-  F.diffraction = f->diffraction;
-  F.out = f->out;
-  F.trails = f->trails;
+  MapFrame F = frame_of(f);
   // environment into the output directly, or into a temporary when stars
   // are composited on top (addStarsAndBackground)
   F.out_bg = (f->star && f->map) ? m->tmp_img : f->out;
@@ -276,6 +284,37 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
     rc = map_run_stars(m->S, F, s);
     if (rc) return rc;
   }
+  return BT_OK;
+}
+
+int bt_map_census(bt_map* m, const bt_frame* f, bt_map_census_t* out, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(m && f && out, "NULL pointer");
+  BT_ARG_CHECK(f->view && (!f->map || f->env) && (!f->star || f->stars),
+               "the frame description of the last render is needed");
+  cudaStream_t s = (cudaStream_t)stream;
+  const MapFrame F = frame_of(f);
+  unsigned long long* dev = nullptr;
+  BT_CUDA_TRY(cudaMallocAsync((void**)&dev, 8 * sizeof(unsigned long long), s));
+  unsigned long long host[8] = {0};
+  cudaError_t e = cudaMemsetAsync(dev, 0, 8 * sizeof(unsigned long long), s);
+  int rc = BT_OK;
+  if (e == cudaSuccess && f->map) rc = map_env_census(m->S, f->env->e.rows, dev, s);
+  if (e == cudaSuccess && rc == BT_OK && f->star) rc = map_star_census(m->S, F, dev + 2, s);
+  if (e == cudaSuccess && rc == BT_OK)
+    e = cudaMemcpyAsync(host, dev, sizeof(host), cudaMemcpyDeviceToHost, s);
+  cudaFreeAsync(dev, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    set_error("census: %s", cudaGetErrorString(e));
+    return BT_ERR_CUDA;
+  }
+  if (rc) return rc;
+  out->env_columns = host[0];
+  out->env_pixels = host[1];
+  out->star_pixels = host[2];
+  out->star_candidates_ref = host[3];
+  out->star_candidates = host[4];
   return BT_OK;
 }
 

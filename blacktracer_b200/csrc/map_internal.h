@@ -72,6 +72,10 @@ StarSet stars_for_frame(const bt_stars* s, int bb_table);
 int trails_run(bt_trails* t, MapScratch& Sc, const MapFrame& F, const StarSet& SS,
                cudaStream_t s);
 const float* trails_buffer(const bt_trails* t);
+// Census of the last frame's environment and star passes (bt_map_census).
+int map_env_census(const MapScratch& S, int env_rows, unsigned long long* out, cudaStream_t s);
+int map_star_census(const MapScratch& Sc, const MapFrame& F, unsigned long long* out,
+                    cudaStream_t s);
 int launch_view_sphere(float2* view, int W, int H, cudaStream_t s);
 int launch_sat(const uint8_t* bgr, int rows, int cols, float4* sat, cudaStream_t s);
 

@@ -715,6 +715,59 @@ __global__ void k_makepix(const float* __restrict__ light, int M, int N,
   out[ij] = st;
 }
 
+// Census of the star pass of the last frame, per pixel outside the shadow:
+// the stars in the kd-tree nodes the search emits (the reference tests all
+// of them, its starsToCheck) and the stars in the leaves left after the
+// node-box pruning (the candidates tested here).  Sums into out[0..2]:
+// pixels, reference candidates, candidates.
+__global__ void k_star_census(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
+                              StarSet S, Cam7 cam, int M, int N, int step,
+                              const float2* __restrict__ view, int lr,
+                              const float* __restrict__ area, unsigned long long* out) {
+  const int j = blockIdx.x * TX + threadIdx.x;
+  const int i = blockIdx.y * TY + threadIdx.y;
+  unsigned long long px = 0, ref = 0, ours = 0;
+  if (i < N && j < M) {
+    PixelStars P;
+    float mn[2], mx[2];
+    if (pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, i, j, P, mn, mx)) {
+      px = 1;
+      P.budget = 0x7fffffffffffL;
+      tree_search(S, mn, mx, [&](int node) {
+        int a0, a1;
+        node_range(S, node, a0, a1);
+        ref += (unsigned long long)(a1 - a0);
+        walk_leaves(P, S, node, node_level(node), [&](int leaf) {
+          int b0, b1;
+          node_range(S, leaf, b0, b1);
+          ours += (unsigned long long)(b1 - b0);
+          return true;
+        });
+        return true;
+      });
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    px += __shfl_down_sync(0xffffffffu, px, o);
+    ref += __shfl_down_sync(0xffffffffu, ref, o);
+    ours += __shfl_down_sync(0xffffffffu, ours, o);
+  }
+  if ((threadIdx.x & 31) == 0 && px) {
+    atomicAdd(out, px);
+    atomicAdd(out + 1, ref);
+    atomicAdd(out + 2, ours);
+  }
+}
+
+int map_star_census(const MapScratch& Sc, const MapFrame& F, unsigned long long* out,
+                    cudaStream_t s) {
+  const StarSet SS = stars_for_frame(F.stars, F.bb_table);
+  k_star_census<<<grid2(Sc.M, Sc.N), dim3(TX, TY), 0, s>>>(
+      Sc.thphi, Sc.bh, SS, F.cam, Sc.M, Sc.N, F.step, F.view, F.lr, Sc.area, out);
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
 int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   const int M = Sc.M, N = Sc.N;
   const StarSet SS = stars_for_frame(F.stars, F.bb_table);

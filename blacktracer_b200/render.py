@@ -300,7 +300,21 @@ class Renderer:
         f.out = out.data_ptr()
         f.trails = trails._h if trails is not None else None
         L.check(L.lib().bt_map_render(self._h, C.byref(f), _stream_ptr(stream)))
+        self._last = (f, env, stars, view)
         return out
+
+    def census(self, stream=None):
+        """Work of the last frame: dict(env_columns, env_pixels, star_pixels,
+        star_candidates_ref, star_candidates) -- environment columns spanned
+        (sum of pixNum + 1), and star candidates per pixel as the reference
+        tests them (its starsToCheck) and as this build does after pruning."""
+        last = getattr(self, "_last", None)
+        if last is None:
+            raise L.BtError(L.BT_ERR_STATE, "no frame rendered yet")
+        c = L.bt_map_census_t()
+        L.check(L.lib().bt_map_census(self._h, C.byref(last[0]), C.byref(c),
+                                      _stream_ptr(stream)))
+        return {k: int(getattr(c, k)) for k, _ in c._fields_}
 
     def scratch(self):
         """Device views of the frame's intermediates (thphi, gap, bh, area, light)."""

@@ -434,6 +434,22 @@ typedef struct bt_map_buffers {
 } bt_map_buffers;
 int bt_map_scratch(const bt_map* m, bt_map_buffers* b);
 
+/* Work census of the last frame a renderer drew (f: that frame's
+ * description): the environment columns the pixels span (distortEnvironment
+ * Map's pixNum, BT/MakeImageKernel.cu:650-657; two summed-area reads each)
+ * and the star candidates per pixel, those of the kd-tree nodes the search
+ * emits (the reference tests them all, its starsToCheck :265-275) and those
+ * left after this build's node-box pruning.  Synchronises `stream`.  For
+ * rooflines and reports; no counterpart in the reference. */
+typedef struct bt_map_census_t {
+  uint64_t env_columns;          /* sum over coloured pixels of pixNum + 1     */
+  uint64_t env_pixels;           /* pixels coloured from the environment       */
+  uint64_t star_pixels;          /* pixels outside the shadow                  */
+  uint64_t star_candidates_ref;  /* sum of starsToCheck                        */
+  uint64_t star_candidates;      /* sum of stars in the leaves tested here     */
+} bt_map_census_t;
+int bt_map_census(bt_map* m, const bt_frame* f, bt_map_census_t* out, void* stream);
+
 /* ----------------------------------------------------------- cache files */
 
 /* The reference's grid and star cache files (cereal binary archives,

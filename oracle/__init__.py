@@ -487,3 +487,39 @@ def ref_trail_frames(f0, f1, stars, width, height, step, view, lr, trailnum=30):
                            np.ascontiguousarray(view, np.float32), int(lr), trailnum, trail,
                            light)
     return trail.reshape(-1, 3), light.reshape(-1, 3)
+
+
+def ref_map_time(grid_f2, grid_rows, grid_cols, gridlvl, view, width, height, cam7, sat,
+                 env_rows, env_cols, stars, step=1, lr=True, row_stride=16, nthreads=0):
+    """The reference's per-pixel map kernels timed on host threads
+    (btref_map_time): corners and areas over the whole frame, environment and
+    stars over every row_stride-th row.  stars = (pos, mag, tree, level); sat
+    (env_rows*env_cols*4 float32).  Returns dict(secs per phase, rows sampled,
+    frame_s = the phases scaled to the whole frame)."""
+    lib = _refmaplib()
+    M, N = width, height
+    pos, mg, tree, tl = stars
+    pad = 2 * grid_rows + 8
+    g = np.full(((grid_rows + 2 * pad) * grid_cols, 2), -2.0, np.float32)
+    g[pad * grid_cols:(pad + grid_rows) * grid_cols] = np.asarray(grid_f2, np.float32).reshape(-1, 2)
+    s = np.zeros((env_rows + 4) * env_cols * 4, np.float32)
+    s[2 * env_cols * 4:(env_rows + 2) * env_cols * 4] = np.asarray(sat, np.float32).reshape(-1)
+    lib.btref_map_time.argtypes = [_f32p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                   C.c_void_p, C.c_int, C.c_int, _f32p, _i32, C.c_int, _f32p,
+                                   C.c_int, _f32p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   np.ctypeslib.ndpointer(dtype=np.float64)]
+    lib.btref_map_time.restype = C.c_int
+    secs = np.zeros(4, np.float64)
+    nr = lib.btref_map_time(np.ascontiguousarray(view, np.float32), M, N,
+                            C.c_void_p(g.ctypes.data + pad * grid_cols * 8), grid_cols, grid_rows,
+                            gridlvl, C.c_void_p(s.ctypes.data + 2 * env_cols * 16), env_rows,
+                            env_cols, np.ascontiguousarray(pos, np.float32),
+                            np.ascontiguousarray(tree, np.int32), len(pos) // 2,
+                            np.ascontiguousarray(mg, np.float32), tl,
+                            np.ascontiguousarray(cam7, np.float32), step, int(lr), row_stride,
+                            nthreads, secs)
+    if nr <= 0:
+        raise RuntimeError("reference map timing failed")
+    frame = secs[0] + secs[1] + (secs[2] + secs[3]) * N / nr
+    return dict(corners_s=float(secs[0]), area_s=float(secs[1]), env_rows_s=float(secs[2]),
+                stars_rows_s=float(secs[3]), rows_sampled=int(nr), frame_s=float(frame))

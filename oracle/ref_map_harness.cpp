@@ -23,7 +23,11 @@
 #include <cstdint>
 #include <cstring>
 #include <strings.h>
+#include <sys/mman.h>
+#include <chrono>
 #include <vector>
+
+#include <omp.h>
 
 #include "opencv2/core/core.hpp"
 // threadIdx & co become per-thread host variables the driver sets.
@@ -46,7 +50,9 @@ using namespace std;
 typedef unsigned int uint;
 
 // ---- device intrinsics used by the kernels, for one host thread ----
-static inline int atomicAdd(int* p, int v) { int o = *p; *p += v; return o; }
+// int atomicAdd is a real atomic: the timing driver below runs pixels on
+// several host threads (addTrails counts hits per star with it).
+static inline int atomicAdd(int* p, int v) { return __atomic_fetch_add(p, v, __ATOMIC_RELAXED); }
 static inline float atomicAdd(float* p, float v) { float o = *p; *p += v; return o; }
 static inline int atomicMin(int* p, int v) { int o = *p; *p = std::min(o, v); return o; }
 static inline int atomicMax(int* p, int v) { int o = *p; *p = std::max(o, v); return o; }
@@ -68,6 +74,27 @@ inline void at(int i, int j) {
   blockIdx.x = i; blockIdx.y = j; blockIdx.z = 0;
   threadIdx.x = threadIdx.y = threadIdx.z = 0;
   blockDim.x = blockDim.y = blockDim.z = 1;
+}
+}  // namespace
+
+namespace {
+// Zero-filled memory reserved on first touch, for arrays indexed by pixel of
+// which a sample touches only a few rows.
+template <class T>
+struct Lazy {
+  T* p = nullptr;
+  size_t bytes = 0;
+  explicit Lazy(size_t n) : bytes(n * sizeof(T)) {
+    void* m = mmap(nullptr, bytes, PROT_READ | PROT_WRITE,
+                   MAP_PRIVATE | MAP_ANONYMOUS | MAP_NORESERVE, -1, 0);
+    p = m == MAP_FAILED ? nullptr : (T*)m;
+  }
+  ~Lazy() {
+    if (p) munmap(p, bytes);
+  }
+};
+double secs_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 }  // namespace
 
@@ -240,6 +267,99 @@ void btref_map_compose(const unsigned char* stars, const unsigned char* bg,
       at(i, j);
       addStarsAndBackground((uchar4*)stars, (uchar4*)bg, (uchar4*)out, M);
     }
+}
+
+// ---- CPU baseline: the reference's map kernels on host threads ----
+
+
+// One frame of the reference's per-pixel map timed on `nthreads` host
+// threads (OpenMP over rows; 0 = all): pixInterpolation over all corners,
+// findBlackPixels + findArea + smoothAreaH/V over all pixels, then
+// distortEnvironmentMap and distortStarMap over every row_stride-th row.
+// secs: [corners, black/area/smooth, environment rows, star rows];
+// returns the rows sampled.  sat points at the summed-area table with zero
+// rows readable before and after it; grid at a map grid with absent rows
+// readable around it (as ref_map_frame pads them).
+int btref_map_time(const float* view, int M, int N, const float* grid, int GM, int GN1,
+                   int gridlvl, const float* sat, int env_rows, int env_cols,
+                   const float* stars, const int* tree, int starSize, const float* mag,
+                   int treeLevel, const float* cam7, int step, int lr, int row_stride,
+                   int nthreads, double* secs) {
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  std::vector<float2> thphi((size_t)(N + 1) * (M + 1));
+  std::vector<int> gap((size_t)(N + 1) * (M + 1));
+  auto t = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i <= N; i++) {
+    float2 border[4] = {};
+    for (int j = 0; j <= M; j++) {
+      at(i, j);
+      pixInterpolation((const float2*)view, M, N, 1, thphi.data(), (const float2*)grid, GM,
+                       GN1, 0.f, 0.f, gap.data(), gridlvl, border, 1000, 0.f);
+    }
+  }
+  secs[0] = secs_since(t);
+  std::vector<unsigned char> bh((size_t)N * M);
+  std::vector<float> area((size_t)N * M), areaS((size_t)N * M);
+  t = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      findBlackPixels(thphi.data(), M, N, bh.data());
+      findArea(thphi.data(), M, N, area.data());
+    }
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      smoothAreaH(areaS.data(), area.data(), bh.data(), gap.data(), M, N);
+    }
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      smoothAreaV(areaS.data(), area.data(), bh.data(), gap.data(), M, N);
+    }
+  secs[1] = secs_since(t);
+  std::vector<int> rows;
+  for (int i = row_stride / 2; i < N; i += row_stride) rows.push_back(i);
+  const int nr = (int)rows.size();
+  std::vector<unsigned char> out((size_t)N * M * 4);
+  int2 imsize = {env_rows, env_cols};
+  t = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int r = 0; r < nr; r++)
+    for (int j = 0; j < M; j++) {
+      at(rows[r], j);
+      distortEnvironmentMap(thphi.data(), (uchar4*)out.data(), bh.data(), imsize, M, N, 0.f,
+                            (float4*)sat, cam7, 0, nullptr, area.data(), (float2*)view,
+                            lr != 0);
+    }
+  secs[2] = secs_since(t);
+  const int filterW = 2 * step + 1;
+  const int searchNr = (int)powf(2, treeLevel / 3 * 2);
+  const int trailnum = 30;
+  Lazy<float3> scratch((size_t)N * M * filterW * filterW);
+  Lazy<int> search((size_t)N * M * searchNr + (size_t)4096 * searchNr);
+  Lazy<int2> stCache((size_t)2 * starSize * trailnum);
+  Lazy<int> stnums((size_t)starSize);
+  Lazy<float3> trail((size_t)N * M);
+  Lazy<float2> grad((size_t)(N + 1) * (M + 1));
+  if (!scratch.p || !search.p || !stCache.p || !stnums.p || !trail.p || !grad.p) return -1;
+  // frame 0: every cache entry empty (clearArrays)
+  for (size_t q = 0; q < (size_t)2 * starSize * trailnum; q++) stCache.p[q] = int2{-1, -1};
+  t = std::chrono::steady_clock::now();
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int r = 0; r < nr; r++)
+    for (int j = 0; j < M; j++) {
+      at(rows[r], j);
+      distortStarMap(scratch.p, thphi.data(), bh.data(), stars, tree, starSize, cam7, mag,
+                     treeLevel, M, N, step, 0.f, search.p, searchNr, stCache.p, stnums.p,
+                     trail.p, trailnum, grad.p, 0, (const float2*)view, lr != 0, area.data());
+    }
+  secs[3] = secs_since(t);
+  return nr;
 }
 
 // ---- trails (addTrails / makeGradField / clearArrays) ----
