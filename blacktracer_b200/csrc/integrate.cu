@@ -119,15 +119,15 @@ k_integrate_plain(const RayParams p, const double* __restrict__ th,
 }
 
 struct PlainPolicy {
-  using State = plain::RayState;
+  using State = plain::CachedState;
   static __device__ __forceinline__ bool begin(const RayParams& p, double th,
                                                double ph, State& s, double& to,
                                                double& po, int32_t& st,
                                                uint8_t& ss) {
-    return plain::begin_ray(p, th, ph, s, to, po, st, ss);
+    return plain::begin_ray_cached(p, th, ph, s, to, po, st, ss);
   }
   static __device__ __forceinline__ bool attempt(const RayParams& p, State& s) {
-    return plain::attempt(p, s);
+    return plain::attempt_cached(p, s);
   }
   static __device__ __forceinline__ void finish(const RayParams& p,
                                                 const State& s, double& to,

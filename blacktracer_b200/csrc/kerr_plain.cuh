@@ -304,6 +304,58 @@ __device__ __forceinline__ bool attempt(const RayParams& p, RayState& s) {
   return s.z <= p.z_end || s.nstp >= p.maxstp;
 }
 
+// odeint1's state plus the slope at the start of the step.  After a
+// rejected attempt the state is unchanged, and the reference's next
+// iteration recomputes derivs from the same values (BT/Metric.h:292): the
+// slope is kept instead, which gives the same results.
+struct CachedState : RayState {
+  double d[5];
+  bool dv;  // d holds the slope of y
+};
+
+__device__ __forceinline__ bool begin_ray_cached(const RayParams& p, double th, double ph,
+                                                 CachedState& s, double& tho, double& pho,
+                                                 int32_t& steps, uint8_t& status) {
+  s.dv = false;
+  return begin_ray(p, th, ph, s, tho, pho, steps, status);
+}
+
+// Step-size update of rkqs (BT/Metric.h:262-268) with one pow for both
+// outcomes, so that lanes that accept and lanes that reject do not run it
+// one after the other (the values are those of the two separate calls).
+__device__ __forceinline__ void update_step(RayState& s, double errmax) {
+  const bool ok = errmax <= 1.0;
+  const double pw = pow(errmax, ok ? kPGrow : kPShrnk);
+  if (ok) s.h = errmax > kErrCon ? kSafety * s.h * pw : kAdaptive * s.h;
+  else s.h = fmin(kSafety * s.h * pw, 0.1 * s.h);
+}
+
+template <class E = EomPlain>
+__device__ __forceinline__ bool attempt_cached(const RayParams& p, CachedState& s) {
+  double scal[5], yt[5], err[5];
+  if (!s.dv) {
+    E::f(s.y, s.d, s.b, s.q, p.a, p.asq);
+    s.dv = true;
+  }
+#pragma unroll
+  for (int i = 0; i < 5; i++) scal[i] = fabs(s.y[i]) + fabs(s.d[i] * s.h) + kTiny;
+  ck_attempt<E>(s.y, s.d, s.h, yt, err, s.b, s.q, p.a, p.asq);
+  double errmax = 0.0;
+#pragma unroll
+  for (int i = 0; i < 5; i++) errmax = fmax(errmax, fabs(err[i] / scal[i]));
+  errmax /= p.eps;
+  if (errmax <= 1.0) {
+    s.z += s.h;
+#pragma unroll
+    for (int i = 0; i < 5; i++) s.y[i] = yt[i];
+    s.dv = false;
+  }
+  update_step(s, errmax);
+  s.step = s.nstp;
+  s.nstp++;
+  return s.z <= p.z_end || s.nstp >= p.maxstp;
+}
+
 // Outputs of a finished ray.  odeint1 copies the state back only when z
 // reached the end point; otherwise the start angles come back
 // (BT/Metric.h:298-302).  Then wrapToPi (BT/Metric.h:322).
@@ -327,13 +379,13 @@ __device__ __forceinline__ void integrate_ray(const RayParams& p, double th,
                                               double ph, double& tho,
                                               double& pho, int32_t& steps,
                                               uint8_t& status) {
-  RayState s;
-  if (!begin_ray(p, th, ph, s, tho, pho, steps, status)) return;
+  CachedState s;
+  if (!begin_ray_cached(p, th, ph, s, tho, pho, steps, status)) return;
   if (p.maxstp <= 0) {
     finish_ray(p, s, tho, pho, steps, status);
     return;
   }
-  while (!attempt(p, s)) {
+  while (!attempt_cached(p, s)) {
   }
   finish_ray(p, s, tho, pho, steps, status);
 }

@@ -29,12 +29,12 @@ struct MixedPolicy {
 };
 
 struct FastPolicy {
-  using State = plain::RayState;
+  using State = fast::FastState;
   static __device__ __forceinline__ bool begin(const RayParams& p, double th,
                                                double ph, State& s, double& to,
                                                double& po, int32_t& st,
                                                uint8_t& ss) {
-    return plain::begin_ray(p, th, ph, s, to, po, st, ss);
+    return fast::begin_ray(p, th, ph, s, to, po, st, ss);
   }
   static __device__ __forceinline__ bool attempt(const RayParams& p, State& s) {
     return fast::attempt(p, s);
