@@ -354,6 +354,9 @@ def full_frame(bt, torch, n_frames):
         "pixels": cen["star_pixels"],
         "candidates_per_pixel_reference": cen["star_candidates_ref"] / max(1, cen["star_pixels"]),
         "candidates_per_pixel": cen["star_candidates"] / max(1, cen["star_pixels"]),
+        "hits_per_pixel": cen["star_hits"] / max(1, cen["star_pixels"]),
+        "heavy_share_of_candidates": cen["heavy_candidates"] / max(1, cen["star_candidates"]),
+        "heavy_share_of_hits": cen["heavy_hits"] / max(1, cen["star_hits"]),
         "census_s": time.perf_counter() - t0}
     del R, out, sp, env, g
     torch.cuda.empty_cache()
@@ -635,8 +638,12 @@ def main():
             "pixels": cen["star_pixels"],
             "candidates_per_pixel_reference": cen["star_candidates_ref"] / max(1, cen["star_pixels"]),
             "candidates_per_pixel": cen["star_candidates"] / max(1, cen["star_pixels"]),
+            "hits_per_pixel": cen["star_hits"] / max(1, cen["star_pixels"]),
+            "heavy_share_of_candidates": cen["heavy_candidates"] / max(1, cen["star_candidates"]),
+            "heavy_share_of_hits": cen["heavy_hits"] / max(1, cen["star_hits"]),
             "note": "reference: stars of the kd-tree nodes its search emits (starsToCheck); "
-                    "this build: stars of the leaves left after node-box pruning"}
+                    "this build: stars of the leaves left after node-box pruning; hits: stars "
+                    "inside the pixel's quad; heavy: pixels with more than 2048 candidates"}
         cpu_map = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             import oracle

@@ -101,7 +101,8 @@ class bt_frame(C.Structure):
 
 class bt_map_census_t(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in ("env_columns", "env_pixels", "star_pixels",
-                                          "star_candidates_ref", "star_candidates")]
+                                          "star_candidates_ref", "star_candidates",
+                                          "star_hits", "heavy_candidates", "heavy_hits")]
 
 
 class bt_trails_info(C.Structure):

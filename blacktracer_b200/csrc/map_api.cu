@@ -298,6 +298,7 @@ int bt_map_census(bt_map* m, const bt_frame* f, bt_map_census_t* out, void* stre
   BT_CUDA_TRY(cudaMallocAsync((void**)&dev, 8 * sizeof(unsigned long long), s));
   unsigned long long host[8] = {0};
   cudaError_t e = cudaMemsetAsync(dev, 0, 8 * sizeof(unsigned long long), s);
+  // out[0..1]: environment; out[2..7]: stars
   int rc = BT_OK;
   if (e == cudaSuccess && f->map) rc = map_env_census(m->S, f->env->e.rows, dev, s);
   if (e == cudaSuccess && rc == BT_OK && f->star) rc = map_star_census(m->S, F, dev + 2, s);
@@ -315,6 +316,9 @@ int bt_map_census(bt_map* m, const bt_frame* f, bt_map_census_t* out, void* stre
   out->star_pixels = host[2];
   out->star_candidates_ref = host[3];
   out->star_candidates = host[4];
+  out->star_hits = host[5];
+  out->heavy_candidates = host[6];
+  out->heavy_hits = host[7];
   return BT_OK;
 }
 

@@ -74,6 +74,17 @@ static dim3 grid2(int w, int h) {
   return dim3((unsigned)((w + TX - 1) / TX), (unsigned)((h + TY - 1) / TY));
 }
 
+// pixel_setup kept out of line where it runs once per lane ahead of a hot
+// loop: its lensing and redshift code is large, and inlined it crowds the
+// loop out of the instruction cache.
+__device__ __noinline__ bool pixel_setup_ool(const float2* thphi, const uint8_t* bh,
+                                             const float* cam, int M, int step,
+                                             const float2* view, int lr, const float* area,
+                                             int i, int j, PixelStars& P, float* mn,
+                                             float* mx) {
+  return pixel_setup(thphi, bh, cam, M, step, view, lr, area, i, j, P, mn, mx);
+}
+
 // Star tests (node tests count kNodeCost) a pixel may spend in the warp
 // path before it is handed to k_star_heavy, and the number of kd-tree
 // leaves it may list.  Pixels next to the shadow project onto quads that
@@ -123,7 +134,7 @@ k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
   if (valid) {
     PixelStars P;
     float mn[2], mx[2];
-    if (pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, i, j, P, mn, mx)) {
+    if (pixel_setup_ool(thphi, bh, cam.v, M, step, view, lr, area, i, j, P, mn, mx)) {
       P.budget = kStarBudget;
       tree_search(S, mn, mx, [&](int node) {
         walk_leaves(P, S, node, node_level(node), [&](int leaf) {
@@ -718,15 +729,17 @@ __global__ void k_makepix(const float* __restrict__ light, int M, int N,
 // Census of the star pass of the last frame, per pixel outside the shadow:
 // the stars in the kd-tree nodes the search emits (the reference tests all
 // of them, its starsToCheck) and the stars in the leaves left after the
-// node-box pruning (the candidates tested here).  Sums into out[0..2]:
-// pixels, reference candidates, candidates.
+// node-box pruning (the candidates tested here), and the stars that pass
+// the quad test (hits, each placed in the pixel and splatted).  Sums into
+// out[0..3]: pixels, reference candidates, candidates, hits; out[4..5]: the
+// candidates and hits of the pixels with more than 2048 candidates.
 __global__ void k_star_census(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
                               StarSet S, Cam7 cam, int M, int N, int step,
                               const float2* __restrict__ view, int lr,
                               const float* __restrict__ area, unsigned long long* out) {
   const int j = blockIdx.x * TX + threadIdx.x;
   const int i = blockIdx.y * TY + threadIdx.y;
-  unsigned long long px = 0, ref = 0, ours = 0;
+  unsigned long long px = 0, ref = 0, ours = 0, hits = 0, big_c = 0, big_h = 0;
   if (i < N && j < M) {
     PixelStars P;
     float mn[2], mx[2];
@@ -741,21 +754,35 @@ __global__ void k_star_census(const float2* __restrict__ thphi, const uint8_t* _
           int b0, b1;
           node_range(S, leaf, b0, b1);
           ours += (unsigned long long)(b1 - b0);
+          for (int q = b0; q < b1; q++) {
+            float st, sp;
+            if (star_test(P, S, q, st, sp)) hits++;
+          }
           return true;
         });
         return true;
       });
+      if (ours > (unsigned long long)kStarBudget) {
+        big_c = ours;
+        big_h = hits;
+      }
     }
   }
   for (int o = 16; o; o >>= 1) {
     px += __shfl_down_sync(0xffffffffu, px, o);
     ref += __shfl_down_sync(0xffffffffu, ref, o);
     ours += __shfl_down_sync(0xffffffffu, ours, o);
+    hits += __shfl_down_sync(0xffffffffu, hits, o);
+    big_c += __shfl_down_sync(0xffffffffu, big_c, o);
+    big_h += __shfl_down_sync(0xffffffffu, big_h, o);
   }
   if ((threadIdx.x & 31) == 0 && px) {
     atomicAdd(out, px);
     atomicAdd(out + 1, ref);
     atomicAdd(out + 2, ours);
+    atomicAdd(out + 3, hits);
+    atomicAdd(out + 4, big_c);
+    atomicAdd(out + 5, big_h);
   }
 }
 

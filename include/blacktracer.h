@@ -439,7 +439,8 @@ int bt_map_scratch(const bt_map* m, bt_map_buffers* b);
  * Map's pixNum, BT/MakeImageKernel.cu:650-657; two summed-area reads each)
  * and the star candidates per pixel, those of the kd-tree nodes the search
  * emits (the reference tests them all, its starsToCheck :265-275) and those
- * left after this build's node-box pruning.  Synchronises `stream`.  For
+ * left after this build's node-box pruning, and the stars that pass the quad
+ * test (each placed in the pixel and splatted).  Synchronises `stream`.  For
  * rooflines and reports; no counterpart in the reference. */
 typedef struct bt_map_census_t {
   uint64_t env_columns;          /* sum over coloured pixels of pixNum + 1     */
@@ -447,6 +448,9 @@ typedef struct bt_map_census_t {
   uint64_t star_pixels;          /* pixels outside the shadow                  */
   uint64_t star_candidates_ref;  /* sum of starsToCheck                        */
   uint64_t star_candidates;      /* sum of stars in the leaves tested here     */
+  uint64_t star_hits;            /* stars that pass the quad test (splatted)   */
+  uint64_t heavy_candidates;     /* candidates of pixels with more than 2048   */
+  uint64_t heavy_hits;           /* hits of those pixels                       */
 } bt_map_census_t;
 int bt_map_census(bt_map* m, const bt_frame* f, bt_map_census_t* out, void* stream);
 
