@@ -83,7 +83,10 @@ struct LatticeView {
 struct GridCounters {
   uint32_t n_check;   // blocks to examine at the current level
   uint32_t n_next;    // blocks for the next level
-  uint32_t n_trace;   // vertices to trace
+  uint32_t n_trace;   // vertices to trace: n_hot from the front of the
+                      // trace list, the rest from its back
+  uint32_t n_hot;     // vertices whose parent block holds a slow ray
+  uint32_t n_cold;
   uint32_t fetch;     // work-queue head of the trace kernel
   uint32_t n_amb;     // mixed form: blocks whose decision waits for FP64
   uint32_t n_retrace; // mixed form: corners re-traced in FP64

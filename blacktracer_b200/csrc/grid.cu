@@ -169,6 +169,8 @@ __global__ void k_seed(const GridDesc* __restrict__ D, SeedShape S) {
       L.vflag[((uint32_t)L.N - 1) * M] = 2;
     }
     ctr->n_trace = S.npole + total;
+    ctr->n_hot = S.npole + total;
+    ctr->n_cold = 0;
     ctr->n_check = S.cols + (uniform ? 0 : S.brows * S.cols);
     ctr->n_next = 0;
     ctr->fetch = 0;
@@ -225,9 +227,16 @@ __global__ void k_queue(const GridDesc* __restrict__ D, int G, uint32_t* qoff,
 }
 
 // ------------------------------------------------------------ refinement
+// A new vertex goes to the front of the trace list when its parent block
+// has a corner whose ray took at least kHotSteps attempts (its own ray is
+// then likely slow too), else to the back: the trace kernel takes the front
+// first, so the longest rays of a level start first instead of whenever a
+// lane happens to reach them.  The order changes no result.
+constexpr int32_t kHotSteps = 100;
+
 __device__ __forceinline__ void claim_vertex(const LatticeView& L, uint32_t i,
                                              uint32_t j, uint32_t* trace,
-                                             GridCounters* ctr) {
+                                             GridCounters* ctr, bool hot) {
   const uint32_t key = i * (uint32_t)L.M + j;
   // 32-bit CAS on the aligned word that holds the byte
   uint32_t* word = (uint32_t*)((uintptr_t)(L.vflag + key) & ~(uintptr_t)3);
@@ -240,8 +249,13 @@ __device__ __forceinline__ void claim_vertex(const LatticeView& L, uint32_t i,
     if (got == old) break;
     old = got;
   }
-  const uint32_t slot = atomicAdd(&ctr->n_trace, 1u);
-  trace[slot] = key;
+  atomicAdd(&ctr->n_trace, 1u);
+  if (hot) {
+    trace[atomicAdd(&ctr->n_hot, 1u)] = key;
+  } else {
+    const uint32_t cap = (uint32_t)L.N * (uint32_t)L.M;
+    trace[cap - 1u - atomicAdd(&ctr->n_cold, 1u)] = key;
+  }
 }
 
 // One level of adaptiveBlockIntegration (BT/Grid.h:476-497) with
@@ -277,11 +291,14 @@ __global__ void k_refine(const GridDesc* __restrict__ D, int level, int cur) {
       continue;
     }
     const uint32_t kh = i + gap / 2, lh = j + gap / 2;
-    claim_vertex(L, kh, j, trace, ctr);
-    claim_vertex(L, kh, lh, trace, ctr);
-    claim_vertex(L, i, lh, trace, ctr);
-    claim_vertex(L, i + gap, lh, trace, ctr);
-    claim_vertex(L, kh, (j + gap) % M, trace, ctr);
+    const int32_t smax = max(max(L.steps[(size_t)i * M + j], L.steps[(size_t)k * M + j]),
+                             max(L.steps[(size_t)i * M + l], L.steps[(size_t)k * M + l]));
+    const bool hot = smax >= kHotSteps;
+    claim_vertex(L, kh, j, trace, ctr, hot);
+    claim_vertex(L, kh, lh, trace, ctr, hot);
+    claim_vertex(L, i, lh, trace, ctr, hot);
+    claim_vertex(L, i + gap, lh, trace, ctr, hot);
+    claim_vertex(L, kh, (j + gap) % M, trace, ctr, hot);
     const uint32_t s = atomicAdd(&ctr->n_next, 4u);
     next[s + 0] = key;
     next[s + 1] = kh * M + j;
@@ -301,6 +318,8 @@ __global__ void k_advance(const GridDesc* __restrict__ D, int G, int after_seed,
   ctr->traced_lo = (uint32_t)t;
   ctr->traced_hi = (uint32_t)(t >> 32);
   ctr->n_trace = 0;
+  ctr->n_hot = 0;
+  ctr->n_cold = 0;
   ctr->fetch = 0;
   if (!after_seed) {
     ctr->n_check = ctr->n_next;

@@ -65,7 +65,11 @@ k_trace_lattice(const GridDesc* __restrict__ D, int G,
         if (k < n) {
           g = queue_grid(qoff, G, k);
           const GridDesc& d = D[g];
-          key = d.trace[k - qoff[g]];
+          // the front segment (n_hot entries), then the back one
+          const uint32_t r = k - qoff[g];
+          const uint32_t nh = *(volatile const uint32_t*)&d.ctr->n_hot;
+          key = r < nh ? d.trace[r]
+                       : d.trace[(uint32_t)d.L.N * (uint32_t)d.L.M - 1u - (r - nh)];
           double th, ph, to, po;
           int32_t s;
           uint8_t ss;
