@@ -253,7 +253,8 @@ def serve_rates(bt, torch, env, sp, n):
             nonlocal done
             for c in S.poll(wait_ms=wait_ms):
                 assert c["status"] == 0, c
-                lat[c["id"]] = (c["t_done"] - c["t_submit"], c["grid_reused"])
+                lat[c["id"]] = (c["t_done"] - c["t_submit"], c["grid_reused"],
+                                c["t_admit"] - c["t_submit"])
                 pools[used.pop(c["id"])[0]].append(used_buf.pop(c["id"]))
                 done += 1
 
@@ -277,10 +278,21 @@ def serve_rates(bt, torch, env, sp, n):
         st = S.stats()
         S.close()
         L = np.array([lat[k][0] for k in range(n)]) * 1e3
+        Wt = np.array([lat[k][2] for k in range(n)]) * 1e3
+        reused = np.array([lat[k][1] for k in range(n)], bool)
+        by_size = {}
+        for (W, H) in SERVE["sizes"]:
+            sel = np.array([sizes[k] == (W, H) for k in range(n)])
+            if sel.any():
+                by_size[f"{W}x{H}"] = {"p50_ms": float(np.percentile(L[sel], 50)),
+                                       "p99_ms": float(np.percentile(L[sel], 99))}
         out["rates"].append({
             "rate_rps": rate, "requests": n, "throughput_rps": n / wall,
             "p50_ms": float(np.percentile(L, 50)), "p99_ms": float(np.percentile(L, 99)),
-            "mean_ms": float(L.mean()),
+            "mean_ms": float(L.mean()), "by_size": by_size,
+            "admission_wait_p99_ms": float(np.percentile(Wt, 99)),
+            "p99_ms_grid_reused": float(np.percentile(L[reused], 99)) if reused.any() else None,
+            "p99_ms_grid_built": float(np.percentile(L[~reused], 99)) if (~reused).any() else None,
             "grid_hits": st["grid_hits"] - st0["grid_hits"],
             "grid_misses": st["grid_misses"] - st0["grid_misses"],
             "grid_sets_built": st["build_sets"] - st0["build_sets"],

@@ -130,6 +130,9 @@ int launch_trace_mixed(const GridDesc* D, int G, const uint32_t* qoff,
 int launch_trace_fast(const GridDesc* D, int G, const uint32_t* qoff,
                       uint32_t* qfetch, TraceShape shape, cudaStream_t s);
 
+// Map grid of a built grid into a caller's buffer (grid.cu).
+int grid_map_export_into(const bt_grid* g, float* dst, cudaStream_t s);
+
 }  // namespace bt
 
 #define BT_CUDA_TRY(expr)                                                   \

@@ -1127,6 +1127,20 @@ int batch_set_timing(bt_batch* b, int on) {
 
 }  // namespace
 
+namespace bt {
+// The map grid of a built grid written into a caller's device buffer of
+// map_rows x M float2 (as bt_grid_map_export returns it), without the
+// grid's own export buffer.
+int grid_map_export_into(const bt_grid* g, float* dst, cudaStream_t s) {
+  const int GN = g->L.N, GM = g->L.M;
+  const int symv = (float)GM / (float)GN > 3 ? 1 : 0;  // dev_sym, BT/MakeImageKernel.cu:1259-1260
+  const int GN1 = symv ? 2 * GN - 1 : GN;
+  k_export_map<<<grid_blocks((size_t)GN * GM, 256), 256, 0, s>>>(g->L, (float2*)dst, GN1, symv);
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+}  // namespace bt
+
 extern "C" {
 
 int bt_grid_dims(int maxlevel, int angle, int32_t* N, int32_t* M) {
@@ -1272,6 +1286,7 @@ int bt_grid_export(bt_grid* g, bt_grid_export_t* out, void* stream) {
       BT_CUDA_TRY(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDefault, s));
   return BT_OK;
 }
+
 
 int bt_grid_map_export(bt_grid* g, const float** grid_out, int32_t* rows,
                        int32_t* cols, int32_t* sym, void* stream) {

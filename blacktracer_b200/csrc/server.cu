@@ -119,7 +119,13 @@ struct bt_server {
   size_t slot_bytes_used = 0;
   std::map<std::pair<int, int>, float*> views;
   bt_batch* set = nullptr;
+  // Stream priorities: grid builds first (a build is a chain of short
+  // latency-bound launches that frames of other requests wait for), then
+  // frames by size, smaller first (slot_priority).
   cudaStream_t build_stream = nullptr;
+  int prio_least = 0, prio_greatest = 0;
+  char* arena = nullptr;                // the grid cache's memory
+  std::vector<float2*> free_grids;      // unused grid slices of the arena
   cudaEvent_t build_done = nullptr;
   bool building = false;
   std::vector<Entry*> to_build;
@@ -144,8 +150,14 @@ void complete(bt_server* S, const Request& q, int status, int reused) {
   S->done_cv.notify_all();
 }
 
-void entry_free(Entry* e) {
-  if (e->grid) cudaFree(e->grid);
+// Grid buffers are slices of one arena of the whole grid-cache budget,
+// reserved when the server is created: growing device memory while frames
+// run (cudaMalloc, or a stream-ordered pool that has to map more memory)
+// blocked the worker thread for up to hundreds of milliseconds.
+void entry_free(bt_server* S, Entry* e);
+
+void entry_free(bt_server* S, Entry* e) {
+  if (e->grid) S->free_grids.push_back(e->grid);
   if (e->ready) cudaEventDestroy(e->ready);
   delete e;
 }
@@ -164,7 +176,7 @@ bool grid_room(bt_server* S, size_t bytes) {
     S->lru.erase(victim->lru);
     S->cache.erase(victim->key);
     S->grid_bytes_used -= S->grid_bytes;
-    entry_free(victim);
+    entry_free(S, victim);
     std::lock_guard<std::mutex> lk(S->mu);
     S->stats.evictions++;
   }
@@ -184,6 +196,15 @@ float* view_for(bt_server* S, int W, int H) {
   cudaStreamSynchronize(S->build_stream);
   S->views[{W, H}] = v;
   return v;
+}
+
+// Priority of the stream of a W x H frame: one level below builds for
+// frames up to 1 MP, two up to 4 MP, the least above (clamped to the
+// device's range; numerically lower is higher priority).
+int slot_priority(const bt_server* S, int W, int H) {
+  const double mp = (double)W * H / 1e6;
+  const int p = S->prio_greatest + (mp <= 1.0 ? 1 : mp <= 4.0 ? 2 : 3);
+  return std::min(std::max(p, S->prio_greatest), S->prio_least);
 }
 
 // An idle slot for W x H: reuse one of that size, else create one within
@@ -212,7 +233,8 @@ Slot* slot_for(bt_server* S, int W, int H) {
   s.bytes = need;
   if (bt_map_create(W, H, &s.map) != BT_OK) return nullptr;
   if (cudaMalloc((void**)&s.dev_out, (size_t)W * H * 4) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&s.stream, cudaStreamNonBlocking,
+                                   slot_priority(S, W, H)) != cudaSuccess ||
       cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess) {
     bt_map_destroy(s.map);
     if (s.dev_out) cudaFree(s.dev_out);
@@ -267,13 +289,9 @@ int launch_builds(bt_server* S) {
     return rc;
   for (int k = 0; k < n; k++) {
     Entry* e = S->to_build[k];
-    const float* g = nullptr;
-    int32_t rows, cols, sym;
-    if (int rc = bt_grid_map_export(bt_batch_grid(S->set, k), &g, &rows, &cols, &sym,
-                                    S->build_stream))
+    if (int rc = bt::grid_map_export_into(bt_batch_grid(S->set, k), (float*)e->grid,
+                                          S->build_stream))
       return rc;
-    BT_CUDA_TRY(cudaMemcpyAsync(e->grid, g, S->grid_bytes, cudaMemcpyDeviceToDevice,
-                                S->build_stream));
     BT_CUDA_TRY(cudaEventRecord(e->ready, S->build_stream));
     e->state = 1;
   }
@@ -303,9 +321,13 @@ void admit(bt_server* S) {
     if (!e) {
       reused = 0;
       e = new (std::nothrow) Entry;
-      if (!e || cudaMalloc((void**)&e->grid, S->grid_bytes) != cudaSuccess ||
+      if (e && !S->free_grids.empty()) {
+        e->grid = S->free_grids.back();
+        S->free_grids.pop_back();
+      }
+      if (!e || !e->grid ||
           cudaEventCreateWithFlags(&e->ready, cudaEventDisableTiming) != cudaSuccess) {
-        if (e) entry_free(e);
+        if (e) entry_free(S, e);
         Request fail = q;
         S->pending.pop_front();
         complete(S, fail, BT_ERR_NOMEM, 0);
@@ -429,13 +451,26 @@ int bt_server_create(const bt_server_config* cfg, bt_server** out) {
   S->grid_bytes = (size_t)S->grid_rows * S->grid_cols * sizeof(float2);
   BT_ARG_CHECK(S->grid_bytes <= cfg->grid_cache_bytes, "grid cache smaller than one grid");
   int rc = bt_batch_create(cfg->maxlevel, cfg->angle, cfg->max_build_batch, &S->set);
-  if (rc == BT_OK && (cudaStreamCreateWithFlags(&S->build_stream, cudaStreamNonBlocking) !=
-                          cudaSuccess ||
+  cudaDeviceGetStreamPriorityRange(&S->prio_least, &S->prio_greatest);
+  if (rc == BT_OK) {
+    const size_t n = cfg->grid_cache_bytes / S->grid_bytes;
+    if (cudaMalloc((void**)&S->arena, n * S->grid_bytes) != cudaSuccess) {
+      set_error("grid cache of %zu bytes could not be reserved", n * S->grid_bytes);
+      rc = BT_ERR_NOMEM;
+    } else {
+      S->free_grids.reserve(n);
+      for (size_t k = n; k-- > 0;)
+        S->free_grids.push_back((float2*)(S->arena + k * S->grid_bytes));
+    }
+  }
+  if (rc == BT_OK && (cudaStreamCreateWithPriority(&S->build_stream, cudaStreamNonBlocking,
+                                                   S->prio_greatest) != cudaSuccess ||
                       cudaEventCreateWithFlags(&S->build_done, cudaEventDisableTiming) !=
                           cudaSuccess))
     rc = BT_ERR_CUDA;
   if (rc) {
     if (S->set) bt_batch_destroy(S->set);
+    if (S->arena) cudaFree(S->arena);
     delete S;
     return rc;
   }
@@ -507,7 +542,8 @@ void bt_server_destroy(bt_server* S) {
     cudaStreamDestroy(s.stream);
     cudaEventDestroy(s.done);
   }
-  for (auto& kv : S->cache) entry_free(kv.second);
+  for (auto& kv : S->cache) entry_free(S, kv.second);
+  if (S->arena) cudaFree(S->arena);
   for (auto& kv : S->views) cudaFree(kv.second);
   bt_batch_destroy(S->set);
   cudaEventDestroy(S->build_done);

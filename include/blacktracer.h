@@ -563,14 +563,19 @@ int bt_view_camera(float* view, int width, int height, double view_angle,
  * grids resident in a cache keyed by the exact camera and spin and reused,
  * the grids missing at an admission round built together as one grid set,
  * frames of different requests on their own streams, overlapping each other
- * and the next grid build.  No counterpart in the reference (a single-scene
- * host program, BT/BlackTracer.cpp). */
+ * and the next grid build.  Grid builds run on the highest-priority stream
+ * and frames on lower ones, smaller frames first; the grid cache's memory is
+ * reserved once, so that serving allocates no device memory for new poses.
+ * No counterpart in the reference (a single-scene host program,
+ * BT/BlackTracer.cpp). */
 typedef struct bt_server bt_server;
 
 typedef struct bt_server_config {
   int32_t maxlevel, startlevel, angle;  /* grids built for requests         */
   int32_t precision;                    /* BT_PRECISION_* of grid builds    */
-  size_t grid_cache_bytes;              /* HBM budget of resident grids     */
+  size_t grid_cache_bytes;              /* HBM budget of resident grids,
+                                           reserved when the server is
+                                           created                          */
   size_t render_bytes;                  /* HBM budget of render slots       */
   int32_t max_inflight;                 /* frames admitted at once          */
   int32_t max_build_batch;              /* grids built together (set size)  */
