@@ -572,20 +572,20 @@ __global__ void k_tfix_pass(const GridDesc* __restrict__ D, int level, int pass,
   const uint32_t M = L.M;
   const uint32_t g = pow2u(L.maxlevel - A.level);
   bool changed = false;
-  for (uint32_t t = lo + blockIdx.x * blockDim.x + threadIdx.x; t < hi;
-       t += gridDim.x * blockDim.x) {
-    const uint32_t key = A.leaves[t];
+  // one thread per (leaf, edge): an edge's T-vertices belong to it alone
+  const uint64_t n4 = 4ull * (hi - lo);
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n4;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t key = A.leaves[lo + (uint32_t)(u >> 2)];
+    const int e = (int)(u & 3u);
     const uint32_t i = key / M, j = key % M;
     if (L.thphi[key].y < 0) continue;  // BT/Grid.h:107
     const uint32_t k = i + g, l = (j + g) % M;
-    Edge e0 = {i, j, 1, g, rank_of(i, j, 0)};
-    Edge e1 = {i, j, 0, g, rank_of(i, j, 1)};
-    Edge e2 = {i, l, 1, g, rank_of(i, j, 2)};
-    Edge e3 = {k, j, 0, g, rank_of(i, j, 3)};
-    changed |= fix_edge(A, e0);
-    changed |= fix_edge(A, e1);
-    changed |= fix_edge(A, e2);
-    changed |= fix_edge(A, e3);
+    const Edge E = e == 0   ? Edge{i, j, 1, g, rank_of(i, j, 0)}
+                   : e == 1 ? Edge{i, j, 0, g, rank_of(i, j, 1)}
+                   : e == 2 ? Edge{i, l, 1, g, rank_of(i, j, 2)}
+                            : Edge{k, j, 0, g, rank_of(i, j, 3)};
+    changed |= fix_edge(A, E);
   }
   if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0)
     atomicOr(&ctr->tfix_flags[A.pass], 1u);
@@ -603,20 +603,21 @@ __global__ void k_tfix_commit(const GridDesc* __restrict__ D, int level, int lo_
   const double2* X = d.X[0];
   const uint32_t M = L.M;
   const uint32_t g = pow2u(L.maxlevel - level);
-  for (uint32_t t = lo + blockIdx.x * blockDim.x + threadIdx.x; t < hi;
-       t += gridDim.x * blockDim.x) {
-    const uint32_t key = d.leaves[t];
+  const uint64_t n4 = 4ull * (hi - lo);
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n4;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t key = d.leaves[lo + (uint32_t)(u >> 2)];
+    const int e = (int)(u & 3u);
     const uint32_t i = key / M, j = key % M;
     if (L.thphi[key].y < 0) continue;
     const uint32_t k = i + g, l = (j + g) % M;
-    const uint32_t si[4] = {i, i, i, k}, sj[4] = {j, j, l, j};
-    const int ud[4] = {1, 0, 1, 0};
-    for (int e = 0; e < 4; e++)
-      for (uint32_t o = 1; o < g; o++) {
-        const uint32_t ip = si[e] + ud[e] * o, jp = sj[e] + (1 - ud[e]) * o;
-        const size_t id = (size_t)ip * M + jp;
-        if (L.vflag[id] == 1) L.thphi[id] = X[id];
-      }
+    const uint32_t si = e == 3 ? k : i, sj = e == 2 ? l : j;
+    const int ud = (e == 0 || e == 2) ? 1 : 0;
+    for (uint32_t o = 1; o < g; o++) {
+      const uint32_t ip = si + ud * o, jp = sj + (1 - ud) * o;
+      const size_t id = (size_t)ip * M + jp;
+      if (L.vflag[id] == 1) L.thphi[id] = X[id];
+    }
   }
 }
 
