@@ -13,8 +13,9 @@
 //   f4 = (cos sin (b^2/sin^2 - a^2) + b^2 cos^3/sin^3) / rho^2
 //        - a^2 cos sin (p_th^2 + p_r^2 Delta) / rho^4 + a^2 cos sin W / (rho^4 Delta)
 // with W = Theta Delta + R.  Within a step, sin and cos of each stage's theta
-// come from those at the start of the step by angle addition (rotate), and
-// the slope at the start of a step is kept across a rejected attempt.
+// come from those at the start of the step by angle addition (rotate), the
+// slope at the start of a step is kept across a rejected attempt, and the
+// step-size factor is computed in FP32.
 // Results agree with the plain form to rounding level (they are not
 // bit-identical).
 #pragma once
@@ -174,7 +175,14 @@ __device__ __forceinline__ bool attempt(const RayParams& p, FastState& s) {
     for (int i = 0; i < 5; i++) s.y[i] = yt[i];
     s.dv = false;
   }
-  update_step(s, errmax);
+  // rkqs's step-size update (BT/Metric.h:262-268) with the growth / shrink
+  // factor errmax^-0.2 / errmax^-0.25 in FP32: the factor only steers the
+  // next step (its error is that of the step-size heuristic, ~1e-7
+  // relative), and an FP64 pow is the longest dependent chain of an attempt
+  const bool ok = errmax <= 1.0;
+  const double pw = (double)powf((float)errmax, ok ? -0.2f : -0.25f);
+  if (ok) s.h = errmax > kErrCon ? kSafety * s.h * pw : kAdaptive * s.h;
+  else s.h = fmin(kSafety * s.h * pw, 0.1 * s.h);
   s.step = s.nstp;
   s.nstp++;
   return s.z <= p.z_end || s.nstp >= p.maxstp;
