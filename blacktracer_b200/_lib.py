@@ -217,6 +217,7 @@ _SIGS = {
     "bt_trails_reset": (C.c_int, [_vp]),
     "bt_trails_query": (C.c_int, [_vp, C.POINTER(bt_trails_info), _vp]),
     "bt_map_census": (C.c_int, [_vp, C.POINTER(bt_frame), C.POINTER(bt_map_census_t), _vp]),
+    "bt_probe_fast_rcp": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),
     "bt_last_error": (C.c_char_p, []),
     "bt_version": (C.c_char_p, []),
 }

@@ -2,6 +2,8 @@
 // (kerr_fast.cuh) integrators.  Compiled with FMA contraction on: these forms
 // are not bit-matched to the reference; their error against the FP64 oracle
 // is measured instead.
+#include <algorithm>
+
 #include "bt_internal.h"
 #include "kerr_fast.cuh"
 #include "kerr_mixed.cuh"
@@ -123,3 +125,23 @@ int launch_trace_fast(const GridDesc* D, int G, const uint32_t* qoff,
 }
 
 }  // namespace bt
+
+namespace bt {
+namespace {
+__global__ void k_probe_rcp(const double* __restrict__ x, double* __restrict__ out, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x)
+    out[k] = fast::rcp_nr(x[k]);
+}
+}  // namespace
+}  // namespace bt
+
+extern "C" int bt_probe_fast_rcp(const double* x, double* out, size_t n, void* stream) {
+  bt::clear_error();
+  BT_ARG_CHECK(x && out, "NULL pointer");
+  if (n == 0) return BT_OK;
+  bt::k_probe_rcp<<<(unsigned)std::min<size_t>((n + 255) / 256, 4096), 256, 0,
+                    (cudaStream_t)stream>>>(x, out, n);
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}

@@ -50,9 +50,10 @@ enum {
                              turning points, for capture and for phi       */
   BT_PRECISION_FAST = 2   /* FP64, the same method with the equations of
                              motion reassociated (3 reciprocals instead of
-                             16 divisions), stage sin/cos by angle addition,
-                             the step-size factor in FP32, FMA: same grid
-                             topology as PLAIN, p99 ~1e-10 rad from it      */
+                             16 divisions, by Newton-refined approximate
+                             reciprocals), stage sin/cos by angle addition,
+                             error ratio and step-size factor in FP32, FMA:
+                             same grid topology as PLAIN, p99 ~1e-10 rad    */
 };
 
 /* Field-for-field the reference Camera (BT/Camera.h:8-11). */
@@ -626,6 +627,11 @@ void bt_server_destroy(bt_server* s);
  * from an independent-chain DFMA kernel timed with CUDA events: the peak
  * the FP64 integrator's roofline is reported against. */
 int bt_probe_fp64_tflops(double* tflops, void* stream);
+
+/* The fast form's reciprocal (approximate reciprocal refined by two
+ * Newton-Raphson steps) on n DEVICE values: for tests that check it against
+ * 1/x.  No counterpart in the reference. */
+int bt_probe_fast_rcp(const double* x, double* out, size_t n, void* stream);
 
 /* Message for the last error on this thread ("" when none). */
 const char* bt_last_error(void);

@@ -109,3 +109,22 @@ def test_empty_and_single_ray(bt, cuda):
     assert out[0].size == 0
     out = run_gpu(bt, cuda, cam.as_array(), 0.6, np.array([1.0]), np.array([2.0]), "plain")
     assert out[0].size == 1 and out[3][0] in (0, 1)
+
+
+def test_fast_reciprocal_within_two_ulp(bt, cuda):
+    """The fast form's reciprocal (approximate reciprocal + two Newton-Raphson
+    steps) against the correctly rounded 1/x, over the magnitudes the
+    equations of motion divide by (rho^2, Delta, sin theta), both signs."""
+    import ctypes as C
+    rng = np.random.default_rng(17)
+    mag = 10.0 ** rng.uniform(-12, 12, 200000)
+    x = mag * rng.choice([-1.0, 1.0], mag.size)
+    xd = cuda.tensor(x, dtype=cuda.float64, device="cuda")
+    out = cuda.empty_like(xd)
+    bt._lib.check(bt.lib().bt_probe_fast_rcp(C.c_void_p(xd.data_ptr()),
+                                             C.c_void_p(out.data_ptr()), x.size, None))
+    got = out.cpu().numpy()
+    ref = 1.0 / x
+    ulp = np.abs(got - ref) / np.spacing(np.abs(ref))
+    print(f"fast reciprocal: max {ulp.max():.2f} ulp, exact {(ulp == 0).mean():.4f}")
+    assert ulp.max() <= 2
