@@ -51,6 +51,20 @@ F_ATTEMPT_FORM = {"plain": F_ATTEMPT, "mixed": F_ATTEMPT,
 WORKLOAD = dict(maxlevel=11, startlevel=6, a=0.999, r=5.0, theta=np.pi / 2)
 
 
+def replica_rate(units_local, secs_local, dist=None, device="cpu"):
+    """Whole-job rate of replicas (one process per GPU, no data exchange):
+    the units all ranks processed over the slowest rank's time.  Returns
+    (rate, slowest seconds).  With dist None or one rank, the local rate."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return units_local / secs_local, secs_local
+    import torch
+    t = torch.tensor([secs_local], dtype=torch.float64, device=device)
+    u = torch.tensor([float(units_local)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(u.item()) / float(t.item()), float(t.item())
+
+
 def hbm_peak():
     """Measured copy bandwidth of this pool's B200s (GB/s), else the fallback."""
     try:
@@ -465,12 +479,159 @@ def main():
         if world > 1:
             dist.barrier()
 
-    def allmax(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    stream = torch.cuda.current_stream()
+    cam = bt.Camera(FULL["theta"], 0.0, FULL["r"], 0.0, a=FULL["a"])
+    g = bt.Grid(FULL["maxlevel"], FULL["startlevel"], True, cam, opts="fast")
+    for _ in range(2):
+        g.build()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ev[0].record(stream)
+    g.build()
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    build_ms = ev[0].elapsed_time(ev[1])
+    rays = g.traced
+    t0 = time.perf_counter()
+    rows, cols = FULL["env"]
+    bgr = value_noise_env(torch, rows, cols, seed=FULL["seed"])
+    env = bt.Environment(bgr)
+    del bgr
+    th, ph, mag, bv = synthetic_stars(FULL["stars"], seed=FULL["seed"] + 1)
+    sp = bt.StarProcessor(th, ph, mag, bv, treeLevel=FULL["tree_level"],
+                          psf=bt.psf_airy(FULL["psf"], 4.0))
+    del th, ph, mag, bv
+    setup_s = time.perf_counter() - t0
+    W, H = FULL["W"], FULL["H"]
+    viewer = bt.Viewer(np.pi / 2, 0.0, 0.0, W, H, True)
+    R = bt.Renderer(W, H)
+    out = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+    kw = dict(env=env, stars=sp, lr=True, diffraction=True, psf_scale=True, bb_table=1, out=out)
+    for _ in range(2):
+        R.render(g, viewer, cam, **kw)
+    torch.cuda.synchronize()
+    lat = []
+    for _ in range(n_frames):
+        ev[0].record(stream)
+        R.render(g, viewer, cam, **kw)
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+        lat.append(ev[0].elapsed_time(ev[1]))
+    lat = np.array(lat)
+    res = {"workload": "Kerr a=0.99, static camera r=8M theta=1.2; grid L6->L12 fast FP64; "
+                       "7680x3840 from 16384x8192 value-noise env; 1e7 stars (tree level 18), "
+                       "33x33 Airy PSF scaled by sqrt(magnification), 1024-entry FP32 "
+                       "blackbody table",
+           "grid_build_ms": build_ms, "grid_rays": rays,
+           "grid_geodesics_per_s": rays / (build_ms / 1e3),
+           "frame_p50_ms": float(np.percentile(lat, 50)),
+           "frame_p99_ms": float(np.percentile(lat, 99)), "frames": n_frames,
+           "frame_plus_grid_ms": float(np.percentile(lat, 50)) + build_ms,
+           "setup_s": setup_s}
+    t0 = time.perf_counter()
+    cen = R.census()
+    res["star_census"] = {
+        "pixels": cen["star_pixels"],
+        "candidates_per_pixel_reference": cen["star_candidates_ref"] / max(1, cen["star_pixels"]),
+        "candidates_per_pixel": cen["star_candidates"] / max(1, cen["star_pixels"]),
+        "hits_per_pixel": cen["star_hits"] / max(1, cen["star_pixels"]),
+        "heavy_share_of_candidates": cen["heavy_candidates"] / max(1, cen["star_candidates"]),
+        "heavy_share_of_hits": cen["heavy_hits"] / max(1, cen["star_hits"]),
+        "census_s": time.perf_counter() - t0}
+    del R, out, sp, env, g
+    torch.cuda.empty_cache()
+    return res
+
+
+def cpu_reference_arm(args):
+    """--impl reference: the reference's own CPU integrator
+    (Grid::integration_wrapper, compiled in place into oracle/_ref) on all
+    host cores, over the rays the workload's grid traces."""
+    import oracle
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    if not oracle.have_ref():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libbtref.so was not built (the reference tree was "
+                          "absent when the library was built)"}))
+        return 0
+    cam = oracle.camera_orbit(WORKLOAD["a"], WORKLOAD["theta"], 0.0, WORKLOAD["r"], 0, 0, 1)
+    g = oracle.grid_build(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam,
+                          WORKLOAD["a"], tfix=0)
+    # the ray set of the grid: every traced vertex (pole copies are not traced)
+    ii, jj = np.nonzero(g["exists"])
+    keep = ~(((ii == 0) | (ii == g["N"] - 1)) & (jj != 0))
+    ii, jj = ii[keep], jj[keep]
+    th = ii / (g["N"] - 1) * np.pi
+    ph = jj / g["M"] * 2 * np.pi
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        oracle.integrate_rays(cam, WORKLOAD["a"], th[:2000], ph[:2000], ref=True, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.integrate_rays(cam, WORKLOAD["a"], th, ph, ref=True, nthreads=cores)
+    el = time.perf_counter() - t0
+    v = len(th) * args.steps / el
+    line = {
+        "metric": METRIC, "value": v, "unit": "geodesics/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "adaptive grid L6->L11, a=0.999, r=5M equatorial Keplerian "
+                               "camera: the grid's traced rays", "rays": int(len(th)),
+                   "parallelism": f"{cores} host threads"},
+        "cpu_baseline": {"value": v, "unit": "geodesics/s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{len(th)} rays of the workload's grid per step "
+                                   "through Grid::integration_wrapper, split over host threads"},
+        "e2e": {"value": v, "unit": "geodesics/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--frames", type=int, default=20, help="4K frames to time (0 = skip)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fast", choices=["fast", "plain", "mixed"],
+                    help="integrator form of the headline value")
+    ap.add_argument("--no-batch", dest="batch", action="store_false",
+                    help="skip the 64-pose batched-grid measurement")
+    ap.add_argument("--no-c5", dest="c5", action="store_false",
+                    help="skip the full-frame measurement (L12, 8K, 10^7 stars, diffraction)")
+    ap.add_argument("--frames-c5", type=int, default=5, help="timed full 8K frames")
+    ap.add_argument("--serve-requests", type=int, default=300,
+                    help="requests per arrival rate of the serving measurement (0 = skip; "
+                         "the serving configuration has 2000)")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        return cpu_reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    import blacktracer_b200 as bt
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
 
     stream = torch.cuda.current_stream()
     cam = c2_camera(bt)
@@ -514,8 +675,9 @@ def main():
     torch.cuda.synchronize()
     barrier()
     clk = clocks.stop()
-    max_ms = allmax(total_ms)
-    value = traced * args.steps * world / (max_ms / 1e3)
+    value, max_s = replica_rate(traced * args.steps, total_ms / 1e3,
+                                dist if world > 1 else None, "cuda")
+    max_ms = max_s * 1e3
 
     # the other two forms, same workload (reported beside the headline), with
     # their error against the plain form
@@ -574,8 +736,8 @@ def main():
         grid.export(out=bufs)
     torch.cuda.synchronize()
     barrier()
-    e2e_s = allmax(time.perf_counter() - t0)
-    e2e_value = traced * args.steps * world / e2e_s
+    e2e_value, e2e_s = replica_rate(traced * args.steps, time.perf_counter() - t0,
+                                    dist if world > 1 else None, "cuda")
 
     # roofline of the dominant kernel (the ray-tracing launches)
     import ctypes as C
