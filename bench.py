@@ -6,8 +6,9 @@ Headline (value): geodesics/s of building the adaptive camera-sky grid of the
 circular equatorial orbit at r = 5M boosted at Keplerian velocity, adaptive
 refinement from level 6 (64x128) to level 11 (2048x4096 equivalent) --
 through the C ABI (bt_grid_build), in the fast FP64 form by default (the
-reference's method with its equations of motion reassociated: same grid
-topology, p99 ~1e-13 rad against the plain form); the plain form (the
+reference's method with its equations of motion reassociated, Newton-refined
+reciprocals and FP32 step control: same grid topology, p99 ~1e-10 rad against
+the plain form); the plain form (the
 reference's operation order) and the FP32-bulk mixed form are reported beside
 it, each with its error against plain.  One step = one complete grid build
 (all levels + T-vertex fix).  Also reported: 4K frames (3840x1920 BGRA8 from
@@ -24,6 +25,7 @@ integrator on the box's host cores on the same ray set.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import subprocess
@@ -258,6 +260,11 @@ def serve_rates(bt, torch, env, sp, n):
             got = 0
             while got < 16:
                 got += len(S.poll(wait_ms=50))
+        # objects of earlier measurements that sit in reference cycles are
+        # freed here rather than by a collection inside the timed schedule,
+        # where a cudaFree of gigabytes would hold up the server's launches
+        gc.collect()
+        torch.cuda.synchronize()
         st0 = S.stats()
         used = {}
         lat, done = {}, 0
@@ -958,8 +965,9 @@ def main():
                                    "Kerr a=0.999, camera r=5M theta=pi/2 Keplerian orbit; "
                                    f"{prec_main} integrator",
                        "integrator": {"fast": "FP64, reference method with reassociated "
-                                              "equations of motion and FMA (error vs plain "
-                                              "under 'plain')",
+                                              "equations of motion, Newton-refined "
+                                              "reciprocals, FP32 error ratio and step "
+                                              "factor, FMA (error vs plain under 'plain')",
                                       "plain": "FP64, reference operation order, no FMA",
                                       "mixed": "FP32 bulk, FP64 guards"}[prec_main],
                        "rays_per_build": traced, "l2": "flushed (256 MB write) before every step",
