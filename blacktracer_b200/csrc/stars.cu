@@ -109,11 +109,15 @@ __device__ __forceinline__ StarHit shfl_hit(const StarHit& h, int b) {
 // Phase A, lane = pixel: corners, lensing, redshift, kd-tree search; the
 // leaves whose stars may fall inside the pixel's quad are listed in shared
 // memory (pixels over the budget go to the heavy list).  Phase B, for each
-// pixel of the warp in turn: the warp tests the listed stars 32 at a time,
-// the lanes holding a hit place their star in the pixel (bisection) and
-// colour it, and the hits are splatted in star order: lane c < (2s+1)^2
-// owns cell c and adds each star's contribution in the order the reference
-// does, so every cell is bit-identical to the reference's.
+// pixel of the warp in turn: the warp tests the listed stars 32 at a time
+// and appends the hits, in star order, to a queue of the warp.  A full queue
+// (or the end of the warp's pixels) is drained: each lane places one queued
+// star in its pixel (bisection) and colours it, then the hits are splatted in
+// queue order: lane c < (2s+1)^2 owns cell c of the pixel being summed and
+// adds each star's contribution in the order the reference does, so every
+// cell is bit-identical to the reference's.  Queueing across pixels lets the
+// bisection run on 32 hits at once instead of on the one or two lanes of a
+// test step that holds a hit.
 __global__ void __launch_bounds__(TX * TY)
 k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
              StarSet S, Cam7 cam, int M, int N, int step,
@@ -160,15 +164,74 @@ k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
   }
   __syncwarp();
 
-  // ---- phase B: the warp splats each listed pixel ----
+  // ---- phase B: the warp tests the stars of each listed pixel; hits wait
+  // in a per-warp queue in test order and are placed 32 at a time ----
+  __shared__ int sh_hq[kWarps][32];
+  __shared__ float2 sh_hpos[kWarps][32];
+  __shared__ uint8_t sh_hpx[kWarps][32];
+  const float maxDistSq = (step + .5f) * (step + .5f);
   int my_any = 0;
+  int qn = 0;
+  int cur = -1;  // the pixel whose cells acc holds
+  float3 acc = make_float3(0.f, 0.f, 0.f);
+  auto flush_cells = [&]() {
+    if (cur >= 0) {
+      const size_t pij = (size_t)i * M + (blockIdx.x * TX + cur);
+      if (lane < fw2) cells[pij * fw2 + lane] = acc;
+      if (lane == cur) my_any = 1;
+    }
+  };
+  auto drain = [&](int count) {
+    StarHit h{};
+    int hpx = 0;
+    if (lane < count) {
+      hpx = sh_hpx[w][lane];
+      PixelStars Q;
+      stars_of(sh_core[w][hpx], step, Q);
+      const float2 pos = sh_hpos[w][lane];
+      h = star_hit(Q, S, sh_hq[w][lane], pos.x, pos.y);
+    }
+    // The cells of G = 32 / (2s+1)^2 queued stars per step: lane g (2s+1)^2 + c
+    // computes cell c of star e0 + g, then lane c adds the G results in queue
+    // order.  A cell outside the splat radius yields +0, which leaves the sum
+    // unchanged (the sums start at +0 and add squares), so every cell sums
+    // exactly what the star-by-star loop of the reference sums.
+    const int G = 32 / fw2;
+    const int g = lane / fw2, c = lane - g * fw2;
+    for (int e0 = 0; e0 < count; e0 += G) {
+      const bool mine = g < G && e0 + g < count;
+      const int src = mine ? e0 + g : 0;
+      const StarHit hb = shfl_hit(h, src);
+      const int pl = __shfl_sync(0xffffffffu, hpx, src);
+      float3 l = make_float3(0.f, 0.f, 0.f);
+      if (mine && !cell_light_v(step, maxDistSq, sh_core[w][pl].frac, hb.st, hb.sp, hb.part,
+                                hb.hsp.x, hb.hsp.y, hb.hsp.z, c / fw, c % fw, l))
+        l = make_float3(0.f, 0.f, 0.f);
+      const int ng = min(G, count - e0);
+      for (int k = 0; k < ng; k++) {
+        const int pe = __shfl_sync(0xffffffffu, hpx, e0 + k);
+        if (pe != cur) {
+          flush_cells();
+          cur = pe;
+          acc = make_float3(0.f, 0.f, 0.f);
+        }
+        const int from = min(k * fw2 + lane, 31);
+        const float lx = __shfl_sync(0xffffffffu, l.x, from);
+        const float ly = __shfl_sync(0xffffffffu, l.y, from);
+        const float lz = __shfl_sync(0xffffffffu, l.z, from);
+        if (lane < fw2) {
+          acc.x += lx;
+          acc.y += ly;
+          acc.z += lz;
+        }
+      }
+    }
+  };
   for (int px = 0; px < 32; px++) {
     const int n = __shfl_sync(0xffffffffu, nleaf, px);
     if (n == 0) continue;
     PixelStars P;
     stars_of(sh_core[w][px], step, P);
-    float3 acc = make_float3(0.f, 0.f, 0.f);
-    bool any = false;
     for (int k = 0; k < n; k++) {
       int a0, a1;
       node_range(S, sh_leaf[w][k][px], a0, a1);
@@ -176,30 +239,30 @@ k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
         const int q = base + lane;
         float st = 0.f, sp = 0.f;
         const bool in = q < a1 && star_test(P, S, q, st, sp);
-        unsigned ball = __ballot_sync(0xffffffffu, in);
+        const unsigned ball = __ballot_sync(0xffffffffu, in);
         if (!ball) continue;
-        any = true;
-        StarHit h{};
-        if (in) h = star_hit(P, S, q, st, sp);
-        while (ball) {
-          const int b = __ffs(ball) - 1;
-          ball &= ball - 1;
-          const StarHit hb = shfl_hit(h, b);
-          float3 l;
-          if (lane < fw2 && cell_light(P, hb, lane / fw, lane % fw, l)) {
-            acc.x += l.x;
-            acc.y += l.y;
-            acc.z += l.z;
-          }
+        const int cnt = __popc(ball);
+        if (qn + cnt > 32) {
+          __syncwarp();
+          drain(qn);
+          __syncwarp();
+          qn = 0;
         }
+        if (in) {
+          const int at = qn + __popc(ball & ((1u << lane) - 1u));
+          sh_hq[w][at] = q;
+          sh_hpos[w][at] = make_float2(st, sp);
+          sh_hpx[w][at] = (uint8_t)px;
+        }
+        qn += cnt;
       }
     }
-    if (any) {
-      const size_t pij = (size_t)i * M + (blockIdx.x * TX + px);
-      if (lane < fw2) cells[pij * fw2 + lane] = acc;
-      if (lane == px) my_any = 1;
-    }
   }
+  if (qn) {
+    __syncwarp();
+    drain(qn);
+  }
+  flush_cells();
   // heavy pixels are written 0 here and flagged again by k_star_heavy
   if (valid) flag[ij] = (uint8_t)my_any;
 }

@@ -290,15 +290,30 @@ BT_HD float3 blackbody_hsp(int k) {
   return h;
 }
 
+// in_quad from the pixel's edge terms: edge k is cross_pos(corner k, corner
+// k+1) with c1 = (P.et[k], P.ep[k]) and c2 = star - corner k+1, the same
+// products and differences in the same order, so the result is identical;
+// the four edges are combined without short-circuit branches.
+BT_HD bool in_quad_edges(const PixelStars& P, float st, float sp) {
+  bool r = true;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const int k1 = (k + 1) & 3;
+    r &= (P.et[k] * (sp - P.p[k1]) - (st - P.t[k1]) * P.ep[k]) > 0;
+  }
+  return r;
+}
+
 // The quad test of star q (with the seam retry), BT/MakeImageKernel.cu:285-291.
 BT_HD bool star_test(const PixelStars& P, const StarSet& S, int q, float& st,
                      float& sp) {
-  st = S.pos[2 * q];
-  sp = S.pos[2 * q + 1];
-  bool in = in_quad(P.t, P.p, st, sp, P.sgn);
+  const float2 pq = reinterpret_cast<const float2*>(S.pos)[q];  // 8-byte aligned
+  st = pq.x;
+  sp = pq.y;
+  bool in = in_quad_edges(P, st, sp);
   if (P.picheck && !in && sp < PI2 * .2f) {
     sp += PI2;
-    in = in_quad(P.t, P.p, st, sp, P.sgn);
+    in = in_quad_edges(P, st, sp);
   }
   return in;
 }
