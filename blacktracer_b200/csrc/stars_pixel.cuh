@@ -116,23 +116,25 @@ BT_HD void in_pixel(float t0, float t1, float t2, float t3, float p0,
     const int a = (((l0312T * l03sP) - (l03sT * l0312P)) > 0.f) ? 1 : -1;
     const int b = (((l0123T * l01sP) - (l01sT * l0123P)) > 0.f) ? 1 : -1;
     perc *= 0.5f;
-    if (sgn * a > 0) {
-      if (sgn * b > 0) {
-        t2 = h12T; t0 = h01T; t3 = midT; p2 = h12P; p0 = h01P; p3 = midP;
-        x -= perc; y -= perc;
-      } else {
-        t2 = midT; t1 = h01T; t3 = h03T; p2 = midP; p1 = h01P; p3 = h03P;
-        x -= perc; y += perc;
-      }
-    } else {
-      if (sgn * b > 0) {
-        t1 = h12T; t3 = h23T; t0 = midT; p1 = h12P; p3 = h23P; p0 = midP;
-        x += perc; y -= perc;
-      } else {
-        t0 = h03T; t1 = midT; t2 = h23T; p0 = h03P; p1 = midP; p2 = h23P;
-        x += perc; y += perc;
-      }
-    }
+    // The reference's four quadrant cases as selects (the same values, no
+    // divergent branches between lanes):
+    //   A  B : t2 = h12, t0 = h01, t3 = mid;  x -= perc, y -= perc
+    //   A !B : t2 = mid, t1 = h01, t3 = h03;  x -= perc, y += perc
+    //  !A  B : t1 = h12, t3 = h23, t0 = mid;  x += perc, y -= perc
+    //  !A !B : t0 = h03, t1 = mid, t2 = h23;  x += perc, y += perc
+    const bool A = sgn * a > 0, B = sgn * b > 0;
+    const float n0T = A ? (B ? h01T : t0) : (B ? midT : h03T);
+    const float n1T = A ? (B ? t1 : h01T) : (B ? h12T : midT);
+    const float n2T = A ? (B ? h12T : midT) : (B ? t2 : h23T);
+    const float n3T = A ? (B ? midT : h03T) : (B ? h23T : t3);
+    const float n0P = A ? (B ? h01P : p0) : (B ? midP : h03P);
+    const float n1P = A ? (B ? p1 : h01P) : (B ? h12P : midP);
+    const float n2P = A ? (B ? h12P : midP) : (B ? p2 : h23P);
+    const float n3P = A ? (B ? midP : h03P) : (B ? h23P : p3);
+    t0 = n0T; t1 = n1T; t2 = n2T; t3 = n3T;
+    p0 = n0P; p1 = n1P; p2 = n2P; p3 = n3P;
+    x = A ? x - perc : x + perc;
+    y = B ? y - perc : y + perc;
     midT = (t0 + t1 + t2 + t3) * .25f;
     midP = (p0 + p1 + p2 + p3) * .25f;
   }
