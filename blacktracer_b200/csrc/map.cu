@@ -550,6 +550,11 @@ __global__ void k_env_wide(const float2* __restrict__ thphi, uchar4* __restrict_
 }
 
 int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s) {
+  if (int rc = map_run_prep(S, F, s)) return rc;
+  return map_run_envmap(S, F, s);
+}
+
+int map_run_prep(MapScratch& S, const MapFrame& F, cudaStream_t s) {
   const int M = S.M, N = S.N;
   GridRef G{F.grid, F.GM, F.GN};
   if (F.grid2) {
@@ -565,6 +570,11 @@ int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s) {
   k_smooth_h<<<grid2(M, N), dim3(TX, TY), 0, s>>>(S.area_tmp, S.area, S.bh, S.gap, M, N);
   k_smooth_v<<<grid2(M, N), dim3(TX, TY), 0, s>>>(S.area_tmp, S.area, S.bh, S.gap, M, N);
   BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
+int map_run_envmap(MapScratch& S, const MapFrame& F, cudaStream_t s) {
+  const int M = S.M, N = S.N;
   if (F.map && F.env) {
     BT_CUDA_TRY(cudaMemsetAsync(S.env_wide_count, 0, sizeof(uint32_t), s));
     k_env<<<grid2(M, N), dim3(TX, TY), 0, s>>>(

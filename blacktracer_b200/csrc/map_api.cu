@@ -24,6 +24,12 @@ struct bt_blend {
 struct bt_map {
   bt::MapScratch S;
   uint8_t* tmp_img;  // env image when stars are composited on top
+  // The environment image of a frame with stars is drawn on a second stream
+  // (the caller's priority) while the star passes run: it needs only the
+  // pixel set-up and the stars need it only when compositing.
+  cudaStream_t side;
+  int side_prio;
+  cudaEvent_t ev_prep, ev_bg;
 };
 
 using namespace bt;
@@ -38,6 +44,27 @@ void map_free(bt_map* m) {
                   m->S.env_wide_count, m->tmp_img};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (m->side) {
+    cudaStreamSynchronize(m->side);
+    cudaStreamDestroy(m->side);
+  }
+  if (m->ev_prep) cudaEventDestroy(m->ev_prep);
+  if (m->ev_bg) cudaEventDestroy(m->ev_bg);
+}
+
+// The side stream at the priority of the caller's stream s.
+int side_stream(bt_map* m, cudaStream_t s) {
+  int prio = 0;
+  BT_CUDA_TRY(cudaStreamGetPriority(s, &prio));
+  if (m->side && prio == m->side_prio) return BT_OK;
+  if (m->side) {
+    BT_CUDA_TRY(cudaStreamSynchronize(m->side));
+    BT_CUDA_TRY(cudaStreamDestroy(m->side));
+    m->side = nullptr;
+  }
+  BT_CUDA_TRY(cudaStreamCreateWithPriority(&m->side, cudaStreamNonBlocking, prio));
+  m->side_prio = prio;
+  return BT_OK;
 }
 
 }  // namespace
@@ -237,6 +264,8 @@ int bt_map_create(int width, int height, bt_map** out) {
   MALLOC(S.heavy_count, 4 * sizeof(uint32_t));
   MALLOC(m->tmp_img, np * 4);
 #undef MALLOC
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->ev_prep, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&m->ev_bg, cudaEventDisableTiming);
   if (e != cudaSuccess) {
     map_free(m);
     delete m;
@@ -278,6 +307,18 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
   // environment into the output directly, or into a temporary when stars
   // are composited on top (addStarsAndBackground)
   F.out_bg = (f->star && f->map) ? m->tmp_img : f->out;
+  if (f->star && f->map) {
+    if (int rc = side_stream(m, s)) return rc;
+    if (int rc = map_run_prep(m->S, F, s)) return rc;
+    BT_CUDA_TRY(cudaEventRecord(m->ev_prep, s));
+    BT_CUDA_TRY(cudaStreamWaitEvent(m->side, m->ev_prep, 0));
+    if (int rc = map_run_envmap(m->S, F, m->side)) return rc;
+    BT_CUDA_TRY(cudaEventRecord(m->ev_bg, m->side));
+    F.bg_ready = m->ev_bg;
+    const int rc = map_run_stars(m->S, F, s);
+    if (rc) cudaStreamWaitEvent(s, m->ev_bg, 0);  // the caller's stream still joins
+    return rc;
+  }
   int rc = map_run_env(m->S, F, s);
   if (rc) return rc;
   if (f->star) {

@@ -61,9 +61,16 @@ struct MapFrame {
   uint8_t* out_bg;      // N*M*4 environment (or final) image
   uint8_t* out;         // N*M*4 final image
   bt_trails* trails;    // star trails between frames, or NULL
+  // Set when the environment image is drawn on another stream: compositing
+  // onto out_bg waits for it.
+  cudaEvent_t bg_ready = nullptr;
 };
 
 int map_run_env(MapScratch& S, const MapFrame& F, cudaStream_t s);
+// The two parts of map_run_env: the per-pixel corners, shadow mask and
+// smoothed solid angles, then the environment image (which reads only those).
+int map_run_prep(MapScratch& S, const MapFrame& F, cudaStream_t s);
+int map_run_envmap(MapScratch& S, const MapFrame& F, cudaStream_t s);
 int blend_prepare(const float2* ga, const float2* gb, int GN, int GM, float2* border,
                   float2* border2, int nang, uint32_t* edge, cudaStream_t s);
 int map_run_stars(MapScratch& S, const MapFrame& F, cudaStream_t s);

@@ -895,6 +895,7 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   }
   const bool diff = F.diffraction && SS.psf && SS.psf_size > 0;
   if (!diff) {
+    if (F.bg_ready) BT_CUDA_TRY(cudaStreamWaitEvent(s, F.bg_ready, 0));
     k_star_gather<true><<<grid2(M, N), dim3(TX, TY), 0, s>>>(
         Sc.cells, Sc.flag, M, N, F.step, Sc.light, (const uchar4*)F.out_bg,
         (uchar4*)F.out, F.map, trail);
@@ -943,6 +944,7 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
     k_diff_scatter<<<sm_count() * 8, 256, 0, s>>>(Sc.light, Sc.light2, Sc.diff_list,
                                                   Sc.diff_count, M, N, SS.psf, SS.psf_size);
   }
+  if (F.bg_ready) BT_CUDA_TRY(cudaStreamWaitEvent(s, F.bg_ready, 0));
   k_makepix<<<grid2(M, N), dim3(TX, TY), 0, s>>>(Sc.light2, M, N,
                                                  (const uchar4*)F.out_bg,
                                                  (uchar4*)F.out, F.map);
