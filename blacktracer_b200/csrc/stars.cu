@@ -308,7 +308,7 @@ __global__ void k_heavy_plan(const float2* __restrict__ thphi,
 // shared counter (giant pixels first).  Thread 0 walks the kd-tree (in
 // passes of kHeavyNodes emitted nodes) into shared memory with a prefix sum
 // of the number of leaves under each node.  The block then takes that flat
-// range of candidate leaves 256 at a time: each thread tests one leaf's
+// range of candidate leaves 512 at a time: each thread tests one leaf's
 // bounding box against the pixel's quad, the survivors are compacted in
 // thread order, and each warp sweeps the stars of one surviving leaf at a
 // time, 32 stars per step.  A thread that holds a hit splats it into its own
