@@ -419,6 +419,11 @@ int bt_trails_query(bt_trails* t, bt_trails_info* info, void* stream);
  * 550 nm, scaled per channel by wavelength (R 610, G 550, B 465 nm), 255 at
  * the centre.  For bt_stars_create's psf_rgb. */
 int bt_psf_airy(int size, float first_zero, uint8_t* rgb);
+/* Renders one frame on `stream`.  A frame that draws both the environment and
+ * stars draws the environment on a second stream owned by `m` (created at the
+ * priority of `stream`) while the star passes run on `stream`; `stream` waits
+ * for it before compositing, so all work of the call is done when the work
+ * queued on `stream` is. */
 int bt_map_render(bt_map* m, const bt_frame* f, void* stream);
 
 /* Device pointers into a renderer's scratch after a frame (for tests and
