@@ -110,14 +110,14 @@ __device__ __forceinline__ StarHit shfl_hit(const StarHit& h, int b) {
 // leaves whose stars may fall inside the pixel's quad are listed in shared
 // memory (pixels over the budget go to the heavy list).  Phase B, for each
 // pixel of the warp in turn: the warp tests the listed stars 32 at a time
-// and appends the hits, in star order, to a queue of the warp.  A full queue
-// (or the end of the warp's pixels) is drained: each lane places one queued
-// star in its pixel (bisection) and colours it, then the hits are splatted in
-// queue order: lane c < (2s+1)^2 owns cell c of the pixel being summed and
-// adds each star's contribution in the order the reference does, so every
-// cell is bit-identical to the reference's.  Queueing across pixels lets the
-// bisection run on 32 hits at once instead of on the one or two lanes of a
-// test step that holds a hit.
+// and appends the hits, in star order, to a queue of the warp.  A queue that
+// cannot take a test step's hits (and the queue at the end) is drained: each
+// lane places one queued star in its pixel (bisection) and colours it, then
+// the stars' cells are computed a few stars per warp step and added in queue
+// order, so each cell of each pixel sums its stars in the order the
+// reference does and is bit-identical to the reference's.  Queueing across
+// pixels lets the bisection run on up to 32 hits at once instead of on the
+// one or two lanes of a test step that hold a hit.
 __global__ void __launch_bounds__(TX * TY)
 k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
              StarSet S, Cam7 cam, int M, int N, int step,
@@ -165,7 +165,8 @@ k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
   __syncwarp();
 
   // ---- phase B: the warp tests the stars of each listed pixel; hits wait
-  // in a per-warp queue in test order and are placed 32 at a time ----
+  // in a per-warp queue of 32 in test order, which is drained (placed and
+  // splatted, one hit per lane) when a test step's hits would not fit ----
   __shared__ int sh_hq[kWarps][32];
   __shared__ float2 sh_hpos[kWarps][32];
   __shared__ uint8_t sh_hpx[kWarps][32];
@@ -191,9 +192,9 @@ k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
       const float2 pos = sh_hpos[w][lane];
       h = star_hit(Q, S, sh_hq[w][lane], pos.x, pos.y);
     }
-    // The cells of G = 32 / (2s+1)^2 queued stars per step: lane g (2s+1)^2 + c
-    // computes cell c of star e0 + g, then lane c adds the G results in queue
-    // order.  A cell outside the splat radius yields +0, which leaves the sum
+    // The cells of G = 32 / (2s+1)^2 queued stars per step: lane
+    // g * (2s+1)^2 + c computes cell c of star e0 + g, then lane c adds the G
+    // results in queue order.  A cell outside the splat radius yields +0, which leaves the sum
     // unchanged (the sums start at +0 and add squares), so every cell sums
     // exactly what the star-by-star loop of the reference sums.
     const int G = 32 / fw2;
