@@ -49,8 +49,9 @@ def _stale(target: str, deps: list[str]) -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(OBJ, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for unit, flags in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(OBJ, unit.replace(".cu", ".o"))
@@ -60,7 +61,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
             if verbose:
                 cmd += ["-Xptxas", "-v"]
                 print(" ".join(cmd), file=sys.stderr)
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    # translation units compile independently
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(lambda c: subprocess.run(c, check=True), cmds))
     if force or _stale(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
         subprocess.run(cmd, check=True)

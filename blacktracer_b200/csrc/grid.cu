@@ -107,8 +107,11 @@ struct bt_batch {
   int graph;
   cudaStream_t cap_stream;
   cudaGraphExec_t exec;
-  int exec_n, exec_startlevel, exec_precision;
+  int exec_n, exec_startlevel, exec_precision, exec_tfix_passes;
   bt::TraceShape exec_shape;
+  // Jacobi passes of the T-vertex fix per level (kMaxTfixPasses unless a
+  // test lowers it with bt_grid_set_tfix_passes)
+  int tfix_passes;
 };
 
 namespace bt {
@@ -592,15 +595,15 @@ __global__ void k_tfix_pass(const GridDesc* __restrict__ D, int level, int pass,
 }
 
 // Copies the converged values of a level's T-vertices into the lattice (the
-// last pass wrote X[0]; passes skipped after convergence left both buffers
-// equal on every written vertex).
+// last pass, `passes`, wrote X[passes & 1]; passes skipped after convergence
+// left both buffers equal on every written vertex).
 __global__ void k_tfix_commit(const GridDesc* __restrict__ D, int level, int lo_slot,
-                              int hi_slot) {
+                              int hi_slot, int passes) {
   const GridDesc& d = D[blockIdx.y];
   GridCounters* ctr = d.ctr;
   const uint32_t lo = ctr->leaf_off[lo_slot], hi = ctr->leaf_off[hi_slot];
   const LatticeView L = d.L;
-  const double2* X = d.X[0];
+  const double2* X = d.X[passes & 1];
   const uint32_t M = L.M;
   const uint32_t g = pow2u(L.maxlevel - level);
   const uint64_t n4 = 4ull * (hi - lo);
@@ -875,6 +878,7 @@ int batch_create(int maxlevel, int angle, int count, bt_batch** out) {
   b->maxlevel = maxlevel;
   b->NM = (size_t)N * M;
   b->shape = TraceShape{128, 0};
+  b->tfix_passes = bt::kMaxTfixPasses;
   b->grids = new (std::nothrow) bt_grid[count];
   if (!b->grids) {
     delete b;
@@ -1012,12 +1016,13 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
   const unsigned nb = set_blocks(NM / 16, 128, G);
   for (int level = startlevel; level < b->maxlevel; level++) {
     const int lo = level - startlevel, hi = level - startlevel + 1;
-    for (int pass = 1; pass <= kMaxTfixPasses; pass++)
+    const int passes = b->tfix_passes;
+    for (int pass = 1; pass <= passes; pass++)
       k_tfix_pass<<<dim3(nb, G), 128, 0, s>>>(b->D, level, pass, lo, hi);
-    k_tfix_commit<<<dim3(nb, G), 128, 0, s>>>(b->D, level, lo, hi);
-    k_tfix_check<<<ga, 128, 0, s>>>(b->D, G, kMaxTfixPasses);
+    k_tfix_commit<<<dim3(nb, G), 128, 0, s>>>(b->D, level, lo, hi, passes);
+    k_tfix_check<<<ga, 128, 0, s>>>(b->D, G, passes);
     BT_CUDA_TRY(cudaGetLastError());
-    nk += kMaxTfixPasses + 2;
+    nk += passes + 2;
   }
   BT_CUDA_TRY(cudaMemcpyAsync(b->ctr_host, b->ctr, G * sizeof(GridCounters),
                               cudaMemcpyDeviceToHost, s));
@@ -1061,6 +1066,7 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int n,
   if (b->graph) {
     const bool same = b->exec && b->exec_n == G && b->exec_startlevel == startlevel &&
                       b->exec_precision == precision &&
+                      b->exec_tfix_passes == b->tfix_passes &&
                       b->exec_shape.threads == b->shape.threads &&
                       b->exec_shape.blocks_per_sm == b->shape.blocks_per_sm;
     if (!same) {
@@ -1089,6 +1095,7 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int n,
       b->exec_n = G;
       b->exec_startlevel = startlevel;
       b->exec_precision = precision;
+      b->exec_tfix_passes = b->tfix_passes;
       b->exec_shape = b->shape;
       b->launches = launches;
     }
@@ -1217,6 +1224,14 @@ int bt_grid_set_timing(bt_grid* g, int on) {
 int bt_grid_set_graph(bt_grid* g, int on) {
   BT_ARG_CHECK(g != nullptr, "NULL grid");
   g->set->graph = on ? 1 : 0;
+  return BT_OK;
+}
+
+int bt_grid_set_tfix_passes(bt_grid* g, int passes) {
+  clear_error();
+  BT_ARG_CHECK(g != nullptr, "NULL grid");
+  BT_ARG_CHECK(passes >= 1 && passes <= kMaxTfixPasses, "passes must be in [1, 8]");
+  g->set->tfix_passes = passes;
   return BT_OK;
 }
 

@@ -7,13 +7,17 @@ match the reference's bit for bit, so the table is the same data; this
 script reads it from the reference tree once and writes the header, which is
 committed.
 
-    python blacktracer_b200/csrc/make_blackbody_table.py /root/reference
+    python blacktracer_b200/csrc/make_blackbody_table.py [reference tree]
+
+The tree defaults to $BT_REFERENCE_DIR.
 """
 import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("BT_REFERENCE_DIR", "")
+if not ref:
+    sys.exit("usage: make_blackbody_table.py <reference tree> (or set BT_REFERENCE_DIR)")
 src = open(os.path.join(ref, "BlackTracer2", "BlackTracer", "Const.h")).read()
 body = src[src.index("tempToRGBx"):]
 body = body[body.index("{") + 1: body.index("}")]

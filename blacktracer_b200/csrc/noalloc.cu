@@ -12,6 +12,9 @@
 #include <cstring>
 #include <mutex>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "bt_internal.h"
 
 namespace {
@@ -27,10 +30,29 @@ static __device__ __align__(256) unsigned char g_static_stage[kStageBytes];
 
 std::mutex g_stage_mu;
 void* g_stage_addr[kMaxDevices] = {};
+CUcontext g_stage_ctx[kMaxDevices] = {};
+PFN_cuCtxGetCurrent_v4000 g_ctx_current = nullptr;
+
+// The current context, through the driver entry point the runtime exposes
+// (no link against the driver library); nullptr if it cannot be had.
+CUcontext current_context() {
+  if (!g_ctx_current) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    g_ctx_current = (PFN_cuCtxGetCurrent_v4000)fn;
+  }
+  CUcontext c = nullptr;
+  return g_ctx_current(&c) == CUDA_SUCCESS ? c : nullptr;
+}
 
 // Device address of the static staging array on the current device.  In
 // host code the symbol names a host-side stand-in, not device memory, so the
-// address is looked up once per device (with that device current) and kept.
+// address is looked up with the device current and kept, per device and per
+// context: after cudaDeviceReset the device gets a new context, the module
+// is loaded again, and the address is looked up again.
 int stage_address(void** out) {
   int dev = 0;
   BT_CUDA_TRY(cudaGetDevice(&dev));
@@ -39,7 +61,10 @@ int stage_address(void** out) {
     return BT_ERR_ARG;
   }
   std::lock_guard<std::mutex> lk(g_stage_mu);
-  if (!g_stage_addr[dev]) {
+  // No current context yet on this thread (the runtime makes the primary
+  // context current on first use) also leads to a lookup, which does that.
+  const CUcontext ctx = current_context();
+  if (!g_stage_addr[dev] || ctx == nullptr || ctx != g_stage_ctx[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_static_stage);
     if (e != cudaSuccess || p == nullptr) {
@@ -48,6 +73,7 @@ int stage_address(void** out) {
       return BT_ERR_CUDA;
     }
     g_stage_addr[dev] = p;
+    g_stage_ctx[dev] = current_context();
   }
   *out = g_stage_addr[dev];
   return BT_OK;
@@ -75,9 +101,9 @@ int bt_integrate_rays_host_static(const bt_camera* cam, double a,
     return BT_ERR_ARG;
   }
   bt::RayParams p;
-  if (bt::make_ray_params(cam, a, o, &p)) {
+  if (int rc = bt::make_ray_params(cam, a, o, &p)) {
     bt::set_error("invalid camera or integrator options");
-    return BT_ERR_ARG;
+    return rc;
   }
   void* base = nullptr;
   if (int rc = stage_address(&base)) return rc;

@@ -239,6 +239,12 @@ class Grid:
         """Capture later builds once into a CUDA graph and replay it."""
         L.check(L.lib().bt_grid_set_graph(self._h, 1 if on else 0))
 
+    def set_tfix_passes(self, passes: int):
+        """Jacobi passes of the T-vertex fix per level of later builds (1..8;
+        default 8).  A level still changing at its last pass is reported as
+        not converged by info() (flag 1, BtError BT_ERR_NUMERIC)."""
+        L.check(L.lib().bt_grid_set_tfix_passes(self._h, int(passes)))
+
     def export(self, out=None, pinned=True):
         """The grid as key-ordered lists (CamToCel, steps, blockLevels).
 

@@ -120,8 +120,10 @@ int bt_integrate_rays_host(const bt_camera* cam, double a, const double* theta,
  * bt_integrate_rays_host_static_capacity() rays (65536), held by every GPU
  * that loads this library until the process exits; larger n is rejected
  * with BT_ERR_ARG.  The first call on a device looks up that array's
- * address (once per device, with the device current); make that first call
- * before any stream capture.  All calls share the one array: calls that
+ * address (with the device current) and keeps it for that device's current
+ * context; a call after cudaDeviceReset, in the new context, looks it up
+ * again.  Make the first call on a device before any stream capture.
+ * status may be NULL.  All calls share the one array: calls that
  * overlap on the GPU (other threads or streams of the same device) race on
  * it and must be serialised by the caller.  Synchronises `stream`. */
 int bt_integrate_rays_host_static(const bt_camera* cam, double a,
@@ -182,6 +184,14 @@ int bt_grid_set_timing(bt_grid* g, int on);
  * level, precision and trace launch shape) and replayed.  No counterpart in
  * the reference (its build is host-driven). */
 int bt_grid_set_graph(bt_grid* g, int on);
+
+/* Diagnostic: the number of Jacobi passes of the T-vertex fix per level of
+ * later builds, 1..8 (default 8, the most any grid needs; 2-3 is typical).
+ * A level whose last pass still changed a vertex is reported as not
+ * converged: flag 1 in bt_grid_info.flags and BT_ERR_NUMERIC from
+ * bt_grid_query.  Lowering it exists to exercise that report.  No
+ * counterpart in the reference (its fixTvertices is sequential). */
+int bt_grid_set_tfix_passes(bt_grid* g, int passes);
 
 /* Synchronises `stream` and reports the build.  Returns BT_ERR_NUMERIC when
  * a bounded loop (T-vertex fixed point) gave up. */

@@ -38,14 +38,25 @@ _u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 _i8p = np.ctypeslib.ndpointer(dtype=np.int8, flags="C_CONTIGUOUS")
 
 
+def reference_dir() -> str:
+    """The reference tree the harness is compiled from: $BT_REFERENCE_DIR,
+    else the default checkout location."""
+    return os.environ.get("BT_REFERENCE_DIR", "/root/reference")
+
+
+def have_reference_tree() -> bool:
+    return os.path.isdir(os.path.join(reference_dir(), "BlackTracer2"))
+
+
 def build(with_ref: bool | None = None) -> None:
     """Compile the restatement (and the reference harness when the reference
     tree is present)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     if with_ref is None:
-        with_ref = os.path.isdir("/root/reference/BlackTracer2")
+        with_ref = have_reference_tree()
     if with_ref:
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={reference_dir()}"],
+                       check=True)
 
 
 _orc = None

@@ -16,7 +16,7 @@ def pytest_configure(config):
 @pytest.fixture(scope="session")
 def oracle_mod():
     import oracle
-    oracle.build(with_ref=os.path.isdir("/root/reference/BlackTracer2"))
+    oracle.build(with_ref=oracle.have_reference_tree())
     return oracle
 
 

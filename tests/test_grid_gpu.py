@@ -108,3 +108,30 @@ def test_fast_grid_topology_matches_plain(bt, cuda, oracle_mod, ml, sl, camname)
     err = ang_err(df["theta"][e], df["phi"][e], dp["theta"][e], dp["phi"][e])
     print(f"fast grid L{ml}{camname}: p99 {np.percentile(err, 99):.2e} max {err.max():.2e}")
     assert np.percentile(err, 99) <= 1e-6
+
+
+def test_tfix_nonconvergence_is_reported(bt, cuda, oracle_mod):
+    """With one T-vertex pass per level the fix cannot see a pass that
+    changed nothing, so the build must report it as not converged: flag 1
+    in bt_grid_info.flags and BT_ERR_NUMERIC from bt_grid_query.  The
+    default pass count converges on the same grid."""
+    import ctypes as C
+
+    from blacktracer_b200 import _lib as L
+    cam, a = oracle_camera(oracle_mod, "c2")
+    g = bt.Grid(9, 6, True, bt.Camera.from_array(cam, a), opts="plain")
+    assert g.info().flags == 0
+    g.set_tfix_passes(1)
+    g.build()
+    inf = L.bt_grid_info()
+    rc = L.lib().bt_grid_query(g._h, C.byref(inf), None)
+    assert rc == L.BT_ERR_NUMERIC
+    assert inf.flags & 1
+    assert b"T-vertex" in L.lib().bt_last_error()
+    with pytest.raises(L.BtError):
+        g.info()
+    g.set_tfix_passes(8)
+    g.build()
+    assert g.info().flags == 0
+    with pytest.raises(L.BtError):
+        g.set_tfix_passes(0)
