@@ -171,6 +171,10 @@ _SIGS = {
     "bt_env_sat": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "bt_stars_tree_size": (C.c_int, [C.c_int]),
     "bt_psf_airy": (C.c_int, [C.c_int, C.c_float, _vp]),
+    "bt_psf_levels": (C.c_int, [_vp, C.c_int, C.c_int, _vp, _vp, C.c_int,
+                                C.POINTER(C.c_int)]),
+    "bt_stars_blackbody": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int, C.POINTER(C.c_int), _vp]),
+    "bt_map_diffract": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "bt_blend_create": (C.c_int, [C.POINTER(_vp)]),
     "bt_blend_destroy": (None, [_vp]),
     "bt_blend_prepare": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp]),

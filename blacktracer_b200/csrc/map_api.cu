@@ -328,6 +328,14 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
   return BT_OK;
 }
 
+int bt_map_diffract(bt_map* m, const bt_stars* stars, const float* light, float* out,
+                    void* stream) {
+  clear_error();
+  BT_ARG_CHECK(m && stars && light && out, "NULL pointer");
+  BT_ARG_CHECK(light != out, "light and out must be different buffers");
+  return map_diffract_light(m->S, stars, light, out, (cudaStream_t)stream);
+}
+
 int bt_map_census(bt_map* m, const bt_frame* f, bt_map_census_t* out, void* stream) {
   clear_error();
   BT_ARG_CHECK(m && f && out, "NULL pointer");

@@ -74,6 +74,12 @@ int map_run_envmap(MapScratch& S, const MapFrame& F, cudaStream_t s);
 int blend_prepare(const float2* ga, const float2* gb, int GN, int GM, float2* border,
                   float2* border2, int nang, uint32_t* edge, cudaStream_t s);
 int map_run_stars(MapScratch& S, const MapFrame& F, cudaStream_t s);
+// addDiffraction of a star-light buffer (N*M*3 floats) into out (stars.cu).
+int map_diffract(MapScratch& S, const StarSet& SS, const float* light, float* out,
+                 int psf_scale, const float2* view, const float* area, cudaStream_t s);
+// The same for a caller's light buffer with a star set's sprite, unscaled.
+int map_diffract_light(MapScratch& S, const bt_stars* stars, const float* light, float* out,
+                       cudaStream_t s);
 StarSet stars_for_frame(const bt_stars* s, int bb_table);
 // Star trails of this frame into the trail buffer (trails.cu).
 int trails_run(bt_trails* t, MapScratch& Sc, const MapFrame& F, const StarSet& SS,

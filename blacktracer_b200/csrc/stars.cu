@@ -593,6 +593,13 @@ __global__ void k_star_gather(const float3* __restrict__ cells,
   out[ij] = st;
 }
 
+// Light of a bright pixel as the reference's thread reads it after adding
+// the sprite's centre term (value `centre`) to its own pixel.
+__device__ __forceinline__ float psf_term_light(float l, float div, float centre) {
+  const float d = l / div * centre;
+  return l + fminf(65025.f, d * d);
+}
+
 // Diffraction, pass 1: pixels brighter than 65025 in any channel.
 __global__ void k_diff_mark(const float* __restrict__ light, int n,
                             uint32_t* __restrict__ list, uint32_t* count) {
@@ -604,7 +611,9 @@ __global__ void k_diff_mark(const float* __restrict__ light, int n,
 
 // Diffraction, pass 2 (addDiffraction, BT/MakeImageKernel.cu:775-800): one
 // block per bright pixel scatters the sprite, reading the snapshot `light`
-// and adding into `acc`.
+// and adding into `acc`.  The reference's thread reads its pixel again for
+// every sprite entry, so the entries after the centre see the centre's term
+// it added to its own pixel (psf_term_light).
 __global__ void k_diff_scatter(const float* __restrict__ light, float* acc,
                                const uint32_t* __restrict__ list,
                                const uint32_t* count, int M, int N,
@@ -620,13 +629,19 @@ __global__ void k_diff_scatter(const float* __restrict__ light, float* acc,
     if (i < fh) startx = fh - i;
     if (i > (N - fh)) endx = N - i + fh;
     const float div = 10000 * powf(mxv, 0.6);
+    const uchar3 dc = psf[fh * fs + fh];
+    const float lx2 = psf_term_light(lx, div, (float)dc.x),
+                ly2 = psf_term_light(ly, div, (float)dc.y),
+                lz2 = psf_term_light(lz, div, (float)dc.z);
     for (int c = threadIdx.x; c < (endx - startx) * fs; c += blockDim.x) {
       const int q = startx + c / fs, p = c % fs;
       const int ti = i - fh + q;
       if (ti < 0 || ti >= N) continue;
       const uchar3 d = psf[q * fs + p];
-      const float dx = lx / div * (float)d.x, dy = ly / div * (float)d.y,
-                  dz = lz / div * (float)d.z;
+      const bool post = q > fh || (q == fh && p > fh);
+      const float dx = (post ? lx2 : lx) / div * (float)d.x,
+                  dy = (post ? ly2 : ly) / div * (float)d.y,
+                  dz = (post ? lz2 : lz) / div * (float)d.z;
       const size_t t = (size_t)ti * M + (j - fh + p + M) % M;
       atomicAdd(&acc[3 * t], fminf(65025.f, dx * dx));
       atomicAdd(&acc[3 * t + 1], fminf(65025.f, dy * dy));
@@ -635,27 +650,41 @@ __global__ void k_diff_scatter(const float* __restrict__ light, float* acc,
   }
 }
 
-// Diffraction as a gather (addDiffraction, BT/MakeImageKernel.cu:775-800,
-// with snapshot reads).  A bright pixel (any channel of its summed star light
-// above 65025) adds min(65025, (light / (10000 max^0.6) * sprite)^2) per
-// channel around itself; written from the receiving side, pixel t gathers
-// that term from every bright pixel t - o for the sprite's non-zero offsets
-// o.  Pass 1 stores each pixel's coefficient light / (10000 max^0.6) (zero
-// for the others); pass 2 reads a tile of coefficients with its halo from
-// shared memory.  No atomics: the frame is deterministic.  The reference's
+// Diffraction as a gather (addDiffraction, BT/MakeImageKernel.cu:775-800).
+// A bright pixel (any channel of its summed star light above 65025) adds
+// min(65025, (light / (10000 max^0.6) * sprite)^2) per channel around
+// itself; written from the receiving side, pixel t gathers that term from
+// every bright pixel t - o for the sprite's non-zero offsets o.  Pass 1
+// stores each pixel's coefficient light / (10000 max^0.6) (zero for the
+// others); pass 2 reads a tile of coefficients with its halo from shared
+// memory.  No atomics: the frame is deterministic.  The reference's
 // arithmetic per term is kept (coefficient times sprite value, squared,
 // clamped); only the summation order differs.
-__global__ void k_diff_coef(const float* __restrict__ light, int n, float3* __restrict__ coef) {
+//
+// What each term reads: the reference's thread reads its own pixel again for
+// every sprite entry, after adding the entries before it, and the centre
+// entry lands on that pixel.  So the entries up to the centre (row-major)
+// use the pixel's light, the entries after it its light plus the centre's
+// term: two coefficients per pixel.  Other bright pixels' terms that land on
+// a bright pixel are read or not depending on thread timing in the
+// reference; here every pixel's coefficients come from the light before any
+// term is added.
+__global__ void k_diff_coef(const float* __restrict__ light, int n, float4 centre,
+                            float3* __restrict__ coef, float3* __restrict__ coef_post) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const float lx = light[3 * q], ly = light[3 * q + 1], lz = light[3 * q + 2];
   const float m = fmaxf(fmaxf(lx, ly), lz);
-  float3 c = make_float3(0.f, 0.f, 0.f);
+  float3 c = make_float3(0.f, 0.f, 0.f), c2 = c;
   if (m > 65025.f) {
     const float div = 10000 * powf(m, 0.6);
     c = make_float3(lx / div, ly / div, lz / div);
+    c2 = make_float3(psf_term_light(lx, div, centre.x) / div,
+                     psf_term_light(ly, div, centre.y) / div,
+                     psf_term_light(lz, div, centre.z) / div);
   }
   coef[q] = c;
+  coef_post[q] = c2;
 }
 
 constexpr int kDiffTX = 32, kDiffTY = 8;
@@ -676,20 +705,12 @@ __device__ __forceinline__ void load_coef_tile(const float3* __restrict__ coef, 
   }
 }
 
-__global__ void __launch_bounds__(kDiffTX * kDiffTY)
-k_diff_gather(const float3* __restrict__ coef, const float* __restrict__ light,
-              float* __restrict__ out, int M, int N, const short2* __restrict__ nzoff,
-              const float4* __restrict__ nzval, int nnz, int H) {
-  extern __shared__ float3 tile[];
-  const int i0 = blockIdx.y * kDiffTY, j0 = blockIdx.x * kDiffTX;
-  load_coef_tile(coef, M, N, i0, j0, H, tile);
-  __syncthreads();
-  const int ti = i0 + threadIdx.y, tj = j0 + threadIdx.x;
-  if (ti >= N || tj >= M) return;
-  const int TW = kDiffTX + 2 * H;
-  const int base = (threadIdx.y + H) * TW + threadIdx.x + H;
-  float ax = 0.f, ay = 0.f, az = 0.f;
-  for (int k = 0; k < nnz; k++) {
+// Sprite entries [k0, k1) gathered from the coefficient tile into a.
+__device__ __forceinline__ void diff_gather_range(const float3* tile, int base, int TW, int k0,
+                                                  int k1, const short2* __restrict__ nzoff,
+                                                  const float4* __restrict__ nzval,
+                                                  float& ax, float& ay, float& az) {
+  for (int k = k0; k < k1; k++) {
     const short2 o = nzoff[k];  // source = target - offset
     const float3 c = tile[base - o.x * TW - o.y];
     if (c.x == 0.f && c.y == 0.f && c.z == 0.f) continue;
@@ -699,6 +720,30 @@ k_diff_gather(const float3* __restrict__ coef, const float* __restrict__ light,
     ay += fminf(65025.f, dy * dy);
     az += fminf(65025.f, dz * dz);
   }
+}
+
+// The sprite entries up to its centre from the tile of `coef`, then the tile
+// is reloaded with `coef_post` for the entries after the centre.
+__global__ void __launch_bounds__(kDiffTX * kDiffTY)
+k_diff_gather(const float3* __restrict__ coef, const float3* __restrict__ coef_post,
+              const float* __restrict__ light, float* __restrict__ out, int M, int N,
+              const short2* __restrict__ nzoff, const float4* __restrict__ nzval, int nsplit,
+              int nnz, int H) {
+  extern __shared__ float3 tile[];
+  const int i0 = blockIdx.y * kDiffTY, j0 = blockIdx.x * kDiffTX;
+  const int ti = i0 + threadIdx.y, tj = j0 + threadIdx.x;
+  const bool in = ti < N && tj < M;
+  const int TW = kDiffTX + 2 * H;
+  const int base = (threadIdx.y + H) * TW + threadIdx.x + H;
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  load_coef_tile(coef, M, N, i0, j0, H, tile);
+  __syncthreads();
+  if (in) diff_gather_range(tile, base, TW, 0, nsplit, nzoff, nzval, ax, ay, az);
+  __syncthreads();
+  load_coef_tile(coef_post, M, N, i0, j0, H, tile);
+  __syncthreads();
+  if (!in) return;
+  diff_gather_range(tile, base, TW, nsplit, nnz, nzoff, nzval, ax, ay, az);
   const size_t t = (size_t)ti * M + tj;
   out[3 * t] = light[3 * t] + ax;
   out[3 * t + 1] = light[3 * t + 1] + ay;
@@ -717,7 +762,9 @@ constexpr int kDiffTYS = 32;
 // angle, as lensing uses), s clamped to [0.25, 4] and rounded to the nearest
 // level s_k (9% steps): the term from offset o is the sprite sampled
 // bilinearly at (centre + o / s_k) divided by s_k^2 -- a scale keeps the
-// sprite's total light -- read from the level's precomputed entries.
+// sprite's total light -- read from the level's precomputed entries.  The
+// reference has no scaled footprint; every term of this one uses the
+// source's light before any term is added (the coefficients of pass 1).
 __global__ void __launch_bounds__(kDiffTX * kDiffTYS)
 k_diff_gather_scaled(const float3* __restrict__ coef, const float* __restrict__ light,
                      float* __restrict__ out, int M, int N, const short2* __restrict__ lvoff,
@@ -859,21 +906,93 @@ int map_star_census(const MapScratch& Sc, const MapFrame& F, unsigned long long*
   return BT_OK;
 }
 
+// The star cells of a splat of width fw: N*M*fw^2 float3, and at least two
+// per pixel (the diffraction coefficients reuse them).
+static int ensure_cells(MapScratch& Sc, int fw) {
+  const size_t np = (size_t)Sc.M * Sc.N;
+  if (Sc.cells && Sc.cells_fw >= fw) return BT_OK;
+  if (Sc.cells) cudaFree(Sc.cells);
+  Sc.cells = nullptr;
+  Sc.cells_fw = 0;
+  cudaError_t e = cudaMalloc((void**)&Sc.cells, np * imax(fw * fw, 2) * sizeof(float3));
+  if (e != cudaSuccess) {
+    set_error("star cell scratch allocation failed: %s", cudaGetErrorString(e));
+    return BT_ERR_NOMEM;
+  }
+  Sc.cells_fw = fw;
+  return BT_OK;
+}
+
+// addDiffraction (BT/MakeImageKernel.cu:775-800) of a star-light buffer
+// (N*M*3 floats) into out (not the same buffer); the coefficients go into the
+// star cells.  psf_scale: footprint scaled by the receiving pixel's
+// magnification, from view and the smoothed solid angles `area`.
+int map_diffract(MapScratch& Sc, const StarSet& SS, const float* light, float* out,
+                 int psf_scale, const float2* view, const float* area, cudaStream_t s) {
+  const int M = Sc.M, N = Sc.N;
+  const size_t np = (size_t)M * N;
+  if (int rc = ensure_cells(Sc, 1)) return rc;
+  float3* coef = Sc.cells;
+  float3* coef_post = Sc.cells + np;
+  k_diff_coef<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(light, (int)np, SS.psf_centre, coef,
+                                                           coef_post);
+  const dim3 dgrid((unsigned)((M + kDiffTX - 1) / kDiffTX), (unsigned)((N + kDiffTY - 1) / kDiffTY));
+  const dim3 dblock(kDiffTX, kDiffTY);
+  constexpr int kMaxHalo = 52;  // (8 + 104) x (32 + 104) float3 = 183 KB of shared memory
+  auto tile_bytes = [](int H, int ty = kDiffTY) {
+    return (size_t)(kDiffTX + 2 * H) * (ty + 2 * H) * sizeof(float3);
+  };
+  if (psf_scale && SS.psf_lvstart) {
+    // the highest level whose footprint fits the shared-memory halo
+    int maxlevel = kPsfLevels - 1;
+    while (maxlevel > 0 &&
+           (int)ceilf(imax(1, SS.psf_rnz) * 0.25f * exp2f(maxlevel / 8.f)) + 1 > kMaxHalo)
+      maxlevel--;
+    const int H = imin(kMaxHalo, (int)ceilf(imax(1, SS.psf_rnz) * 0.25f * exp2f(maxlevel / 8.f)) + 1);
+    BT_CUDA_TRY(cudaFuncSetAttribute(k_diff_gather_scaled,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tile_bytes(H, kDiffTYS)));
+    const dim3 sgrid((unsigned)((M + kDiffTX - 1) / kDiffTX),
+                     (unsigned)((N + kDiffTYS - 1) / kDiffTYS));
+    k_diff_gather_scaled<<<sgrid, dim3(kDiffTX, kDiffTYS), tile_bytes(H, kDiffTYS), s>>>(
+        coef, light, out, M, N, SS.psf_lvoff, SS.psf_lvval, SS.psf_lvstart, maxlevel, H, view,
+        area);
+  } else if (SS.psf_rnz <= kMaxHalo) {
+    const int H = imax(1, SS.psf_rnz);
+    BT_CUDA_TRY(cudaFuncSetAttribute(k_diff_gather, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)tile_bytes(kMaxHalo)));
+    k_diff_gather<<<dgrid, dblock, tile_bytes(H), s>>>(coef, coef_post, light, out, M, N,
+                                                       SS.psf_nzoff, SS.psf_nzval, SS.psf_nsplit,
+                                                       SS.psf_nnz, H);
+  } else {
+    // sprites wider than the shared-memory halo: scatter with atomics
+    BT_CUDA_TRY(cudaMemcpyAsync(out, light, np * 3 * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    BT_CUDA_TRY(cudaMemsetAsync(Sc.diff_count, 0, sizeof(uint32_t), s));
+    k_diff_mark<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(light, (int)np, Sc.diff_list,
+                                                            Sc.diff_count);
+    k_diff_scatter<<<sm_count() * 8, 256, 0, s>>>(light, out, Sc.diff_list, Sc.diff_count, M, N,
+                                                  SS.psf, SS.psf_size);
+  }
+  BT_CUDA_TRY(cudaGetLastError());
+  return BT_OK;
+}
+
+int map_diffract_light(MapScratch& Sc, const bt_stars* stars, const float* light, float* out,
+                       cudaStream_t s) {
+  const StarSet& SS = stars->s;
+  if (!SS.psf || SS.psf_size <= 0) {
+    set_error("invalid argument: the star set has no diffraction sprite");
+    return BT_ERR_ARG;
+  }
+  return map_diffract(Sc, SS, light, out, 0, nullptr, nullptr, s);
+}
+
 int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   const int M = Sc.M, N = Sc.N;
   const StarSet SS = stars_for_frame(F.stars, F.bb_table);
   const int fw = 2 * F.step + 1;
   const size_t np = (size_t)M * N;
-  if (!Sc.cells || Sc.cells_fw < fw) {
-    if (Sc.cells) cudaFree(Sc.cells);
-    Sc.cells = nullptr;
-    cudaError_t e = cudaMalloc((void**)&Sc.cells, np * fw * fw * sizeof(float3));
-    if (e != cudaSuccess) {
-      set_error("star cell scratch allocation failed: %s", cudaGetErrorString(e));
-      return BT_ERR_NOMEM;
-    }
-    Sc.cells_fw = fw;
-  }
+  if (int rc = ensure_cells(Sc, fw)) return rc;
   if (F.step > 2) {
     set_error("star splat step > 2 is not supported");
     return BT_ERR_ARG;
@@ -906,45 +1025,8 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   k_star_gather<false><<<grid2(M, N), dim3(TX, TY), 0, s>>>(
       Sc.cells, Sc.flag, M, N, F.step, Sc.light, nullptr, nullptr, F.map, trail);
   // the star cells are consumed: their buffer holds the coefficients
-  float3* coef = Sc.cells;
-  k_diff_coef<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(Sc.light, (int)np, coef);
-  const dim3 dgrid((unsigned)((M + kDiffTX - 1) / kDiffTX), (unsigned)((N + kDiffTY - 1) / kDiffTY));
-  const dim3 dblock(kDiffTX, kDiffTY);
-  constexpr int kMaxHalo = 52;  // (8 + 104) x (32 + 104) float3 = 183 KB of shared memory
-  auto tile_bytes = [](int H, int ty = kDiffTY) {
-    return (size_t)(kDiffTX + 2 * H) * (ty + 2 * H) * sizeof(float3);
-  };
-  if (F.psf_scale && SS.psf_lvstart) {
-    // the highest level whose footprint fits the shared-memory halo
-    int maxlevel = kPsfLevels - 1;
-    while (maxlevel > 0 &&
-           (int)ceilf(imax(1, SS.psf_rnz) * 0.25f * exp2f(maxlevel / 8.f)) + 1 > kMaxHalo)
-      maxlevel--;
-    const int H = imin(kMaxHalo, (int)ceilf(imax(1, SS.psf_rnz) * 0.25f * exp2f(maxlevel / 8.f)) + 1);
-    BT_CUDA_TRY(cudaFuncSetAttribute(k_diff_gather_scaled,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tile_bytes(H, kDiffTYS)));
-    const dim3 sgrid((unsigned)((M + kDiffTX - 1) / kDiffTX),
-                     (unsigned)((N + kDiffTYS - 1) / kDiffTYS));
-    k_diff_gather_scaled<<<sgrid, dim3(kDiffTX, kDiffTYS), tile_bytes(H, kDiffTYS), s>>>(
-        coef, Sc.light, Sc.light2, M, N, SS.psf_lvoff, SS.psf_lvval, SS.psf_lvstart, maxlevel,
-        H, F.view, Sc.area);
-  } else if (SS.psf_rnz <= kMaxHalo) {
-    const int H = imax(1, SS.psf_rnz);
-    BT_CUDA_TRY(cudaFuncSetAttribute(k_diff_gather, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tile_bytes(kMaxHalo)));
-    k_diff_gather<<<dgrid, dblock, tile_bytes(H), s>>>(coef, Sc.light, Sc.light2, M, N,
-                                                       SS.psf_nzoff, SS.psf_nzval, SS.psf_nnz, H);
-  } else {
-    // sprites wider than the shared-memory halo: scatter with atomics
-    BT_CUDA_TRY(cudaMemcpyAsync(Sc.light2, Sc.light, np * 3 * sizeof(float),
-                                cudaMemcpyDeviceToDevice, s));
-    BT_CUDA_TRY(cudaMemsetAsync(Sc.diff_count, 0, sizeof(uint32_t), s));
-    k_diff_mark<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(Sc.light, (int)np, Sc.diff_list,
-                                                            Sc.diff_count);
-    k_diff_scatter<<<sm_count() * 8, 256, 0, s>>>(Sc.light, Sc.light2, Sc.diff_list,
-                                                  Sc.diff_count, M, N, SS.psf, SS.psf_size);
-  }
+  if (int rc = map_diffract(Sc, SS, Sc.light, Sc.light2, F.psf_scale, F.view, Sc.area, s))
+    return rc;
   if (F.bg_ready) BT_CUDA_TRY(cudaStreamWaitEvent(s, F.bg_ready, 0));
   k_makepix<<<grid2(M, N), dim3(TX, TY), 0, s>>>(Sc.light2, M, N,
                                                  (const uchar4*)F.out_bg,
@@ -1041,11 +1123,99 @@ bool node_boxes(const float* pos, int n, const int* tree, int L,
   return true;
 }
 
+// The sprite resampled at the footprint scales s_k = 0.25 * 2^(k/8),
+// k = 0..kPsfLevels-1 (StarSet::psf_lvoff): level k lists the offsets
+// (dq, dp) within R_k = ceil(max(1, rnz) s_k) + 1 of the centre whose
+// bilinear sample of the sprite at (centre + offset / s_k), divided by s_k^2,
+// is non-zero in some channel; level k is [lvstart[k], lvstart[k + 1]).
+void psf_levels(const uint8_t* psf_rgb, int psf_size, int rnz, std::vector<short2>& lvoff,
+                std::vector<float4>& lvval, std::vector<int>& lvstart) {
+  lvoff.clear();
+  lvval.clear();
+  lvstart.assign(1, 0);
+  if (psf_size < 2) return;
+  const float c0 = (float)(psf_size / 2);
+  auto px = [&](int q, int p, int ch) {
+    return (float)psf_rgb[((size_t)q * psf_size + p) * 3 + ch];
+  };
+  for (int k = 0; k < kPsfLevels; k++) {
+    const float sc = 0.25f * std::exp2((float)k / 8.f), is = 1.f / sc;
+    const int R = (int)std::ceil(std::max(1, rnz) * sc) + 1;
+    for (int dq = -R; dq <= R; dq++)
+      for (int dp = -R; dp <= R; dp++) {
+        const float u = c0 + dq * is, v = c0 + dp * is;
+        if (u < 0.f || v < 0.f || u > psf_size - 1 || v > psf_size - 1) continue;
+        const int u0 = std::min((int)u, psf_size - 2), v0 = std::min((int)v, psf_size - 2);
+        const float fu = u - u0, fv = v - v0;
+        float val[3];
+        for (int ch = 0; ch < 3; ch++)
+          val[ch] = ((1 - fu) * (1 - fv) * px(u0, v0, ch) + (1 - fu) * fv * px(u0, v0 + 1, ch) +
+                     fu * (1 - fv) * px(u0 + 1, v0, ch) + fu * fv * px(u0 + 1, v0 + 1, ch)) *
+                    is * is;
+        if (val[0] == 0.f && val[1] == 0.f && val[2] == 0.f) continue;
+        lvoff.push_back(make_short2((short)dq, (short)dp));
+        lvval.push_back(make_float4(val[0], val[1], val[2], 0.f));
+      }
+    lvstart.push_back((int)lvoff.size());
+  }
+}
+
 }  // namespace
 
 extern "C" {
 
 int bt_stars_tree_size(int treeLevel) { return (1 << (treeLevel + 1)) - 1; }
+
+int bt_psf_levels(const uint8_t* psf_rgb, int psf_size, int level, int16_t* offsets,
+                  float* values, int capacity, int* count) {
+  clear_error();
+  BT_ARG_CHECK(psf_rgb && count && psf_size >= 2, "invalid sprite");
+  BT_ARG_CHECK(level >= 0 && level < kPsfLevels, "level must be in [0, 32]");
+  int rnz = 0;
+  for (int q = 0; q < psf_size; q++)
+    for (int p = 0; p < psf_size; p++) {
+      const uint8_t* v = psf_rgb + ((size_t)q * psf_size + p) * 3;
+      if (v[0] || v[1] || v[2])
+        rnz = std::max(rnz, std::max(std::abs(q - psf_size / 2), std::abs(p - psf_size / 2)));
+    }
+  std::vector<short2> off;
+  std::vector<float4> val;
+  std::vector<int> start;
+  psf_levels(psf_rgb, psf_size, rnz, off, val, start);
+  const int n = start[level + 1] - start[level];
+  *count = n;
+  if (!offsets || !values || capacity < n) return BT_OK;
+  for (int e = 0; e < n; e++) {
+    const short2 o = off[start[level] + e];
+    const float4 v = val[start[level] + e];
+    offsets[2 * e] = o.x;
+    offsets[2 * e + 1] = o.y;
+    values[3 * e] = v.x;
+    values[3 * e + 1] = v.y;
+    values[3 * e + 2] = v.z;
+  }
+  return BT_OK;
+}
+
+int bt_stars_blackbody(const bt_stars* st, int table, float* hsp, float* rgb, int capacity,
+                       int* count, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(st && count, "NULL pointer");
+  BT_ARG_CHECK(table == 0 || table == 1, "table must be 0 (391 entries) or 1 (1024)");
+  const int n = table ? kBlackbody1k : kBlackbodyEntries;
+  *count = n;
+  if (!hsp || !rgb || capacity < n) return BT_OK;
+  const float4* dev = table ? st->bb1k : st->bb;
+  std::vector<float4> h(2 * (size_t)n);
+  cudaStream_t s = (cudaStream_t)stream;
+  BT_CUDA_TRY(cudaMemcpyAsync(h.data(), dev, 2 * n * sizeof(float4), cudaMemcpyDeviceToHost, s));
+  BT_CUDA_TRY(cudaStreamSynchronize(s));
+  for (int k = 0; k < n; k++) {
+    hsp[3 * k] = h[k].x; hsp[3 * k + 1] = h[k].y; hsp[3 * k + 2] = h[k].z;
+    rgb[3 * k] = h[n + k].x; rgb[3 * k + 1] = h[n + k].y; rgb[3 * k + 2] = h[n + k].z;
+  }
+  return BT_OK;
+}
 
 int bt_psf_airy(int size, float first_zero, uint8_t* rgb) {
   clear_error();
@@ -1128,46 +1298,24 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   // the sprite's non-zero entries, offsets from its centre (index size/2)
   std::vector<short2> nzoff;
   std::vector<float4> nzval;
-  int rnz = 0;
+  int rnz = 0, nsplit = 0;
+  float4 centre = make_float4(0.f, 0.f, 0.f, 0.f);
   for (int q = 0; q < psf_size; q++)
     for (int p = 0; p < psf_size; p++) {
       const uint8_t* v = psf_rgb + ((size_t)q * psf_size + p) * 3;
-      if (!v[0] && !v[1] && !v[2]) continue;
       const int dq = q - psf_size / 2, dp = p - psf_size / 2;
+      if (dq == 0 && dp == 0) centre = make_float4((float)v[0], (float)v[1], (float)v[2], 0.f);
+      if (!v[0] && !v[1] && !v[2]) continue;
       nzoff.push_back(make_short2((short)dq, (short)dp));
       nzval.push_back(make_float4((float)v[0], (float)v[1], (float)v[2], 0.f));
+      if (dq < 0 || (dq == 0 && dp <= 0)) nsplit = (int)nzoff.size();
       rnz = std::max(rnz, std::max(std::abs(dq), std::abs(dp)));
     }
   // resampled levels for the magnification-scaled footprint
   std::vector<short2> lvoff;
   std::vector<float4> lvval;
   std::vector<int> lvstart(1, 0);
-  if (psf_size >= 2) {
-    const float c0 = (float)(psf_size / 2);
-    auto px = [&](int q, int p, int ch) {
-      return (float)psf_rgb[((size_t)q * psf_size + p) * 3 + ch];
-    };
-    for (int k = 0; k < kPsfLevels; k++) {
-      const float sc = 0.25f * std::exp2((float)k / 8.f), is = 1.f / sc;
-      const int R = (int)std::ceil(std::max(1, rnz) * sc) + 1;
-      for (int dq = -R; dq <= R; dq++)
-        for (int dp = -R; dp <= R; dp++) {
-          const float u = c0 + dq * is, v = c0 + dp * is;
-          if (u < 0.f || v < 0.f || u > psf_size - 1 || v > psf_size - 1) continue;
-          const int u0 = std::min((int)u, psf_size - 2), v0 = std::min((int)v, psf_size - 2);
-          const float fu = u - u0, fv = v - v0;
-          float val[3];
-          for (int ch = 0; ch < 3; ch++)
-            val[ch] = ((1 - fu) * (1 - fv) * px(u0, v0, ch) + (1 - fu) * fv * px(u0, v0 + 1, ch) +
-                       fu * (1 - fv) * px(u0 + 1, v0, ch) + fu * fv * px(u0 + 1, v0 + 1, ch)) *
-                      is * is;
-          if (val[0] == 0.f && val[1] == 0.f && val[2] == 0.f) continue;
-          lvoff.push_back(make_short2((short)dq, (short)dp));
-          lvval.push_back(make_float4(val[0], val[1], val[2], 0.f));
-        }
-      lvstart.push_back((int)lvoff.size());
-    }
-  }
+  psf_levels(psf_rgb, psf_size, rnz, lvoff, lvval, lvstart);
   if (e == cudaSuccess && psf_size)
     e = cudaMalloc((void**)&st->psf, (size_t)psf_size * psf_size * 3);
   if (e == cudaSuccess && !lvoff.empty()) {
@@ -1233,6 +1381,8 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
   st->s.psf_nzval = st->psf_nzval;
   st->s.psf_nnz = (int)nzoff.size();
   st->s.psf_rnz = rnz;
+  st->s.psf_nsplit = nsplit;
+  st->s.psf_centre = centre;
   st->s.psf_lvoff = st->psf_lvoff;
   st->s.psf_lvval = st->psf_lvval;
   st->s.psf_lvstart = st->psf_lvstart;

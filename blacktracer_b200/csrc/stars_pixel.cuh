@@ -26,6 +26,10 @@ struct StarSet {
   const short2* psf_nzoff;
   const float4* psf_nzval;
   int psf_nnz, psf_rnz;
+  // Entries [0, psf_nsplit) lie at or before the centre in row-major order;
+  // psf_centre = the sprite's value at its centre (index size/2, size/2).
+  int psf_nsplit;
+  float4 psf_centre;
   // The sprite resampled at footprint scales s_k = 0.25 * 2^(k/8), k = 0..32:
   // entry values = bilinear sample at (centre + offset / s_k) / s_k^2, non-zero
   // entries only, level k at [lvl_start[k], lvl_start[k + 1]).

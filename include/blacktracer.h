@@ -332,6 +332,16 @@ int bt_stars_create(const float* star_pos, const float* star_mag, int n,
                     int psf_size, bt_stars** out, void* stream);
 void bt_stars_destroy(bt_stars* s);
 
+/* The blackbody colour tables of a star set, copied to HOST arrays of
+ * 3 * count floats: per entry its RGBtoHSP (h, s, p) and 255 * HSPtoRGB of
+ * that.  table 0: the reference's 391 entries (BT/Const.h:7, 1000-40000 K in
+ * 100 K steps); table 1: the 1024-entry FP32 table (bt_frame.bb_table = 1;
+ * no counterpart in the reference), entry k the linear interpolation of the
+ * reference's entries at k * 390 / 1023.  *count = entries; nothing is
+ * copied when capacity is smaller (or arrays NULL).  Synchronises stream. */
+int bt_stars_blackbody(const bt_stars* s, int table, float* hsp, float* rgb, int capacity,
+                       int* count, void* stream);
+
 /* A renderer: per-resolution device scratch (the reference's dev_in,
  * dev_gap, dev_bh, dev_area, star buffers), created once per output size. */
 typedef struct bt_map bt_map;
@@ -429,6 +439,30 @@ int bt_trails_query(bt_trails* t, bt_trails_info* info, void* stream);
  * 550 nm, scaled per channel by wavelength (R 610, G 550, B 465 nm), 255 at
  * the centre.  For bt_stars_create's psf_rgb. */
 int bt_psf_airy(int size, float first_zero, uint8_t* rgb);
+
+/* HOST only.  The sprite resampled for the magnification-scaled footprint
+ * (bt_frame.psf_scale; no counterpart in the reference, whose sprite has one
+ * size): level k in [0, 32] is the scale s_k = 0.25 * 2^(k/8), its entries the
+ * offsets (row, column) from the centre within ceil(max(1, r) s_k) + 1 (r =
+ * the largest offset of a non-zero sprite entry) whose bilinear sample of
+ * the sprite at centre + offset / s_k, divided by s_k^2, is non-zero: 2 int16
+ * offsets and 3 float values per entry, row-major.  *count = the level's
+ * entries; nothing is written when capacity is smaller (or arrays NULL). */
+int bt_psf_levels(const uint8_t* psf_rgb, int psf_size, int level, int16_t* offsets,
+                  float* values, int capacity, int* count);
+
+/* addDiffraction (BT/MakeImageKernel.cu:775-800) on a caller's star-light
+ * buffer: light and out are DEVICE arrays of width*height*3 floats (the
+ * renderer's size; the summed star light sumStarLight produces), different
+ * buffers; the sprite is the star set's psf.  A pixel whose brightest
+ * channel exceeds 65025 adds min(65025, (light / (10000 max^0.6) * sprite)^2)
+ * per channel around itself, rows clipped at the image's edges, columns
+ * wrapped.  As the reference's thread reads its own pixel for every sprite
+ * entry, the entries after the centre (row-major) see the centre's term
+ * added to it; terms of other bright pixels are not seen (in the reference
+ * that depends on thread timing).  Deterministic; uses m's scratch. */
+int bt_map_diffract(bt_map* m, const bt_stars* stars, const float* light, float* out,
+                    void* stream);
 /* Renders one frame on `stream`.  A frame that draws both the environment and
  * stars draws the environment on a second stream owned by `m` (created at the
  * priority of `stream`) while the star passes run on `stream`; `stream` waits

@@ -500,6 +500,90 @@ def ref_trail_frames(f0, f1, stars, width, height, step, view, lr, trailnum=30):
     return trail.reshape(-1, 3), light.reshape(-1, 3)
 
 
+def ref_map_diffraction(light, width, height, sprite):
+    """The reference's addDiffraction run pixel by pixel in row-major order on
+    a copy of `light` ((height*width*3,) float32 summed star light) with an
+    (fs, fs, 3) uint8 sprite; returns the diffracted light (height*width*3,).
+    The extra row the kernel can write past the image is dropped."""
+    lib = _refmaplib()
+    lib.btref_map_diffraction.argtypes = [_f32p, C.c_int, C.c_int, _u8p, C.c_int]
+    M, N = width, height
+    buf = np.zeros((N + 1) * M * 3, np.float32)
+    buf[:N * M * 3] = np.asarray(light, np.float32).reshape(-1)
+    sp = np.ascontiguousarray(sprite, dtype=np.uint8)
+    lib.btref_map_diffraction(buf, M, N, sp, sp.shape[0])
+    return buf[:N * M * 3].copy()
+
+
+def ref_map_sat(bgr):
+    """The summed-area table of the reference's driver (cudaPrep,
+    BT/MakeImageKernel.cu:1312-1330) over a (rows, cols, 3) BGR8 image, as
+    (rows*cols*4,) float32 (host threads over columns)."""
+    lib = _refmaplib()
+    bgr = np.ascontiguousarray(bgr, dtype=np.uint8)
+    rows, cols = bgr.shape[:2]
+    sat = np.zeros(rows * cols * 4, np.float32)
+    lib.btref_map_sat(bgr, rows, cols, sat)
+    return sat
+
+
+def ref_map_frame_rows(grid_f2, grid_rows, grid_cols, gridlvl, view, width, height, cam7,
+                       rows, sat=None, env_shape=None, stars=None, step=1, lr=True,
+                       nthreads=0):
+    """One frame through the reference's own map kernels on host threads
+    (btref_map_frame_rows): corners, black-hole mask and smoothed solid angles
+    of the whole frame, and the environment, star and composite colours of the
+    listed rows.  sat = ref_map_sat(bgr) with env_shape = (rows, cols), or
+    None; stars = (pos, mag, tree, level) or None.  Returns dict(thphi, gap,
+    bh, area, env, stars, image) with the row images as (len(rows), W, 4)."""
+    lib = _refmaplib()
+    M, N = width, height
+    rows = np.ascontiguousarray(rows, dtype=np.int32)
+    nr = rows.size
+    pad = 2 * grid_rows + 8
+    g = np.full(((grid_rows + 2 * pad) * grid_cols, 2), -2.0, np.float32)
+    g[pad * grid_cols:(pad + grid_rows) * grid_cols] = np.asarray(grid_f2, np.float32).reshape(-1, 2)
+    if sat is not None:
+        er, ec = env_shape
+        sp = np.zeros((er + 4) * ec * 4, np.float32)
+        sp[2 * ec * 4:(er + 2) * ec * 4] = np.asarray(sat, np.float32).reshape(-1)
+        sat_ptr = C.c_void_p(sp.ctypes.data + 2 * ec * 16)
+    else:
+        er = ec = 0
+        sat_ptr = None
+    if stars is not None:
+        pos, mg, tree, tl = stars
+        pos = np.ascontiguousarray(pos, np.float32)
+        mg = np.ascontiguousarray(mg, np.float32)
+        tree = np.ascontiguousarray(tree, np.int32)
+        sptr = (pos.ctypes.data, tree.ctypes.data, len(pos) // 2, mg.ctypes.data, tl)
+    else:
+        sptr = (None, None, 0, None, 0)
+    thphi = np.zeros(((N + 1) * (M + 1), 2), np.float32)
+    gap = np.zeros((N + 1) * (M + 1), np.int32)
+    bh = np.zeros(N * M, np.uint8)
+    area = np.zeros(N * M, np.float32)
+    env = np.zeros((nr, M, 4), np.uint8) if sat is not None else None
+    simg = np.zeros((nr, M, 4), np.uint8) if stars is not None else None
+    img = np.zeros((nr, M, 4), np.uint8) if (sat is not None and stars is not None) else None
+    vp = C.c_void_p
+    lib.btref_map_frame_rows.argtypes = [
+        _f32p, C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int,
+        vp, vp, C.c_int, vp, C.c_int, _f32p, C.c_int, C.c_int, _i32, C.c_int, C.c_int,
+        _f32p, _i32, _u8p, _f32p, vp, vp, vp]
+    lib.btref_map_frame_rows.restype = C.c_int
+    ptr = lambda a: None if a is None else C.c_void_p(a.ctypes.data)  # noqa: E731
+    rc = lib.btref_map_frame_rows(
+        np.ascontiguousarray(view, np.float32), M, N,
+        C.c_void_p(g.ctypes.data + pad * grid_cols * 8), grid_cols, grid_rows, gridlvl,
+        sat_ptr, er, ec, sptr[0], sptr[1], sptr[2], sptr[3], sptr[4],
+        np.ascontiguousarray(cam7, np.float32), step, int(lr), rows, nr, nthreads,
+        thphi, gap, bh, area, ptr(env), ptr(simg), ptr(img))
+    if rc != 0:
+        raise RuntimeError("reference frame rows failed (scratch reservation)")
+    return dict(thphi=thphi, gap=gap, bh=bh, area=area, env=env, stars=simg, image=img)
+
+
 def ref_map_time(grid_f2, grid_rows, grid_cols, gridlvl, view, width, height, cam7, sat,
                  env_rows, env_cols, stars, step=1, lr=True, row_stride=16, nthreads=0):
     """The reference's per-pixel map kernels timed on host threads

@@ -187,6 +187,8 @@ void btref_map_smooth(float* area, float* areaSmooth, const unsigned char* bh,
 // image (cv::imread's channel order), rows x cols; out: rows*cols float4.
 void btref_map_sat(const unsigned char* bgr, int rows, int cols, float* out) {
   float pxsz = PI2 / (1.f * cols);
+  // columns are independent (each is summed down its rows)
+#pragma omp parallel for schedule(static)
   for (int q = 0; q < cols; q++) {
     float prev[4] = {0.f, 0.f, 0.f, 0.f};
     float phi[4] = {pxsz * q, pxsz * q, pxsz * (q + 1), pxsz * (q + 1)};
@@ -256,6 +258,21 @@ void btref_map_stars(const float* thphi, const unsigned char* bh,
     for (int j = 0; j < M; j++) {
       at(i, j);
       makePix((float3*)light, (uchar4*)out, M, N, nullptr);
+    }
+}
+
+// addDiffraction (BT/MakeImageKernel.cu:775-800) for every pixel, one after
+// the other in row-major order, on the summed star light (N*M float3, with
+// one more row after it: the kernel's row bound lets the pixel at row
+// N - filtersize/2 write one row past the image).  The sprite is
+// filtersize^2 RGB8.  Run sequentially, a pixel sees every term added before
+// it, including its own sprite centre's.
+void btref_map_diffraction(float* light, int M, int N, const unsigned char* sprite,
+                           int filtersize) {
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      addDiffraction((float3*)light, M, N, (const uchar3*)sprite, filtersize);
     }
 }
 
@@ -360,6 +377,139 @@ int btref_map_time(const float* view, int M, int N, const float* grid, int GM, i
     }
   secs[3] = secs_since(t);
   return nr;
+}
+
+// One frame of the reference's map kernels on host threads, with the colour
+// passes restricted to the listed rows (all rows, or a sample of a frame too
+// large to run whole).  pixInterpolation over every corner, findBlackPixels,
+// findArea and smoothAreaH/V over every pixel (thphi, gap, bh and the
+// smoothed area are returned whole); then for each listed row
+// distortEnvironmentMap, and distortStarMap over the rows within `step` of a
+// listed row followed by sumStarLight, makePix and addStarsAndBackground on
+// the listed rows.  env_rows / star_rows / img_rows: nr x M BGRA8 (any may be
+// NULL; img_rows needs both passes).  sat and grid are padded as for
+// btref_map_time.  Rows of the star pass run in chunks; chunks next to each
+// other never run at the same time, so searchTree's writes past a pixel's
+// slots (into the next pixel's) land where only the same thread reads.
+// Returns 0, or -1 if scratch memory could not be reserved.
+int btref_map_frame_rows(const float* view, int M, int N, const float* grid, int GM, int GN1,
+                         int gridlvl, const float* sat, int env_rows, int env_cols,
+                         const float* stars, const int* tree, int starSize, const float* mag,
+                         int treeLevel, const float* cam7, int step, int lr,
+                         const int* rows, int nr, int nthreads, float* thphi_out,
+                         int* gap_out, unsigned char* bh_out, float* area_out,
+                         unsigned char* env_rows_out, unsigned char* star_rows_out,
+                         unsigned char* img_rows_out) {
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  float2* thphi = (float2*)thphi_out;
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i <= N; i++) {
+    float2 border[4] = {};
+    for (int j = 0; j <= M; j++) {
+      at(i, j);
+      pixInterpolation((const float2*)view, M, N, 1, thphi, (const float2*)grid, GM, GN1, 0.f,
+                       0.f, gap_out, gridlvl, border, 1000, 0.f);
+    }
+  }
+  std::vector<float> areaS((size_t)N * M);
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      findBlackPixels(thphi, M, N, bh_out);
+      findArea(thphi, M, N, area_out);
+    }
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      smoothAreaH(areaS.data(), area_out, bh_out, gap_out, M, N);
+    }
+#pragma omp parallel for schedule(dynamic, 2)
+  for (int i = 0; i < N; i++)
+    for (int j = 0; j < M; j++) {
+      at(i, j);
+      smoothAreaV(areaS.data(), area_out, bh_out, gap_out, M, N);
+    }
+  // distortEnvironmentMap writes out[ij]: a full-frame buffer reserved lazily
+  Lazy<uchar4> env_img((size_t)N * M);
+  if (!env_img.p) return -1;
+  if (env_rows_out || img_rows_out) {
+    int2 imsize = {env_rows, env_cols};
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int r = 0; r < nr; r++)
+      for (int j = 0; j < M; j++) {
+        at(rows[r], j);
+        distortEnvironmentMap(thphi, env_img.p, bh_out, imsize, M, N, 0.f, (float4*)sat,
+                              cam7, 0, nullptr, area_out, (float2*)view, lr != 0);
+      }
+    if (env_rows_out)
+      for (int r = 0; r < nr; r++)
+        memcpy(env_rows_out + (size_t)r * M * 4, env_img.p + (size_t)rows[r] * M, (size_t)M * 4);
+  }
+  if (star_rows_out || img_rows_out) {
+    const int filterW = 2 * step + 1;
+    const int searchNr = (int)powf(2, treeLevel / 3 * 2);
+    const int trailnum = 30;
+    Lazy<float3> scratch((size_t)N * M * filterW * filterW);
+    Lazy<int> search((size_t)N * M * searchNr + (size_t)4096 * searchNr);
+    Lazy<int2> stCache((size_t)2 * starSize * trailnum);
+    Lazy<int> stnums((size_t)starSize);
+    Lazy<float3> trail((size_t)N * M);
+    Lazy<float2> grad((size_t)(N + 1) * (M + 1));
+    Lazy<float3> light((size_t)N * M);
+    Lazy<uchar4> simg((size_t)N * M);
+    Lazy<uchar4> comp((size_t)N * M);
+    if (!scratch.p || !search.p || !stCache.p || !stnums.p || !trail.p || !grad.p || !light.p ||
+        !simg.p || !comp.p)
+      return -1;
+    for (size_t q = 0; q < (size_t)2 * starSize * trailnum; q++) stCache.p[q] = int2{-1, -1};
+    // rows the star pass needs, as runs of consecutive rows cut into chunks
+    std::vector<char> need(N, 0);
+    for (int r = 0; r < nr; r++)
+      for (int u = -step; u <= step; u++)
+        if (rows[r] + u >= 0 && rows[r] + u < N) need[rows[r] + u] = 1;
+    constexpr int kChunk = 4;
+    std::vector<std::pair<int, int>> chunks[2];  // [first, last) by parity in their run
+    for (int i = 0; i < N;) {
+      if (!need[i]) { i++; continue; }
+      int k = 0;
+      while (i < N && need[i]) {
+        int e = i;
+        while (e < N && need[e] && e - i < kChunk) e++;
+        chunks[k & 1].push_back({i, e});
+        k++;
+        i = e;
+      }
+    }
+    for (int ph = 0; ph < 2; ph++) {
+      const auto& C = chunks[ph];
+#pragma omp parallel for schedule(dynamic, 1)
+      for (int c = 0; c < (int)C.size(); c++)
+        for (int i = C[c].first; i < C[c].second; i++)
+          for (int j = 0; j < M; j++) {
+            at(i, j);
+            distortStarMap(scratch.p, thphi, bh_out, stars, tree, starSize, cam7, mag, treeLevel,
+                           M, N, step, 0.f, search.p, searchNr, stCache.p, stnums.p, trail.p,
+                           trailnum, grad.p, 0, (const float2*)view, lr != 0, area_out);
+          }
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int r = 0; r < nr; r++)
+      for (int j = 0; j < M; j++) {
+        at(rows[r], j);
+        sumStarLight(scratch.p, trail.p, light.p, step, M, N, filterW);
+        makePix(light.p, simg.p, M, N, nullptr);
+        if (img_rows_out) addStarsAndBackground(simg.p, env_img.p, comp.p, M);
+      }
+    for (int r = 0; r < nr; r++) {
+      if (star_rows_out)
+        memcpy(star_rows_out + (size_t)r * M * 4, simg.p + (size_t)rows[r] * M, (size_t)M * 4);
+      if (img_rows_out)
+        memcpy(img_rows_out + (size_t)r * M * 4, comp.p + (size_t)rows[r] * M, (size_t)M * 4);
+    }
+  }
+  return 0;
 }
 
 // ---- trails (addTrails / makeGradField / clearArrays) ----
@@ -472,6 +622,12 @@ int btref_search_tree(const int* tree, const float* mn, const float* mx,
   searchTree(tree, mn, mx, treeLevel, buf.data(), 0, pos, 0);
   for (int k = 0; k < pos && k < cap; k++) nodes[k] = buf[k];
   return pos;
+}
+
+// The reference's blackbody table (tempToRGB, BT/kernel.cuh:45): 391 RGB
+// triplets, 1000-40000 K in 100 K steps.
+void btref_blackbody(int* out) {
+  for (int k = 0; k < 1173; k++) out[k] = (int)tempToRGB[k];
 }
 
 // The reference's device helpers, one call each (for unit checks).

@@ -35,20 +35,22 @@ def ang_err(t0, p0, t1, p1):
     return np.maximum(dt, dp)
 
 
-def value_noise_bgr(rows, cols, seed, cell=16, octaves=3):
+def value_noise_bgr(rows, cols, seed, cell=16, octaves=3, dtype=np.float64):
     """Seeded 2-D value noise in [0, 255] per channel, BGR8 (rows, cols, 3);
-    the synthetic environment map of the benchmark configurations."""
+    the synthetic environment map of the benchmark configurations (dtype:
+    the arithmetic of the interpolation; float32 for the largest maps)."""
     rng = np.random.default_rng(seed)
-    img = np.zeros((rows, cols, 3), np.float64)
+    img = np.zeros((rows, cols, 3), dtype)
     amp, tot = 1.0, 0.0
     for o in range(octaves):
         c = max(2, cell >> o)
         gr, gc = rows // c + 2, cols // c + 2
-        lat = rng.uniform(0, 1, (gr, gc, 3))
+        lat = rng.uniform(0, 1, (gr, gc, 3)).astype(dtype)
         y = np.arange(rows) / c
         x = np.arange(cols) / c
         y0, x0 = np.floor(y).astype(int), np.floor(x).astype(int)
-        fy, fx = (y - y0)[:, None, None], (x - x0)[None, :, None]
+        fy = (y - y0)[:, None, None].astype(dtype)
+        fx = (x - x0)[None, :, None].astype(dtype)
         fy, fx = fy * fy * (3 - 2 * fy), fx * fx * (3 - 2 * fx)
         a = lat[y0][:, x0]
         b = lat[y0][:, x0 + 1]

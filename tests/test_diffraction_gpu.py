@@ -1,14 +1,26 @@
 """Diffraction and the frame extensions of the largest configuration.
 
-* The diffraction scatter (addDiffraction, BT/MakeImageKernel.cu:775-800) is
-  checked against a numpy restatement with snapshot reads (every pixel's
-  source light is read before any add; the reference's kernel reads while
-  others add, a data race): same bright-pixel threshold, amplitude, clamp,
-  edge rows and column wrap.  Sums of atomics differ in order only:
-  rtol 1e-5.
+* addDiffraction (BT/MakeImageKernel.cu:775-800) against the reference's own
+  kernel, run pixel by pixel on the host (oracle/_ref), on star light whose
+  bright pixels lie further apart than the sprite is wide: there every term
+  the reference adds is the same whatever order its threads run in, so the
+  result is defined, and it is compared at rtol 1e-5 (the device's powf and
+  summation order).  Both device forms: the shared-memory gather (sprite
+  radius <= 52) and the atomic scatter (wider sprites).
+* In frames, bright pixels within a sprite width of each other also take
+  terms of each other in the reference, which it reads or not depending on
+  thread timing; there the device result is compared with a numpy
+  restatement of its own rule (terms from each pixel's light before any term
+  is added, except its own centre term, which the entries after the centre
+  see), at rtol 1e-5.
 * The Airy sprite generator (host) -- no GPU needed.
-* The magnification-scaled footprint and the 1024-entry FP32 blackbody table
-  stay close to the reference behaviour they extend."""
+* The magnification-scaled footprint: its resampled sprite levels against a
+  numpy restatement of the bilinear resampling (host), and the scaled gather
+  in a frame against a restatement from the frame's own light and solid
+  angles.
+* The 1024-entry FP32 blackbody table against the linear interpolation of
+  the reference's table it is defined by, through the reference's RGBtoHSP /
+  HSPtoRGB."""
 import math
 
 import numpy as np
@@ -28,24 +40,85 @@ def test_airy_sprite(bt):
 
 
 def scatter_reference(light, M, N, psf):
-    """addDiffraction with snapshot reads, float32 (numpy restatement)."""
+    """The device's addDiffraction rule in numpy (float32): each bright
+    pixel's terms from its light before any term is added, the entries after
+    the sprite's centre from its light plus its own centre term."""
     fs = psf.shape[0]
     fh = fs // 2
     L = light.reshape(N, M, 3).astype(np.float32)
     acc = L.copy()
     mx = L.max(-1)
+    centre = psf[fh, fh].astype(np.float32)
     for i, j in zip(*np.nonzero(mx > np.float32(65025.0))):
         startx = fh - i if i < fh else 0
         endx = N - i + fh if i > N - fh else fs
         div = np.float32(10000.0) * np.float32(mx[i, j]) ** np.float32(0.6)
+        d0 = L[i, j] / div * centre
+        post = L[i, j] + np.minimum(np.float32(65025.0), d0 * d0)
         for q in range(startx, endx):
             ti = i - fh + q
             if ti >= N:  # the reference writes one row past the image at i = N - fh
                 continue
             cols = (j - fh + np.arange(fs) + M) % M
-            d = (L[i, j] / div)[None, :] * psf[q].astype(np.float32)
+            after = (q > fh) | ((q == fh) & (np.arange(fs) > fh))
+            src = np.where(after[:, None], post[None, :], L[i, j][None, :])
+            d = src / div * psf[q].astype(np.float32)
             acc[ti, cols] += np.minimum(np.float32(65025.0), d * d)
     return acc.reshape(-1)
+
+
+def isolated_light(W, H, fs, seed):
+    """Dim star light (< 1000) with bright pixels (brightest channel 1e5..1e9)
+    one per band of fs + 2 columns, at rows cycling through the top and bottom
+    edges (rows the sprite is clipped at, and the row N - fs/2 whose last
+    sprite row falls past the image) and the interior."""
+    rng = np.random.default_rng(seed)
+    L = rng.uniform(0, 1000, (H, W, 3)).astype(np.float32)
+    fh = fs // 2
+    rows = [0, 1, fh - 1, H // 2, H - fh, H - fh + 1, H - 1, H // 3]
+    band = fs + 2
+    nb = W // band
+    for c in range(nb):
+        i = rows[c % len(rows)]
+        j = c * band + int(rng.integers(0, band - fs + 1)) + fh
+        top = np.float32(10.0 ** rng.uniform(5, 9))
+        v = rng.uniform(0, 1, 3).astype(np.float32) * top
+        v[rng.integers(0, 3)] = top
+        L[i, j] = v
+    return L.reshape(-1), nb
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sprite", ["airy33", "random121"])
+def test_diffraction_vs_reference_kernel(bt, cuda, oracle_mod, sprite):
+    if not oracle_mod.have_ref_map():
+        pytest.skip("reference map harness not built")
+    import ctypes as C
+    if sprite == "airy33":
+        psf, W, H = bt.psf_airy(33, 4.0), 1024, 256
+    else:  # all entries non-zero, radius 60: the atomic scatter form
+        psf = np.random.default_rng(5).integers(1, 256, (121, 121, 3)).astype(np.uint8)
+        W, H = 2048, 512
+    light, nb = isolated_light(W, H, psf.shape[0], seed=11)
+    th, ph, mag, bv = synthetic_stars(10, seed=1)
+    sp = bt.StarProcessor(th, ph, mag, bv, treeLevel=2, psf=psf)
+    R = bt.Renderer(W, H)
+    dl = cuda.tensor(light, device="cuda")
+    out = cuda.empty_like(dl)
+    L = bt._lib
+    for _ in range(2):  # the second call reuses the renderer's scratch
+        L.check(L.lib().bt_map_diffract(R._h, sp._h, C.c_void_p(dl.data_ptr()),
+                                        C.c_void_p(out.data_ptr()), None))
+        got = out.cpu().numpy()
+        ref = oracle_mod.ref_map_diffraction(light, W, H, psf)
+        assert (light.reshape(-1, 3).max(-1) > 65025).sum() == nb
+        changed = int((ref != light).sum())
+        print(f"{sprite}: {nb} bright pixels, {changed} values changed by the reference")
+        assert changed > nb * psf.shape[0]
+        np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-3)
+    with pytest.raises(L.BtError):
+        L.check(L.lib().bt_map_diffract(R._h, sp._h, C.c_void_p(dl.data_ptr()),
+                                        C.c_void_p(dl.data_ptr()), None))
 
 
 @pytest.fixture(scope="module")
@@ -63,7 +136,7 @@ def frame_setup(bt, cuda):
 
 
 @pytest.mark.gpu
-def test_diffraction_matches_snapshot_restatement(bt, cuda, frame_setup):
+def test_diffraction_in_frame_matches_restatement(bt, cuda, frame_setup):
     cam, grid, W, H, sp, view, env, psf = frame_setup
     R = bt.Renderer(W, H)
     R.render(grid, view, cam, env=env, stars=sp, diffraction=True)
@@ -73,6 +146,14 @@ def test_diffraction_matches_snapshot_restatement(bt, cuda, frame_setup):
     assert (light.reshape(-1, 3).max(-1) > 65025).sum() > 10, "no saturated pixels"
     ref = scatter_reference(light, W, H, psf)
     np.testing.assert_allclose(got, ref, rtol=1e-5, atol=1e-2)
+    # the standalone entry point on the same light gives the frame's result
+    import ctypes as C
+    L = bt._lib
+    dl = sc["light"].clone()
+    out = cuda.empty_like(dl)
+    L.check(L.lib().bt_map_diffract(R._h, sp._h, C.c_void_p(dl.data_ptr()),
+                                    C.c_void_p(out.data_ptr()), None))
+    assert np.array_equal(out.cpu().numpy(), got)
 
 
 @pytest.mark.gpu
@@ -89,6 +170,184 @@ def test_scaled_diffraction(bt, cuda, frame_setup):
     assert (added >= 0).all(), (added.min(), np.argwhere(added < 0)[:5])
     assert added.sum() > 0
     assert not np.array_equal(a, b), "scaling the footprint changed nothing"
+
+
+def psf_levels(bt, psf, level):
+    import ctypes as C
+    L = bt._lib
+    n = C.c_int()
+    L.check(L.lib().bt_psf_levels(psf.ctypes.data, psf.shape[0], level, None, None, 0,
+                                  C.byref(n)))
+    off = np.empty((n.value, 2), np.int16)
+    val = np.empty((n.value, 3), np.float32)
+    L.check(L.lib().bt_psf_levels(psf.ctypes.data, psf.shape[0], level, off.ctypes.data,
+                                  val.ctypes.data, n.value, C.byref(n)))
+    return off, val
+
+
+def psf_levels_restated(psf, level):
+    """The scaled footprint's sprite at scale s = 0.25 * 2^(level/8): for every
+    offset within ceil(max(1, r) s) + 1 of the centre (r = the sprite's largest
+    non-zero offset), the bilinear sample at centre + offset / s, divided by
+    s^2, kept where non-zero (float32, row-major)."""
+    fs = psf.shape[0]
+    f32 = np.float32
+    nz = np.argwhere(psf.max(-1) > 0) - fs // 2
+    r = int(np.abs(nz).max()) if len(nz) else 0
+    sc = f32(0.25) * np.exp2(f32(level) / f32(8))
+    inv = f32(1) / sc
+    R = int(np.ceil(f32(max(1, r)) * sc)) + 1
+    c0 = f32(fs // 2)
+    px = psf.astype(np.float32)
+    off, val = [], []
+    for dq in range(-R, R + 1):
+        for dp in range(-R, R + 1):
+            u, v = c0 + f32(dq) * inv, c0 + f32(dp) * inv
+            if u < 0 or v < 0 or u > fs - 1 or v > fs - 1:
+                continue
+            u0, v0 = min(int(u), fs - 2), min(int(v), fs - 2)
+            fu, fv = u - f32(u0), v - f32(v0)
+            one = f32(1)
+            x = (((one - fu) * (one - fv) * px[u0, v0] + (one - fu) * fv * px[u0, v0 + 1] +
+                  fu * (one - fv) * px[u0 + 1, v0] + fu * fv * px[u0 + 1, v0 + 1]) * inv * inv)
+            if (x == 0).all():
+                continue
+            off.append((dq, dp))
+            val.append(x)
+    return np.array(off, np.int16).reshape(-1, 2), np.array(val, np.float32).reshape(-1, 3)
+
+
+@pytest.mark.parametrize("level", [0, 5, 16, 27, 32])
+def test_scaled_sprite_levels_vs_restatement(bt, level):
+    for name, psf in (("airy", bt.psf_airy(33, 4.0)),
+                      ("random", np.random.default_rng(9).integers(0, 256, (9, 9, 3))
+                       .astype(np.uint8))):
+        off, val = psf_levels(bt, psf, level)
+        roff, rval = psf_levels_restated(psf, level)
+        assert np.array_equal(off, roff)
+        np.testing.assert_allclose(val, rval, rtol=1e-6, atol=1e-6)
+        # a scale keeps the light of a sprite that fades out before its edge
+        # (samples stop at the outermost entries' centres)
+        if name == "airy" and level >= 8:
+            tot = psf.reshape(-1, 3).astype(np.float64).sum(0)
+            np.testing.assert_allclose(val.astype(np.float64).sum(0), tot, rtol=0.08)
+
+
+@pytest.mark.gpu
+def test_scaled_diffraction_vs_restatement(bt, cuda, oracle_mod, frame_setup):
+    """Receiving pixels near bright pixels: the scaled gather's result equals
+    light + the sum over the level's entries of min(65025, (coef(t - o) *
+    value)^2), the level from the pixel's magnification (its camera-sky
+    solid angle, by the reference's calcArea, over its smoothed celestial
+    one)."""
+    if not oracle_mod.have_ref_map():
+        pytest.skip("reference map harness not built")
+    import ctypes as C
+    cam, grid, W, H, sp, view, env, psf = frame_setup
+    R = bt.Renderer(W, H)
+    R.render(grid, view, cam, stars=sp, diffraction=True, psf_scale=True)
+    sc = {k: v.cpu().numpy() for k, v in R.scratch().items()}
+    light = sc["light"].reshape(H, W, 3)
+    got = sc["light_diffracted"].reshape(H, W, 3)
+    area = sc["area"].reshape(H, W)
+    vm = view.viewMatrix.cpu().numpy().reshape(H + 1, W + 1, 2)
+    mx = light.max(-1)
+    bright = np.argwhere(mx > np.float32(65025.0))
+    assert len(bright) > 10
+    with np.errstate(all="ignore"):
+        div = np.float32(10000.0) * mx.astype(np.float32) ** np.float32(0.6)
+        coef = np.where((mx > np.float32(65025.0))[..., None], light / div[..., None],
+                        np.float32(0.0)).astype(np.float32)
+    nz = np.argwhere(psf.max(-1) > 0) - psf.shape[0] // 2
+    rnz = int(np.abs(nz).max())
+    maxlevel = 32
+    while maxlevel > 0 and int(np.ceil(max(1, rnz) * 0.25 * 2 ** (maxlevel / 8))) + 1 > 52:
+        maxlevel -= 1
+    lib = oracle_mod._refmaplib()
+    lib.btref_calc_area.restype = C.c_float
+    lib.btref_calc_area.argtypes = [np.ctypeslib.ndpointer(np.float32)] * 2
+    levels = {}
+    rng = np.random.default_rng(21)
+    checked = 0
+    for b in bright[rng.permutation(len(bright))[:200]]:
+        ti = int(b[0]) + int(rng.integers(-6, 7))
+        tj = (int(b[1]) + int(rng.integers(-6, 7))) % W
+        if not 0 <= ti < H or not np.isfinite(got[ti, tj]).all() or area[ti, tj] <= 0:
+            continue
+        c = [vm[ti, tj], vm[ti, tj + 1], vm[ti + 1, tj + 1], vm[ti + 1, tj]]
+        ver = np.array([x[0] for x in c], np.float32)
+        hor = np.array([x[1] for x in c], np.float32)
+        mag = np.float32(lib.btref_calc_area(ver, hor)) / area[ti, tj]
+        kf = np.float32(4.0) * np.log2(mag) + np.float32(16.0)
+        if not np.isfinite(kf) or abs(kf - np.floor(kf) - 0.5) < 0.02:
+            continue  # the device's level could round the other way
+        k = min(maxlevel, max(0, int(np.rint(kf))))
+        if k not in levels:
+            levels[k] = psf_levels(bt, psf, k)
+        off, val = levels[k]
+        acc = np.zeros(3, np.float32)
+        for (oq, op), v in zip(off, val):
+            si, sj = ti - int(oq), (tj - int(op)) % W
+            if not 0 <= si < H:
+                continue
+            cs = coef[si, sj]
+            if (cs == 0).all():
+                continue
+            d = cs * v
+            acc += np.minimum(np.float32(65025.0), d * d)
+        exp = light[ti, tj] + acc
+        np.testing.assert_allclose(got[ti, tj], exp, rtol=1e-5, atol=1e-2)
+        checked += 1
+    print(f"scaled diffraction: {checked} pixels checked over levels {sorted(levels)}")
+    assert checked >= 50 and len(levels) >= 2
+
+
+@pytest.mark.gpu
+def test_blackbody_tables_vs_reference(bt, cuda, oracle_mod, frame_setup):
+    """Table 0 holds the reference's 391 colours through its RGBtoHSP /
+    HSPtoRGB; table 1 (1024 entries) the linear interpolation of the
+    reference's colours at k * 390/1023, through the same functions."""
+    if not oracle_mod.have_ref_map():
+        pytest.skip("reference map harness not built")
+    import ctypes as C
+    sp = frame_setup[4]
+    L = bt._lib
+    lib = oracle_mod._refmaplib()
+    ref = np.empty(1173, np.int32)
+    lib.btref_blackbody.argtypes = [np.ctypeslib.ndpointer(np.int32)]
+    lib.btref_blackbody(ref)
+    ref = ref.reshape(391, 3).astype(np.float32)
+    lib.btref_rgb_hsp.argtypes = [C.c_float] * 3 + [np.ctypeslib.ndpointer(np.float32)]
+    lib.btref_hsp_rgb.argtypes = [C.c_float] * 3 + [np.ctypeslib.ndpointer(np.float32)]
+
+    def hsp_rgb(c):
+        h = np.empty(3, np.float32)
+        lib.btref_rgb_hsp(float(c[0]), float(c[1]), float(c[2]), h)
+        o = np.empty(3, np.float32)
+        lib.btref_hsp_rgb(float(h[0]), float(h[1]), float(h[2]), o)
+        return h, np.float32(255.0) * o
+
+    for table, n in ((0, 391), (1, 1024)):
+        cnt = C.c_int()
+        hsp = np.empty((n, 3), np.float32)
+        rgb = np.empty((n, 3), np.float32)
+        L.check(L.lib().bt_stars_blackbody(sp._h, table, hsp.ctypes.data, rgb.ctypes.data, n,
+                                           C.byref(cnt), None))
+        assert cnt.value == n
+        for k in range(n):
+            if table == 0:
+                col = ref[k] / np.float32(255.0)
+            else:
+                t = np.float32(k) * (np.float32(390) / np.float32(1023))
+                i0 = min(int(t), 389)
+                f = t - np.float32(i0)
+                col = ((np.float32(1) - f) * ref[i0] + f * ref[i0 + 1]) / np.float32(255.0)
+            h, o = hsp_rgb(col)
+            np.testing.assert_allclose(hsp[k], h, rtol=1e-5, atol=1e-6, err_msg=f"{table} {k}")
+            np.testing.assert_allclose(rgb[k], o, rtol=1e-4, atol=1e-3, err_msg=f"{table} {k}")
+        if table == 1:  # the table's ends are the reference's first and last colours
+            np.testing.assert_allclose(rgb[0], hsp_rgb(ref[0] / 255)[1], rtol=1e-5)
+            np.testing.assert_allclose(rgb[-1], hsp_rgb(ref[-1] / 255)[1], rtol=1e-5)
 
 
 @pytest.mark.gpu

@@ -82,3 +82,35 @@ def test_newton_cap_reports_status(oracle_mod):
     th, ph = seeded_rays(200, seed=3)
     to, po, st, status = oracle_mod.integrate_rays(cam, 0.0, th, ph)
     assert set(np.unique(status)) <= {0, 1, 2, 3}
+
+
+def test_ref_frame_rows_equal_whole_frame(oracle_mod):
+    """The reference map kernels run on host threads with the colour passes
+    restricted to listed rows (ref_map_frame_rows, used for the full-size
+    frames) give the same corners, mask, areas and row colours as the
+    whole-frame single-thread run."""
+    if not oracle_mod.have_ref_map():
+        pytest.skip("reference map harness not built here")
+    from parity import map_grid_from_dense, sphere_view, synthetic_stars, value_noise_bgr
+    g = np.load(os.path.join(GOLD, "g_c2_l7s4.npz"))
+    grid, rows, GM = map_grid_from_dense(g["theta"], g["phi"], g["exists"], True)
+    W, H, tl = 256, 128, 7
+    bgr = value_noise_bgr(256, 512, seed=256)
+    stars = synthetic_stars(4000, seed=4000, tmax=15000.0)
+    pos, mg, tree = oracle_mod.ref_star_tree(*stars, tl)
+    cam7 = np.array([0.3, 0.9, 0.1, 1.2, 0.0, 0.0, 1.0], np.float32)
+    view = sphere_view(W, H)
+    ml = int(g["maxlevel"])
+    ref = oracle_mod.ref_map_frame(grid, rows, GM, ml, view, W, H, cam7, bgr=bgr,
+                                   stars=(pos, mg, tree, tl), lr=True)
+    sat = oracle_mod.ref_map_sat(bgr)
+    assert np.array_equal(sat, ref["sat"])
+    for sel in (np.arange(H), np.arange(3, H, 16)):
+        r = oracle_mod.ref_map_frame_rows(grid, rows, GM, ml, view, W, H, cam7, sel, sat=sat,
+                                          env_shape=bgr.shape[:2], stars=(pos, mg, tree, tl),
+                                          lr=True, nthreads=4)
+        for k in ("thphi", "gap", "bh", "area"):
+            assert np.array_equal(r[k], ref[k]), k
+        assert np.array_equal(r["env"], ref["env"].reshape(H, W, 4)[sel])
+        assert np.array_equal(r["stars"], ref["stars"].reshape(H, W, 4)[sel])
+        assert np.array_equal(r["image"], ref["image"].reshape(H, W, 4)[sel])
