@@ -97,27 +97,6 @@ int make_ray_params(const bt_camera* c, double a, const bt_integ_opts* o,
   return BT_OK;
 }
 
-// ---------------------------------------------------------------- kernels
-// One ray per thread, grid-stride.  256 threads, the FP64 register file
-// limits residency to ~2 blocks/SM.
-__global__ void __launch_bounds__(128)
-k_integrate_plain(const RayParams p, const double* __restrict__ th,
-                  const double* __restrict__ ph, size_t n,
-                  double* __restrict__ tho, double* __restrict__ pho,
-                  int32_t* __restrict__ steps, uint8_t* __restrict__ status) {
-  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n;
-       r += (size_t)gridDim.x * blockDim.x) {
-    double to, po;
-    int32_t st;
-    uint8_t s;
-    plain::integrate_ray(p, th[r], ph[r], to, po, st, s);
-    tho[r] = to;
-    pho[r] = po;
-    steps[r] = st;
-    if (status) status[r] = s;
-  }
-}
-
 struct PlainPolicy {
   using State = plain::CachedState;
   static __device__ __forceinline__ bool begin(const RayParams& p, double th,
@@ -157,18 +136,11 @@ int launch_integrate(const RayParams& p, const double* th, const double* ph,
                      size_t n, double* tho, double* pho, int32_t* steps,
                      uint8_t* status, cudaStream_t s) {
   if (n == 0) return BT_OK;
-  const int threads = 128;
-  size_t blocks = (n + threads - 1) / threads;
-  const size_t cap = (size_t)sm_count() * 16;
-  if (blocks > cap) blocks = cap;
   if (p.precision == BT_PRECISION_MIXED)
     return launch_integrate_mixed(p, th, ph, n, tho, pho, steps, status, s);
   if (p.precision == BT_PRECISION_FAST)
     return launch_integrate_fast(p, th, ph, n, tho, pho, steps, status, s);
-  k_integrate_plain<<<(unsigned)blocks, threads, 0, s>>>(p, th, ph, n, tho,
-                                                         pho, steps, status);
-  BT_CUDA_TRY(cudaGetLastError());
-  return BT_OK;
+  return launch_trace_rays<PlainPolicy>(p, th, ph, n, tho, pho, steps, status, s);
 }
 
 // Independent DFMA chains: 8 accumulators per thread, no memory traffic.

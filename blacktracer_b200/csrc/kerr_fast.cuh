@@ -202,16 +202,5 @@ __device__ __forceinline__ bool attempt(const RayParams& p, FastState& s) {
   return s.z <= p.z_end || s.nstp >= p.maxstp;
 }
 
-__device__ __forceinline__ void integrate_ray(const RayParams& p, double th, double ph,
-                                              double& tho, double& pho, int32_t& steps,
-                                              uint8_t& status) {
-  FastState s;
-  if (!begin_ray(p, th, ph, s, tho, pho, steps, status)) return;
-  if (p.maxstp > 0)
-    while (!attempt(p, s)) {
-    }
-  plain::finish_ray(p, s, tho, pho, steps, status);
-}
-
 }  // namespace fast
 }  // namespace bt

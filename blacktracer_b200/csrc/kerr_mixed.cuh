@@ -158,17 +158,5 @@ __device__ __forceinline__ bool begin_ray(const RayParams& p, double th,
   return go;
 }
 
-__device__ __forceinline__ void integrate_ray(const RayParams& p, double th,
-                                              double ph, double& tho,
-                                              double& pho, int32_t& steps,
-                                              uint8_t& status) {
-  MixedState m;
-  if (!begin_ray(p, th, ph, m, tho, pho, steps, status)) return;
-  if (p.maxstp > 0)
-    while (!attempt(p, m)) {
-    }
-  plain::finish_ray(p, m.s, tho, pho, steps, status);
-}
-
 }  // namespace mixed
 }  // namespace bt

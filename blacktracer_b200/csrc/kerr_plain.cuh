@@ -373,22 +373,5 @@ __device__ __forceinline__ void finish_ray(const RayParams& p,
   status = done ? BT_RAY_ESCAPED : BT_RAY_MAXSTEP;
 }
 
-// Complete integration of one ray (integration_wrapper body + rkckIntegrate1
-// + odeint1, BT/Grid.h:549-553, BT/Metric.h:276-324).
-__device__ __forceinline__ void integrate_ray(const RayParams& p, double th,
-                                              double ph, double& tho,
-                                              double& pho, int32_t& steps,
-                                              uint8_t& status) {
-  CachedState s;
-  if (!begin_ray_cached(p, th, ph, s, tho, pho, steps, status)) return;
-  if (p.maxstp <= 0) {
-    finish_ray(p, s, tho, pho, steps, status);
-    return;
-  }
-  while (!attempt_cached(p, s)) {
-  }
-  finish_ray(p, s, tho, pho, steps, status);
-}
-
 }  // namespace plain
 }  // namespace bt

@@ -49,55 +49,11 @@ struct FastPolicy {
   }
 };
 
-__global__ void __launch_bounds__(128)
-k_integrate_fast(const RayParams p, const double* __restrict__ th,
-                 const double* __restrict__ ph, size_t n,
-                 double* __restrict__ tho, double* __restrict__ pho,
-                 int32_t* __restrict__ steps, uint8_t* __restrict__ status) {
-  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n;
-       r += (size_t)gridDim.x * blockDim.x) {
-    double to, po;
-    int32_t st;
-    uint8_t s;
-    fast::integrate_ray(p, th[r], ph[r], to, po, st, s);
-    tho[r] = to;
-    pho[r] = po;
-    steps[r] = st;
-    if (status) status[r] = s;
-  }
-}
-
-__global__ void __launch_bounds__(128)
-k_integrate_mixed(const RayParams p, const double* __restrict__ th,
-                  const double* __restrict__ ph, size_t n,
-                  double* __restrict__ tho, double* __restrict__ pho,
-                  int32_t* __restrict__ steps, uint8_t* __restrict__ status) {
-  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < n;
-       r += (size_t)gridDim.x * blockDim.x) {
-    double to, po;
-    int32_t st;
-    uint8_t s;
-    mixed::integrate_ray(p, th[r], ph[r], to, po, st, s);
-    tho[r] = to;
-    pho[r] = po;
-    steps[r] = st;
-    if (status) status[r] = s;
-  }
-}
-
 int launch_integrate_mixed(const RayParams& p, const double* th,
                            const double* ph, size_t n, double* tho,
                            double* pho, int32_t* steps, uint8_t* status,
                            cudaStream_t s) {
-  if (n == 0) return BT_OK;
-  const int threads = 128;
-  size_t blocks = (n + threads - 1) / threads;
-  const size_t cap = (size_t)sm_count() * 16;
-  if (blocks > cap) blocks = cap;
-  k_integrate_mixed<<<(unsigned)blocks, threads, 0, s>>>(p, th, ph, n, tho,
-                                                         pho, steps, status);
-  BT_CUDA_TRY(cudaGetLastError());
-  return BT_OK;
+  return launch_trace_rays<MixedPolicy>(p, th, ph, n, tho, pho, steps, status, s);
 }
 
 int launch_trace_mixed(const GridDesc* D, int G, const uint32_t* qoff,
@@ -108,15 +64,7 @@ int launch_trace_mixed(const GridDesc* D, int G, const uint32_t* qoff,
 int launch_integrate_fast(const RayParams& p, const double* th, const double* ph,
                           size_t n, double* tho, double* pho, int32_t* steps,
                           uint8_t* status, cudaStream_t s) {
-  if (n == 0) return BT_OK;
-  const int threads = 128;
-  size_t blocks = (n + threads - 1) / threads;
-  const size_t cap = (size_t)sm_count() * 16;
-  if (blocks > cap) blocks = cap;
-  k_integrate_fast<<<(unsigned)blocks, threads, 0, s>>>(p, th, ph, n, tho, pho, steps,
-                                                        status);
-  BT_CUDA_TRY(cudaGetLastError());
-  return BT_OK;
+  return launch_trace_rays<FastPolicy>(p, th, ph, n, tho, pho, steps, status, s);
 }
 
 int launch_trace_fast(const GridDesc* D, int G, const uint32_t* qoff,

@@ -2,12 +2,14 @@
 //
 // One ray per lane.  Rays take from 1 to 1000 attempts, so a warp that ran
 // each lane's ray to completion would idle most lanes behind the longest ray.
-// Instead every lane whose ray finishes takes the next ray from a global work
-// queue at once (warp-aggregated atomicAdd on the queue head), so lanes stay
-// busy until the queue is empty; only the last rays leave idle lanes.
+// Instead every lane whose ray finishes takes the next ray at once, so lanes
+// stay busy until the work runs out; only the last rays leave idle lanes.
+// Grid builds take rays from a work queue in device memory (warp-aggregated
+// atomicAdd on its head); the ray-list form of bt_integrate_rays gives each
+// warp a fixed stride of the caller's rays (no state outside the call).
 //
 // Policy supplies State, begin(), attempt(), finish() -- see PlainPolicy in
-// integrate.cu and MixedPolicy in mixed.cu.
+// integrate.cu and MixedPolicy / FastPolicy in mixed.cu.
 #pragma once
 
 #include "bt_internal.h"
@@ -74,9 +76,13 @@ k_trace_lattice(const GridDesc* __restrict__ D, int G,
           int32_t s;
           uint8_t ss;
           lattice_seed(d.L, key, th, ph);
-          if (Policy::begin(d.p, th, ph, st, to, po, s, ss)) {
+          // a ray past the capture test takes its attempts (none when
+          // maxstp is 0: odeint1's loop, BT/Metric.h:283, does not run)
+          const bool go = Policy::begin(d.p, th, ph, st, to, po, s, ss);
+          if (go && d.p.maxstp > 0) {
             slot = k;
           } else {
+            if (go) Policy::finish(d.p, st, to, po, s, ss);
             d.L.thphi[key] = make_double2(to, po);
             d.L.steps[key] = s;
             d.L.vstat[key] = ss;
@@ -139,46 +145,51 @@ int launch_trace_shape(const GridDesc* D, int G, const uint32_t* qoff,
   }
 }
 
-// Ray-list form (bt_integrate_rays): rays 0..n-1, queue head in *fetch.
+// Ray-list form (bt_integrate_rays): rays 0..n-1 of caller arrays.  A
+// persistent launch (the resident blocks only); warp w of the W warps owns
+// rays w, w + W, w + 2W, ... and its lanes take them in that order as they
+// finish: the warp's next-ray counter is a register every lane holds (all
+// lanes add the same ballot count), so nothing outside the call's arrays is
+// read or written and calls on different streams share no state.  Striding
+// spreads each warp's rays over the whole list, so warps see similar mixes
+// of short and long rays.
 template <class Policy>
 __global__ void __launch_bounds__(128)
-k_trace_list(const RayParams p, const double* __restrict__ th_in,
+k_trace_rays(const RayParams p, const double* __restrict__ th_in,
              const double* __restrict__ ph_in, size_t n,
              double* __restrict__ tho, double* __restrict__ pho,
-             int32_t* __restrict__ steps, uint8_t* __restrict__ status,
-             unsigned long long* fetch) {
+             int32_t* __restrict__ steps, uint8_t* __restrict__ status) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
+  const size_t W = (size_t)gridDim.x * (blockDim.x >> 5);
+  const size_t w = (size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  size_t next = 0;  // warp-uniform
   bool idle = true, done = false;
   size_t r = 0;
   typename Policy::State st;
   for (;;) {
     const bool need = idle && !done;
     const unsigned m = __ballot_sync(0xffffffffu, need);
-    if (m) {
-      const int leader = __ffs(m) - 1;
-      unsigned long long base = 0;
-      if ((int)lane == leader)
-        base = atomicAdd(fetch, (unsigned long long)__popc(m));
-      base = __shfl_sync(0xffffffffu, base, leader);
-      if (need) {
-        const unsigned long long k = base + (unsigned)__popc(m & lt_mask);
-        if (k < n) {
-          r = (size_t)k;
-          double to, po;
-          int32_t s;
-          uint8_t ss;
-          if (Policy::begin(p, th_in[r], ph_in[r], st, to, po, s, ss)) {
-            idle = false;
-          } else {
-            tho[r] = to; pho[r] = po; steps[r] = s;
-            if (status) status[r] = ss;
-          }
+    if (need) {
+      const size_t k = w + (next + (size_t)__popc(m & lt_mask)) * W;
+      if (k < n) {
+        r = k;
+        double to, po;
+        int32_t s;
+        uint8_t ss;
+        const bool go = Policy::begin(p, th_in[r], ph_in[r], st, to, po, s, ss);
+        if (go && p.maxstp > 0) {
+          idle = false;
         } else {
-          done = true;
+          if (go) Policy::finish(p, st, to, po, s, ss);
+          tho[r] = to; pho[r] = po; steps[r] = s;
+          if (status) status[r] = ss;
         }
+      } else {
+        done = true;
       }
     }
+    next += (size_t)__popc(m);
     if (__all_sync(0xffffffffu, done)) break;
     if (!idle) {
       if (Policy::attempt(p, st)) {
@@ -192,6 +203,30 @@ k_trace_list(const RayParams p, const double* __restrict__ th_in,
       }
     }
   }
+}
+
+// Launch of k_trace_rays: as many 128-thread blocks as are resident on the
+// device at once, fewer when there are fewer rays than lanes.
+template <class Policy>
+int launch_trace_rays(const RayParams& p, const double* th, const double* ph, size_t n,
+                      double* tho, double* pho, int32_t* steps, uint8_t* status,
+                      cudaStream_t s) {
+  if (n == 0) return BT_OK;
+  static int per_sm = 0;  // per Policy
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_rays<Policy>, 128, 0);
+    if (per_sm < 1) per_sm = 1;
+  }
+  size_t blocks = (size_t)sm_count() * per_sm;
+  const size_t need = (n + 127) / 128;
+  if (blocks > need) blocks = need;
+  k_trace_rays<Policy><<<(unsigned)blocks, 128, 0, s>>>(p, th, ph, n, tho, pho, steps, status);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error("ray launch: %s", cudaGetErrorString(e));
+    return BT_ERR_CUDA;
+  }
+  return BT_OK;
 }
 
 }  // namespace bt

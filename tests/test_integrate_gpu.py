@@ -128,3 +128,26 @@ def test_fast_reciprocal_within_two_ulp(bt, cuda):
     ulp = np.abs(got - ref) / np.spacing(np.abs(ref))
     print(f"fast reciprocal: max {ulp.max():.2f} ulp, exact {(ulp == 0).mean():.4f}")
     assert ulp.max() <= 2
+
+
+@pytest.mark.parametrize("prec", ["plain", "fast"])
+@pytest.mark.parametrize("maxstp,eps", [(0, 1e-5), (5, 1e-5), (1000, 1e-7)])
+def test_options_vs_oracle(bt, cuda, oracle_mod, prec, maxstp, eps):
+    """Non-default step control (odeint1's MAXSTP, rkckIntegrate1's eps):
+    maxstp 0 runs no attempt (the state stays the start state), a small
+    maxstp stops rays early, a tighter eps takes more steps."""
+    cam, a = oracle_camera(oracle_mod, "c2")
+    th, ph = seeded_rays(4000, seed=19)
+    ro = oracle_mod.integrate_rays(cam, a, th, ph, opts=(eps, 0.01, -1e7, maxstp))
+    opts = bt.IntegOpts(prec, eps=eps, maxstp=maxstp)
+    to, po, st, ss = run_gpu(bt, cuda, cam, a, th, ph, opts)
+    assert np.array_equal(ss == 1, ro[3] == 1), "capture classification differs"
+    assert np.array_equal(ss, ro[3]) or prec == "fast"
+    err = ang_err(to, po, ro[0], ro[1])
+    same = float((st == ro[2]).mean())
+    print(f"{prec} maxstp {maxstp} eps {eps}: same steps {same:.4f} "
+          f"p99 {np.percentile(err, 99):.2e} max {err.max():.2e}")
+    tol = PLAIN_TOL if prec == "plain" else MIXED_P99
+    assert same >= 0.99 and float((err <= tol).mean()) >= 0.99
+    if maxstp == 0:
+        assert np.array_equal(st, ro[2]) and err.max() == 0.0
