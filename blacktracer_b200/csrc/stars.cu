@@ -268,9 +268,9 @@ k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
   if (valid) flag[ij] = (uint8_t)my_any;
 }
 
-constexpr int kHeavyThreads = 512;  // one block per deferred pixel
-constexpr int kHeavyWarps = kHeavyThreads / 32;
 constexpr int kHeavyNodes = 1024;   // nodes per search pass (shared memory)
+// Candidate leaves box-tested per batch of a deferred pixel.
+constexpr int kHeavyBatch = 2048;
 // Deferred pixels with at least this many candidate leaves are scheduled
 // first, so that the longest pixels do not start last.
 constexpr long long kGiantLeaves = 512;
@@ -306,36 +306,40 @@ __global__ void k_heavy_plan(const float2* __restrict__ thphi,
 }
 
 // The deferred pixels, one block at a time each, taken from the queues by a
-// shared counter (giant pixels first).  Thread 0 walks the kd-tree (in
-// passes of kHeavyNodes emitted nodes) into shared memory with a prefix sum
-// of the number of leaves under each node.  The block then takes that flat
-// range of candidate leaves 512 at a time: each thread tests one leaf's
-// bounding box against the pixel's quad, the survivors are compacted in
-// thread order, and each warp sweeps the stars of one surviving leaf at a
-// time, 32 stars per step.  A thread that holds a hit splats it into its own
-// (2s+1)^2 cell registers with the per-star form of the brightness
-// (star_fast); the threads' cells are added by a block reduction at the end.
-// Sums are reassociated relative to the reference's star order, which
-// changes them only by float rounding; the order is fixed, so frames are
-// reproducible.
-template <int kStep>
-__global__ void __launch_bounds__(kHeavyThreads, 1)
+// shared counter (giant pixels first); kThreads-thread blocks, several per
+// SM, so that one block's barrier waits overlap another's work.  Thread 0
+// walks the kd-tree (in passes of kHeavyNodes emitted nodes) into shared
+// memory with a prefix sum of the number of leaves under each node.  The
+// block then takes that flat range of candidate leaves kHeavyBatch at a time:
+// thread t box-tests leaves t, t + kThreads, ... of the batch against the
+// pixel's quad, each warp lists its survivors in its own segment, and after
+// one barrier the warps sweep the survivors round-robin, one leaf at a time,
+// 32 stars per step.  Hits wait in a per-warp queue and are splatted 32 at a
+// time, one per lane, into the lane's (2s+1)^2 cell registers with the
+// per-star form of the brightness (star_fast); the threads' cells are added
+// by a block reduction at the end.  Sums are reassociated relative to the
+// reference's star order, which changes them only by float rounding; the
+// order is fixed, so frames are reproducible.
+template <int kStep, int kThreads>
+__global__ void __launch_bounds__(kThreads, 512 / kThreads)
 k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
              StarSet S, Cam7 cam, int M, int N, const float2* __restrict__ view,
              int lr, const float* __restrict__ area, float3* __restrict__ cells,
              uint8_t* __restrict__ flag, const uint32_t* __restrict__ order,
              uint32_t* hc, uint32_t np) {
   constexpr int FW = 2 * kStep + 1, FW2 = FW * FW;
+  constexpr int kWarps = kThreads / 32;
+  constexpr int kPer = kHeavyBatch / kThreads;  // leaves per thread per batch
   __shared__ int sh_node[kHeavyNodes];
   __shared__ long long sh_end[kHeavyNodes];  // inclusive prefix of leaf counts
   __shared__ int sh_count, sh_more;
   __shared__ long long sh_total;
-  __shared__ int sh_surv[kHeavyThreads];
-  __shared__ int sh_wcount[kHeavyWarps];
-  __shared__ float3 sh_red[kHeavyWarps][FW2];
+  __shared__ int sh_surv[kWarps][kPer * 32];
+  __shared__ int sh_wcount[kWarps];
+  __shared__ float3 sh_red[kWarps][FW2];
   __shared__ uint32_t sh_item;
-  __shared__ int sh_q[kHeavyWarps][64];
-  __shared__ float2 sh_qpos[kHeavyWarps][64];
+  __shared__ int sh_q[kWarps][64];
+  __shared__ float2 sh_qpos[kWarps][64];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const int L = S.treeLevel;
   for (;;) {
@@ -398,35 +402,39 @@ k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
       __syncthreads();
       const int count = sh_count;
       const long long total = sh_total;
-      for (long long base = 0; base < total; base += kHeavyThreads) {
-        const long long k = base + tid;
-        int leaf = -1;
-        if (k < total) {
-          int lo = 0, hi = count - 1;
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (sh_end[mid] > k) hi = mid;
-            else lo = mid + 1;
+      for (long long base = 0; base < total; base += kHeavyBatch) {
+        // box tests: this warp's survivors, in (round, lane) order
+        int wn = 0;
+#pragma unroll 1
+        for (int r = 0; r < kPer; r++) {
+          const long long k = base + (long long)r * kThreads + tid;
+          int leaf = -1;
+          if (k < total) {
+            int lo = 0, hi = count - 1;
+            while (lo < hi) {
+              const int mid = (lo + hi) >> 1;
+              if (sh_end[mid] > k) hi = mid;
+              else lo = mid + 1;
+            }
+            const int node = sh_node[lo];
+            const int d = L - node_level(node);
+            leaf = (int)((((long long)node + 1) << d) - 1 + (k - (lo ? sh_end[lo - 1] : 0)));
+            if (node_excluded(P, S.box[leaf])) leaf = -1;
           }
-          const int node = sh_node[lo];
-          const int d = L - node_level(node);
-          leaf = (int)((((long long)node + 1) << d) - 1 + (k - (lo ? sh_end[lo - 1] : 0)));
-          if (node_excluded(P, S.box[leaf])) leaf = -1;
+          const unsigned keep = __ballot_sync(0xffffffffu, leaf >= 0);
+          if (leaf >= 0) sh_surv[w][wn + __popc(keep & ((1u << lane) - 1u))] = leaf;
+          wn += __popc(keep);
         }
-        // compaction in thread order
-        const unsigned keep = __ballot_sync(0xffffffffu, leaf >= 0);
-        if (lane == 0) sh_wcount[w] = __popc(keep);
+        if (lane == 0) sh_wcount[w] = wn;
         __syncthreads();
-        int wbase = 0, ns = 0;
-        for (int ww = 0; ww < kHeavyWarps; ww++) {
-          if (ww < w) wbase += sh_wcount[ww];
-          ns += sh_wcount[ww];
-        }
-        if (leaf >= 0) sh_surv[wbase + __popc(keep & ((1u << lane) - 1u))] = leaf;
-        __syncthreads();
-        for (int s = w; s < ns; s += kHeavyWarps) {
+        int ns = 0;
+        for (int ww = 0; ww < kWarps; ww++) ns += sh_wcount[ww];
+        // sweep: survivor s (over the warps' segments in order) to warp s % kWarps
+        int seg = 0, segbase = 0;
+        for (int s = w; s < ns; s += kWarps) {
+          while (s >= segbase + sh_wcount[seg]) segbase += sh_wcount[seg++];
           int a0, a1;
-          node_range(S, sh_surv[s], a0, a1);
+          node_range(S, sh_surv[seg][s - segbase], a0, a1);
           for (int qb = a0; qb < a1; qb += 32) {
             const int q = qb + lane;
             float st = 0.f, sp = 0.f;
@@ -477,7 +485,7 @@ k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
       __syncthreads();
       if (tid < FW2) {
         float3 v = make_float3(0.f, 0.f, 0.f);
-        for (int ww = 0; ww < kHeavyWarps; ww++) {
+        for (int ww = 0; ww < kWarps; ww++) {
           v.x += sh_red[ww][tid].x;
           v.y += sh_red[ww][tid].y;
           v.z += sh_red[ww][tid].z;
@@ -521,9 +529,19 @@ __global__ void k_blackbody_tables_1k(float4* __restrict__ bb) {
   bb[kBlackbody1k + k] = make_float4(255.f * r, 255.f * g, 255.f * b, 0.f);
 }
 
+// Threads per block of k_star_heavy; the launch fills the SMs with as many
+// blocks as are resident at once.
+constexpr int kHeavyThreads = 256;
+
 template <int kStep>
 void launch_heavy(MapScratch& Sc, const MapFrame& F, const StarSet& SS, cudaStream_t s) {
-  k_star_heavy<kStep><<<sm_count() * 2, kHeavyThreads, 0, s>>>(
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_star_heavy<kStep, kHeavyThreads>,
+                                                  kHeavyThreads, 0);
+    if (per_sm < 1) per_sm = 1;
+  }
+  k_star_heavy<kStep, kHeavyThreads><<<sm_count() * per_sm, kHeavyThreads, 0, s>>>(
       Sc.thphi, Sc.bh, SS, F.cam, Sc.M, Sc.N, F.view, F.lr, Sc.area, Sc.cells,
       Sc.flag, Sc.heavy_order, Sc.heavy_count, (uint32_t)((size_t)Sc.M * Sc.N));
 }

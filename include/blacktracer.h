@@ -47,7 +47,15 @@ enum {
 enum {
   BT_PRECISION_PLAIN = 0, /* FP64, reference operation order, no FMA      */
   BT_PRECISION_MIXED = 1, /* FP32 bulk, FP64 near the photon sphere, at
-                             turning points, for capture and for phi       */
+                             turning points, for capture and for phi.
+                             Does NOT meet 1e-6 rad against the reference:
+                             p99 ~1.6e-4 rad on the C2 grid, with a
+                             different grid topology.  The reference's step
+                             controller reads an error estimate whose FP32
+                             rounding noise (1e-4..1e-1 relative where the
+                             FP64 one is 1e-9..5e-4) changes its accept /
+                             grow decisions, so the rays follow other step
+                             sequences; FAST is the form that meets 1e-6.  */
   BT_PRECISION_FAST = 2   /* FP64, the same method with the equations of
                              motion reassociated (3 reciprocals instead of
                              16 divisions, by Newton-refined approximate
