@@ -531,7 +531,7 @@ __global__ void k_blackbody_tables_1k(float4* __restrict__ bb) {
 
 // Threads per block of k_star_heavy; the launch fills the SMs with as many
 // blocks as are resident at once.
-constexpr int kHeavyThreads = 256;
+constexpr int kHeavyThreads = 512;
 
 template <int kStep>
 void launch_heavy(MapScratch& Sc, const MapFrame& F, const StarSet& SS, cudaStream_t s) {

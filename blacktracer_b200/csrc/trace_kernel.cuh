@@ -19,6 +19,12 @@ namespace bt {
 constexpr uint32_t kLaneIdle = 0xffffffffu;  // needs a ray
 constexpr uint32_t kLaneDone = 0xfffffffeu;  // queue exhausted
 
+// A warp refills its idle lanes once at least this many are idle (or none is
+// busy): a new ray's set-up and capture test (a Newton and a golden-section
+// loop, about two attempts of FP64 work) runs for all refilled lanes at once
+// while the warp's other lanes wait, instead of once per finishing lane.
+constexpr int kRefillMin = 8;
+
 // Ray seeds of lattice vertex (i, j), Grid::callKernel BT/Grid.h:388-389.
 __device__ __forceinline__ void lattice_seed(const LatticeView& L, uint32_t key,
                                              double& th, double& ph) {
@@ -57,7 +63,8 @@ k_trace_lattice(const GridDesc* __restrict__ D, int G,
   for (;;) {
     const bool need = slot == kLaneIdle;
     const unsigned m = __ballot_sync(0xffffffffu, need);
-    if (m) {
+    const unsigned busy = __ballot_sync(0xffffffffu, slot < kLaneDone);
+    if (m && (__popc(m) >= kRefillMin || !busy)) {
       const int leader = __ffs(m) - 1;
       uint32_t base = 0;
       if ((int)lane == leader) base = atomicAdd(qfetch, (uint32_t)__popc(m));
@@ -147,10 +154,11 @@ int launch_trace_shape(const GridDesc* D, int G, const uint32_t* qoff,
 
 // Ray-list form (bt_integrate_rays): rays 0..n-1 of caller arrays.  A
 // persistent launch (the resident blocks only); warp w of the W warps owns
-// rays w, w + W, w + 2W, ... and its lanes take them in that order as they
-// finish: the warp's next-ray counter is a register every lane holds (all
-// lanes add the same ballot count), so nothing outside the call's arrays is
-// read or written and calls on different streams share no state.  Striding
+// rays w, w + W, w + 2W, ... and its idle lanes take them in that order (as
+// the grid form, kRefillMin at a time): the warp's next-ray counter is a
+// register every lane holds (all lanes add the same ballot count), so nothing
+// outside the call's arrays is read or written and calls on different
+// streams share no state.  Striding
 // spreads each warp's rays over the whole list, so warps see similar mixes
 // of short and long rays.
 template <class Policy>
@@ -170,26 +178,29 @@ k_trace_rays(const RayParams p, const double* __restrict__ th_in,
   for (;;) {
     const bool need = idle && !done;
     const unsigned m = __ballot_sync(0xffffffffu, need);
-    if (need) {
-      const size_t k = w + (next + (size_t)__popc(m & lt_mask)) * W;
-      if (k < n) {
-        r = k;
-        double to, po;
-        int32_t s;
-        uint8_t ss;
-        const bool go = Policy::begin(p, th_in[r], ph_in[r], st, to, po, s, ss);
-        if (go && p.maxstp > 0) {
-          idle = false;
+    const unsigned busy = __ballot_sync(0xffffffffu, !idle);
+    if (m && (__popc(m) >= kRefillMin || !busy)) {
+      if (need) {
+        const size_t k = w + (next + (size_t)__popc(m & lt_mask)) * W;
+        if (k < n) {
+          r = k;
+          double to, po;
+          int32_t s;
+          uint8_t ss;
+          const bool go = Policy::begin(p, th_in[r], ph_in[r], st, to, po, s, ss);
+          if (go && p.maxstp > 0) {
+            idle = false;
+          } else {
+            if (go) Policy::finish(p, st, to, po, s, ss);
+            tho[r] = to; pho[r] = po; steps[r] = s;
+            if (status) status[r] = ss;
+          }
         } else {
-          if (go) Policy::finish(p, st, to, po, s, ss);
-          tho[r] = to; pho[r] = po; steps[r] = s;
-          if (status) status[r] = ss;
+          done = true;
         }
-      } else {
-        done = true;
       }
+      next += (size_t)__popc(m);
     }
-    next += (size_t)__popc(m);
     if (__all_sync(0xffffffffu, done)) break;
     if (!idle) {
       if (Policy::attempt(p, st)) {
