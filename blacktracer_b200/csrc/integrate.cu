@@ -105,6 +105,10 @@ struct PlainPolicy {
                                                uint8_t& ss) {
     return plain::begin_ray_cached(p, th, ph, s, to, po, st, ss);
   }
+  static __device__ __forceinline__ void start(const RayParams& p, const plain::RayStart& rs,
+                                               State& s) {
+    plain::start_ray_cached(p, rs, s);
+  }
   static __device__ __forceinline__ bool attempt(const RayParams& p, State& s) {
     return plain::attempt_cached(p, s);
   }

@@ -164,6 +164,12 @@ __device__ __forceinline__ bool begin_ray(const RayParams& p, double th, double 
   return plain::begin_ray(p, th, ph, s, tho, pho, steps, status);
 }
 
+__device__ __forceinline__ void start_ray(const RayParams& p, const plain::RayStart& rs,
+                                          FastState& s) {
+  s.dv = false;
+  plain::start_ray(p, rs, s);
+}
+
 // One quality-controlled attempt (odeint1 loop body + rkqs, BT/Metric.h
 // :291-302, 253-270) in the fast form.
 __device__ __forceinline__ bool attempt(const RayParams& p, FastState& s) {

@@ -158,5 +158,12 @@ __device__ __forceinline__ bool begin_ray(const RayParams& p, double th,
   return go;
 }
 
+__device__ __forceinline__ void start_ray(const RayParams& p, const plain::RayStart& rs,
+                                          MixedState& m) {
+  plain::start_ray(p, rs, m.s);
+  m.r0 = (float)rs.r0;
+  m.n64 = 0;
+}
+
 }  // namespace mixed
 }  // namespace bt

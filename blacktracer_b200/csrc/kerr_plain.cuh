@@ -248,31 +248,60 @@ struct RayState {
   int32_t nstp, step;
 };
 
+// The result of a ray's set-up and capture test when it must be integrated:
+// initial momenta, the constants of motion and the spherical photon-orbit
+// radius of its b (the capture test's Newton solution).
+struct RayStart {
+  double pR, pTheta, b, q, r0;
+};
+
 // Set-up + capture test of one ray (BT/Grid.h:524-552).  Returns true when
-// the ray must be integrated; otherwise tho/pho/steps/status are final.
-__device__ __forceinline__ bool begin_ray(const RayParams& p, double th,
-                                          double ph, RayState& s, double& tho,
-                                          double& pho, int32_t& steps,
-                                          uint8_t& status,
-                                          double* r0_out = nullptr) {
+// the ray must be integrated (rs filled); otherwise tho/pho/steps/status are
+// final.
+__device__ __forceinline__ bool setup_ray(const RayParams& p, double th, double ph,
+                                          RayStart& rs, double& tho, double& pho,
+                                          int32_t& steps, uint8_t& status) {
   double pR, pTheta, b, q;
   ray_setup(p, th, ph, pR, pTheta, b, q);
   tho = -1;
   pho = -1;
   steps = 0;
-  const int cel = celestial(p, pR, b, q, r0_out);
+  double r0 = 0;
+  const int cel = celestial(p, pR, b, q, &r0);
   if (cel <= 0) {
     status = cel < 0 ? BT_RAY_NONCONVERGED : BT_RAY_CAPTURED;
     return false;
   }
-  s.y[0] = p.rS; s.y[1] = p.thetaS; s.y[2] = p.phiS; s.y[3] = pR;
-  s.y[4] = pTheta;
+  rs.pR = pR;
+  rs.pTheta = pTheta;
+  rs.b = b;
+  rs.q = q;
+  rs.r0 = r0;
+  return true;
+}
+
+// odeint1's start state (BT/Metric.h:276-281, rkckIntegrate1 :307-324).
+__device__ __forceinline__ void start_ray(const RayParams& p, const RayStart& rs,
+                                          RayState& s) {
+  s.y[0] = p.rS; s.y[1] = p.thetaS; s.y[2] = p.phiS; s.y[3] = rs.pR;
+  s.y[4] = rs.pTheta;
   s.z = 0.0;
   s.h = p.h1 * (p.z_end > 0 ? 1 : (p.z_end < 0 ? -1 : 0));
-  s.b = b;
-  s.q = q;
+  s.b = rs.b;
+  s.q = rs.q;
   s.nstp = 0;
   s.step = 0;
+}
+
+__device__ __forceinline__ bool begin_ray(const RayParams& p, double th,
+                                          double ph, RayState& s, double& tho,
+                                          double& pho, int32_t& steps,
+                                          uint8_t& status,
+                                          double* r0_out = nullptr) {
+  RayStart rs;
+  if (!setup_ray(p, th, ph, rs, tho, pho, steps, status)) return false;
+  if (r0_out) *r0_out = rs.r0;
+  start_ray(p, rs, s);
   return true;
 }
 
@@ -318,6 +347,12 @@ __device__ __forceinline__ bool begin_ray_cached(const RayParams& p, double th, 
                                                  int32_t& steps, uint8_t& status) {
   s.dv = false;
   return begin_ray(p, th, ph, s, tho, pho, steps, status);
+}
+
+__device__ __forceinline__ void start_ray_cached(const RayParams& p, const RayStart& rs,
+                                                 CachedState& s) {
+  s.dv = false;
+  start_ray(p, rs, s);
 }
 
 // Step-size update of rkqs (BT/Metric.h:262-268) with one pow for both

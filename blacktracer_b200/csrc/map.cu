@@ -271,24 +271,73 @@ __global__ void k_smooth_v(const float* __restrict__ in, float* __restrict__ are
   area[(size_t)i * M + j] = sum / (1.f * count);
 }
 
-// Summed-area table of the environment map, one thread per column, rows in
-// order: the reference's sequential float accumulation (cudaPrep,
-// BT/MakeImageKernel.cu:1312-1330).  Channels: B^2.2*A, G^2.2*A, R^2.2*A, A.
-__global__ void k_sat(const uint8_t* __restrict__ bgr, int rows, int cols,
-                      float4* __restrict__ sat) {
+// Summed-area table of the environment map (cudaPrep, BT/MakeImageKernel.cu
+// :1312-1330): per column, down the rows, the running float sums of
+// B^2.2 A, G^2.2 A, R^2.2 A and A, A the cell's solid angle (calcArea,
+// BT/kernel.cuh:586-610).  The reference computes it on the host, and a
+// cell of a 2048- to 16384-column map is so small that calcArea's float
+// result carries rounding noise of ~1e-3 relative which the host's sinf /
+// cosf / atanf decide.  To give the reference's table, the cell areas take
+// the host's sinf and cosf of the grid angles (every argument is pxsz * k,
+// k integer: tables made by the host) and atanf as the double atan rounded
+// to float (which equals the host's atanf on the arguments calcArea
+// produces: checked on every cell of 2048- and sampled cells of 8192- and
+// 16384-column maps), and byte^2.2 the host's powf (a 256-entry table); the
+// float operations are calcArea's, FMA off.
+//
+// Pass 1: one thread per cell writes its four terms into the table.
+__global__ void k_sat_terms(const uint8_t* __restrict__ bgr, int rows, int cols,
+                            const float* __restrict__ sin_t, const float* __restrict__ cos_t,
+                            const float* __restrict__ pow_t, float4* __restrict__ sat) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= cols) return;
-  const float pxsz = PI2 / (1.f * cols);
-  float4 prev = make_float4(0.f, 0.f, 0.f, 0.f);
-  const float phi[4] = {pxsz * q, pxsz * q, pxsz * (q + 1), pxsz * (q + 1)};
-  for (int p = 0; p < rows; p++) {
-    const float theta[4] = {pxsz * (p + 1), pxsz * p, pxsz * p, pxsz * (p + 1)};
-    const float area = calc_area(theta, phi);
+  for (int p = blockIdx.y; p < rows; p += gridDim.y) {
+    // theta = {pxsz (p+1), pxsz p, pxsz p, pxsz (p+1)}, phi = {pxsz q, pxsz q,
+    // pxsz (q+1), pxsz (q+1)}
+    const int it[4] = {p + 1, p, p, p + 1};
+    const int ip[4] = {q, q, q + 1, q + 1};
+    float x[4], y[4], z[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const float sint = sin_t[it[k]];
+      x[k] = sint * cos_t[ip[k]];
+      y[k] = sint * sin_t[ip[k]];
+      z[k] = cos_t[it[k]];
+    }
+    float dotpr1 = 1.f;
+    dotpr1 += x[0] * x[2] + y[0] * y[2] + z[0] * z[2];
+    float dotpr2 = dotpr1;
+    dotpr1 += x[2] * x[1] + y[2] * y[1] + z[2] * z[1];
+    dotpr1 += x[0] * x[1] + y[0] * y[1] + z[0] * z[1];
+    dotpr2 += x[0] * x[3] + y[0] * y[3] + z[0] * z[3];
+    dotpr2 += x[2] * x[3] + y[2] * y[3] + z[2] * z[3];
+    const float triprod1 = fabsf(x[0] * (y[1] * z[2] - y[2] * z[1]) -
+                                 y[0] * (x[1] * z[2] - x[2] * z[1]) +
+                                 z[0] * (x[1] * y[2] - x[2] * y[1]));
+    const float triprod2 = fabsf(x[0] * (y[2] * z[3] - y[3] * z[2]) -
+                                 y[0] * (x[2] * z[3] - x[3] * z[2]) +
+                                 z[0] * (x[2] * y[3] - x[3] * y[2]));
+    const float a1 = (float)atan((double)(triprod1 / dotpr1));
+    const float a2 = (float)atan((double)(triprod2 / dotpr2));
+    const float area = 2.f * (a1 + a2);
     const uint8_t* px = bgr + ((size_t)p * cols + q) * 3;
-    prev.x += powf((float)px[0], 2.2f) * area;
-    prev.y += powf((float)px[1], 2.2f) * area;
-    prev.z += powf((float)px[2], 2.2f) * area;
-    prev.w += area;
+    sat[(size_t)p * cols + q] =
+        make_float4(pow_t[px[0]] * area, pow_t[px[1]] * area, pow_t[px[2]] * area, area);
+  }
+}
+
+// Pass 2: one thread per column adds the terms down the rows in place, in
+// the reference's order.
+__global__ void k_sat_scan(int rows, int cols, float4* __restrict__ sat) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= cols) return;
+  float4 prev = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int p = 0; p < rows; p++) {
+    const float4 t = sat[(size_t)p * cols + q];
+    prev.x += t.x;
+    prev.y += t.y;
+    prev.z += t.z;
+    prev.w += t.w;
     sat[(size_t)p * cols + q] = prev;
   }
 }
@@ -627,8 +676,11 @@ int launch_view_sphere(float2* view, int W, int H, cudaStream_t s) {
   return BT_OK;
 }
 
-int launch_sat(const uint8_t* bgr, int rows, int cols, float4* sat, cudaStream_t s) {
-  k_sat<<<(cols + 127) / 128, 128, 0, s>>>(bgr, rows, cols, sat);
+int launch_sat(const uint8_t* bgr, int rows, int cols, const float* sin_t, const float* cos_t,
+               const float* pow_t, float4* sat, cudaStream_t s) {
+  k_sat_terms<<<dim3((cols + 127) / 128, rows < 65535 ? rows : 65535), 128, 0, s>>>(
+      bgr, rows, cols, sin_t, cos_t, pow_t, sat);
+  k_sat_scan<<<(cols + 127) / 128, 128, 0, s>>>(rows, cols, sat);
   BT_CUDA_TRY(cudaGetLastError());
   return BT_OK;
 }

@@ -3,6 +3,8 @@
 // makeImage / cudaPrep (annemiekie/BlackTracer BT/MakeImageKernel.cu:1206-1559).
 #include <cstring>
 #include <new>
+#include <vector>
+#include <cmath>
 
 #include "bt_internal.h"
 #include "map_internal.h"
@@ -41,7 +43,9 @@ void map_free(bt_map* m) {
                   m->S.area_tmp, m->S.light, m->S.light2, m->S.stars_img,
                   m->S.flag, m->S.cells, m->S.diff_list, m->S.diff_count,
                   m->S.heavy_list, m->S.heavy_order, m->S.heavy_count, m->S.env_wide,
-                  m->S.env_wide_count, m->tmp_img};
+                  m->S.env_wide_count, m->tmp_img, m->S.hv_nn, m->S.hv_nl, m->S.hv_noff,
+                  m->S.hv_uoff, m->S.hv_pool, m->S.hv_pend, m->S.hv_partial, m->S.hv_uany,
+                  m->S.hv_ctl};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (m->side) {
@@ -128,26 +132,43 @@ int bt_env_create(const uint8_t* bgr, int rows, int cols, int bgr_on_device,
     set_error("summed-area table allocation failed: %s", cudaGetErrorString(err));
     return BT_ERR_NOMEM;
   }
+  // The host's sinf / cosf of the grid angles and powf of the byte values
+  // (the reference computes the table on the host: its values are those).
+  const int kmax = rows > cols ? rows : cols;
+  const float pxsz = kPi2F / (1.f * cols);
+  std::vector<float> tabs((size_t)2 * (kmax + 1) + 256);
+  for (int k = 0; k <= kmax; k++) {
+    tabs[k] = sinf(pxsz * k);
+    tabs[(size_t)kmax + 1 + k] = cosf(pxsz * k);
+  }
+  for (int v = 0; v < 256; v++) tabs[(size_t)2 * (kmax + 1) + v] = powf((float)v, 2.2f);
   const uint8_t* src = bgr;
   uint8_t* staged = nullptr;
-  if (!bgr_on_device) {
+  float* dtabs = nullptr;
+  err = cudaMalloc((void**)&dtabs, tabs.size() * sizeof(float));
+  if (err == cudaSuccess)
+    err = cudaMemcpyAsync(dtabs, tabs.data(), tabs.size() * sizeof(float),
+                          cudaMemcpyHostToDevice, s);
+  if (err == cudaSuccess && !bgr_on_device) {
     err = cudaMalloc((void**)&staged, n * 3);
     if (err == cudaSuccess)
       err = cudaMemcpyAsync(staged, bgr, n * 3, cudaMemcpyHostToDevice, s);
-    if (err != cudaSuccess) {
-      if (staged) cudaFree(staged);
-      cudaFree(e->e.sat);
-      delete e;
-      set_error("environment upload failed: %s", cudaGetErrorString(err));
-      return BT_ERR_CUDA;
-    }
     src = staged;
   }
-  int rc = launch_sat(src, rows, cols, e->e.sat, s);
-  if (staged) {
-    cudaStreamSynchronize(s);
-    cudaFree(staged);
+  if (err != cudaSuccess) {
+    if (staged) cudaFree(staged);
+    if (dtabs) cudaFree(dtabs);
+    cudaFree(e->e.sat);
+    delete e;
+    set_error("environment upload failed: %s", cudaGetErrorString(err));
+    return BT_ERR_CUDA;
   }
+  int rc = launch_sat(src, rows, cols, dtabs, dtabs + kmax + 1, dtabs + 2 * (kmax + 1),
+                      e->e.sat, s);
+  // the host tables and staging must outlive the copies and the kernels
+  cudaStreamSynchronize(s);
+  if (staged) cudaFree(staged);
+  cudaFree(dtabs);
   if (rc) {
     cudaFree(e->e.sat);
     delete e;
@@ -326,6 +347,14 @@ int bt_map_render(bt_map* m, const bt_frame* f, void* stream) {
     if (rc) return rc;
   }
   return BT_OK;
+}
+
+int bt_map_set_star_capacity(bt_map* m, size_t nodes, size_t units) {
+  clear_error();
+  BT_ARG_CHECK(m != nullptr, "NULL renderer");
+  BT_ARG_CHECK(units == 0 || units >= 2, "units must be 0 (default) or at least 2");
+  BT_ARG_CHECK(nodes <= 0xffffffffu && units <= 0xffffffffu, "capacity above 2^32 - 1");
+  return map_set_star_capacity(m->S, nodes, units);
 }
 
 int bt_map_diffract(bt_map* m, const bt_stars* stars, const float* light, float* out,

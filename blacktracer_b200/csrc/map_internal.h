@@ -37,6 +37,18 @@ struct MapScratch {
   uint32_t* heavy_list; // pixels deferred to the block-per-pixel star path
   uint32_t* heavy_order;// the same, queued giant-first
   uint32_t* heavy_count;// 4 counters (deferred, giant, other, next item)
+  // deferred pixels in units of candidate leaves (stars.cu, lazy): per
+  // deferred pixel its nodes and leaves, node and unit offsets; the node
+  // pool with the leaves up to each node; per unit its cell sums and whether
+  // it splatted a star; control words
+  uint32_t *hv_nn, *hv_nl, *hv_noff, *hv_uoff;
+  int* hv_pool;
+  uint32_t* hv_pend;
+  float* hv_partial;
+  uint8_t* hv_uany;
+  uint32_t* hv_ctl;
+  size_t hv_node_cap, hv_unit_cap;  // 0: the defaults
+  int hv_fw;
 };
 
 struct StarSet;
@@ -77,6 +89,8 @@ int map_run_stars(MapScratch& S, const MapFrame& F, cudaStream_t s);
 // addDiffraction of a star-light buffer (N*M*3 floats) into out (stars.cu).
 int map_diffract(MapScratch& S, const StarSet& SS, const float* light, float* out,
                  int psf_scale, const float2* view, const float* area, cudaStream_t s);
+// Capacities of the star pass's unit path (stars.cu; 0 = the defaults).
+int map_set_star_capacity(MapScratch& S, size_t nodes, size_t units);
 // The same for a caller's light buffer with a star set's sprite, unscaled.
 int map_diffract_light(MapScratch& S, const bt_stars* stars, const float* light, float* out,
                        cudaStream_t s);
@@ -90,6 +104,10 @@ int map_env_census(const MapScratch& S, int env_rows, unsigned long long* out, c
 int map_star_census(const MapScratch& Sc, const MapFrame& F, unsigned long long* out,
                     cudaStream_t s);
 int launch_view_sphere(float2* view, int W, int H, cudaStream_t s);
-int launch_sat(const uint8_t* bgr, int rows, int cols, float4* sat, cudaStream_t s);
+// Summed-area table from a device BGR8 image; sin_t / cos_t: the host's
+// sinf / cosf of pxsz * k for k = 0..max(rows, cols) (pxsz = 2 pi / cols),
+// pow_t: the host's powf(v, 2.2f) for v = 0..255 (device copies).
+int launch_sat(const uint8_t* bgr, int rows, int cols, const float* sin_t, const float* cos_t,
+               const float* pow_t, float4* sat, cudaStream_t s);
 
 }  // namespace bt

@@ -19,6 +19,10 @@ struct MixedPolicy {
                                                uint8_t& ss) {
     return mixed::begin_ray(p, th, ph, s, to, po, st, ss);
   }
+  static __device__ __forceinline__ void start(const RayParams& p, const plain::RayStart& rs,
+                                               State& s) {
+    mixed::start_ray(p, rs, s);
+  }
   static __device__ __forceinline__ bool attempt(const RayParams& p, State& s) {
     return mixed::attempt(p, s);
   }
@@ -37,6 +41,10 @@ struct FastPolicy {
                                                double& po, int32_t& st,
                                                uint8_t& ss) {
     return fast::begin_ray(p, th, ph, s, to, po, st, ss);
+  }
+  static __device__ __forceinline__ void start(const RayParams& p, const plain::RayStart& rs,
+                                               State& s) {
+    fast::start_ray(p, rs, s);
   }
   static __device__ __forceinline__ bool attempt(const RayParams& p, State& s) {
     return fast::attempt(p, s);

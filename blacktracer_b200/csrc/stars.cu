@@ -271,22 +271,32 @@ k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
 constexpr int kHeavyNodes = 1024;   // nodes per search pass (shared memory)
 // Candidate leaves box-tested per batch of a deferred pixel.
 constexpr int kHeavyBatch = 2048;
-// Deferred pixels with at least this many candidate leaves are scheduled
-// first, so that the longest pixels do not start last.
-constexpr long long kGiantLeaves = 512;
 
-// heavy_count layout: [0] deferred pixels, [1] giant, [2] other, [3] the
-// workers' shared item counter.
+// heavy_count layout: [0] deferred pixels, [1] and [2] the two queues of
+// k_star_heavy (front and back of `order`; the unit path fills only the
+// first, with the pixels that did not fit its node pool), [3] its shared
+// item counter.
 enum { kHcDeferred = 0, kHcGiant = 1, kHcOther = 2, kHcNext = 3, kHcWords = 4 };
 
-// Sorts the deferred pixels into two queues in `order`: giant pixels from
-// the front, the others from the back.
-__global__ void k_heavy_plan(const float2* __restrict__ thphi,
-                             const uint8_t* __restrict__ bh, StarSet S, Cam7 cam,
-                             int M, int step, const float2* __restrict__ view, int lr,
-                             const float* __restrict__ area,
-                             const uint32_t* __restrict__ heavy, uint32_t* hc,
-                             uint32_t* __restrict__ order, uint32_t np) {
+// ---- Deferred pixels in units of candidate leaves ----
+// A deferred pixel's kd-tree search emits nodes; the leaves under them, laid
+// end to end in emission order, are the pixel's candidate leaves.  All
+// deferred pixels' candidate leaves are cut into units of U leaves (one
+// pixel per unit) that warps take from a counter: a pixel of a million
+// candidate stars spreads over every SM instead of holding one block.  Each
+// unit's cell sums go to its own slot, and a last pass adds a pixel's units
+// in unit order, so frames are reproducible.  Pixels whose nodes do not fit
+// the node pool go to the block-per-pixel kernel (k_star_heavy).
+enum { kHvUnits = 0, kHvUnitLeaves = 1, kHvFetch = 2, kHvWords = 4 };
+
+// Pass 1, one thread per deferred pixel: the nodes its search emits and the
+// leaves under them.
+__global__ void k_hv_count(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
+                           StarSet S, Cam7 cam, int M, int step,
+                           const float2* __restrict__ view, int lr,
+                           const float* __restrict__ area, const uint32_t* __restrict__ heavy,
+                           const uint32_t* __restrict__ hc, uint32_t* __restrict__ nn,
+                           uint32_t* __restrict__ nl) {
   const uint32_t n = hc[kHcDeferred];
   const int L = S.treeLevel;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
@@ -294,20 +304,311 @@ __global__ void k_heavy_plan(const float2* __restrict__ thphi,
     const uint32_t ij = heavy[k];
     PixelStars P;
     float mn[2], mx[2];
-    pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, ij / M, ij % M, P, mn, mx);
-    long long leaves = 0;
-    tree_search(S, mn, mx, [&](int node) {
-      leaves += 1ll << (L - node_level(node));
-      return leaves < kGiantLeaves;
-    });
-    if (leaves >= kGiantLeaves) order[atomicAdd(&hc[kHcGiant], 1u)] = ij;
-    else order[np - 1 - atomicAdd(&hc[kHcOther], 1u)] = ij;
+    uint32_t nodes = 0, leaves = 0;
+    if (pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, ij / M, ij % M, P, mn, mx))
+      tree_search(S, mn, mx, [&](int node) {
+        nodes++;
+        leaves += 1u << (L - node_level(node));  // disjoint nodes: at most 2^L leaves
+        return true;
+      });
+    nn[k] = nodes;
+    nl[k] = leaves;
   }
 }
 
-// The deferred pixels, one block at a time each, taken from the queues by a
-// shared counter (giant pixels first); kThreads-thread blocks, several per
-// SM, so that one block's barrier waits overlap another's work.  Thread 0
+// Exclusive scan of one value per thread of a 1024-thread block; *total
+// receives the block's sum.  sh: 32 words of shared memory.
+__device__ __forceinline__ unsigned long long block_scan(unsigned long long v,
+                                                         unsigned long long* sh,
+                                                         unsigned long long* total) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned long long x = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    unsigned long long t = sh[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    sh[lane] = t;
+  }
+  __syncthreads();
+  const unsigned long long before = w ? sh[w - 1] : 0ull;
+  *total = sh[31];
+  __syncthreads();
+  return before + x - v;
+}
+
+// Pass 2, one block: node offsets (noff, n + 1 entries), the unit size and
+// unit offsets (uoff).  The first `ok` pixels are kept: ok is the first
+// pixel whose nodes would end past node_cap, and at most unit_cap / 2; the
+// others go to the fallback queue (order, as k_star_heavy's giant queue)
+// with no nodes and no units.  U = 32 R leaves with R = ceil(kept leaves /
+// (32 (unit_cap - ok))): each pixel's last unit may be partial, so the
+// units number at most kept / U + ok <= unit_cap.
+__global__ void __launch_bounds__(1024)
+k_hv_scan(const uint32_t* __restrict__ heavy, uint32_t* hc, const uint32_t* __restrict__ nn,
+          const uint32_t* __restrict__ nl, uint32_t* __restrict__ noff,
+          uint32_t* __restrict__ uoff, uint32_t* __restrict__ order, uint32_t* ctl,
+          uint32_t node_cap, uint32_t unit_cap) {
+  __shared__ unsigned long long sh[32];
+  __shared__ uint32_t sh_ok, sh_nodes;
+  const uint32_t n = hc[kHcDeferred];
+  // pixels [0, ok) keep their nodes
+  if (threadIdx.x == 0) sh_ok = min(n, unit_cap / 2);
+  unsigned long long base = 0;
+  for (uint32_t c = 0; c < n; c += blockDim.x) {
+    const uint32_t k = c + threadIdx.x;
+    const unsigned long long v = k < n ? nn[k] : 0ull;
+    unsigned long long tot;
+    const unsigned long long off = base + block_scan(v, sh, &tot);
+    if (k < n && off + v > node_cap) atomicMin(&sh_ok, k);
+    base += tot;
+    if (k < n) noff[k] = (uint32_t)(off < node_cap ? off : node_cap);
+  }
+  __syncthreads();
+  const uint32_t ok = sh_ok;
+  // the kept pixels' leaves, and the fallback queue
+  unsigned long long kept = 0;
+  for (uint32_t c = 0; c < n; c += blockDim.x) {
+    const uint32_t k = c + threadIdx.x;
+    const unsigned long long lv = (k < ok) ? nl[k] : 0ull;
+    unsigned long long tot;
+    block_scan(lv, sh, &tot);
+    kept += tot;
+    if (k < n && k >= ok) order[k - ok] = heavy[k];
+  }
+  const unsigned long long slots = 32ull * (unit_cap - ok);  // ok <= unit_cap / 2
+  const unsigned long long U = 32ull * (kept > slots ? (kept + slots - 1) / slots : 1ull);
+  unsigned long long ubase = 0;
+  for (uint32_t c = 0; c < n; c += blockDim.x) {
+    const uint32_t k = c + threadIdx.x;
+    const unsigned long long u = (k < ok) ? (nl[k] + U - 1) / U : 0ull;
+    unsigned long long tot;
+    const unsigned long long off = ubase + block_scan(u, sh, &tot);
+    ubase += tot;
+    if (k < n) uoff[k] = (uint32_t)off;
+  }
+  if (threadIdx.x == 0) sh_nodes = ok > 0 ? noff[ok - 1] + nn[ok - 1] : 0u;
+  __syncthreads();
+  const uint32_t nodes_ok = sh_nodes;
+  for (uint32_t k = ok + threadIdx.x; k <= n; k += blockDim.x) noff[k] = nodes_ok;
+  if (threadIdx.x == 0) {
+    uoff[n] = (uint32_t)ubase;
+    ctl[kHvUnits] = (uint32_t)ubase;
+    ctl[kHvUnitLeaves] = (uint32_t)U;
+    ctl[kHvFetch] = 0;
+    // k_star_heavy takes the fallback pixels as its giant queue
+    hc[kHcGiant] = n - ok;
+    hc[kHcOther] = 0;
+    hc[kHcNext] = 0;
+  }
+}
+
+// Pass 3, one thread per kept deferred pixel: its search again, the nodes
+// into the pool with the leaves up to each (within the pixel).
+__global__ void k_hv_nodes(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
+                           StarSet S, Cam7 cam, int M, int step,
+                           const float2* __restrict__ view, int lr,
+                           const float* __restrict__ area, const uint32_t* __restrict__ heavy,
+                           const uint32_t* __restrict__ hc, const uint32_t* __restrict__ noff,
+                           int* __restrict__ pool, uint32_t* __restrict__ pend) {
+  const uint32_t n = hc[kHcDeferred];
+  const int L = S.treeLevel;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += gridDim.x * blockDim.x) {
+    const uint32_t b0 = noff[k], b1 = noff[k + 1];
+    if (b0 == b1) continue;
+    const uint32_t ij = heavy[k];
+    PixelStars P;
+    float mn[2], mx[2];
+    pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, ij / M, ij % M, P, mn, mx);
+    uint32_t e = b0, cum = 0;
+    tree_search(S, mn, mx, [&](int node) {
+      if (e >= b1) return false;  // the same search as pass 1: never taken
+      cum += 1u << (L - node_level(node));
+      pool[e] = node;
+      pend[e] = cum;
+      e++;
+      return true;
+    });
+  }
+}
+
+// Pass 4: warps take units.  A unit is leaves [f0, f0 + U) of its pixel's
+// candidate leaves; lane l box-tests leaf f0 + 32 r + l, the warp sweeps the
+// survivors' stars 32 at a time, queues the hits and splats them 32 at a
+// time, one per lane, into the lane's cell registers (the per-star form of
+// the brightness, star_fast); the warp's sums go to the unit's slot.
+template <int kStep>
+__global__ void __launch_bounds__(256)
+k_star_units(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh, StarSet S,
+             Cam7 cam, int M, const float2* __restrict__ view, int lr,
+             const float* __restrict__ area, const uint32_t* __restrict__ heavy,
+             const uint32_t* __restrict__ hc, const uint32_t* __restrict__ noff,
+             const uint32_t* __restrict__ uoff, const int* __restrict__ pool,
+             const uint32_t* __restrict__ pend, uint32_t* ctl, float* __restrict__ partial,
+             uint8_t* __restrict__ uany) {
+  constexpr int FW = 2 * kStep + 1, FW2 = FW * FW;
+  constexpr int kWarps = 256 / 32;
+  __shared__ int sh_q[kWarps][64];
+  __shared__ float2 sh_qpos[kWarps][64];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int L = S.treeLevel;
+  const uint32_t n = hc[kHcDeferred];
+  const uint32_t total = ctl[kHvUnits];
+  const uint32_t U = ctl[kHvUnitLeaves];
+  for (;;) {
+    uint32_t u = 0;
+    if (lane == 0) u = atomicAdd(&ctl[kHvFetch], 1u);
+    u = __shfl_sync(0xffffffffu, u, 0);
+    if (u >= total) break;
+    // the unit's pixel: the last k with uoff[k] <= u (pixels without units
+    // share their offset with the next pixel)
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi + 1) >> 1;
+      if (uoff[mid] <= u) lo = mid;
+      else hi = mid - 1;
+    }
+    const uint32_t k = lo;
+    const uint32_t ij = heavy[k];
+    PixelStars P;
+    float mn[2], mx[2];
+    pixel_setup(thphi, bh, cam.v, M, kStep, view, lr, area, ij / M, ij % M, P, mn, mx);
+    const uint32_t n0 = noff[k], n1 = noff[k + 1];
+    const uint32_t f0 = (u - uoff[k]) * U;
+    const uint32_t f1 = min(f0 + U, pend[n1 - 1]);
+    float3 acc[FW2];
+#pragma unroll
+    for (int c = 0; c < FW2; c++) acc[c] = make_float3(0.f, 0.f, 0.f);
+    int any = 0, qn = 0;
+    auto splat_queued = [&](int q_at) {
+      const int q = sh_q[w][q_at];
+      const float2 pos = sh_qpos[w][q_at];
+      const StarHit h = star_hit(P, S, q, pos.x, pos.y);
+      const StarFast f = star_fast(P, S, h);
+#pragma unroll
+      for (int c = 0; c < FW2; c++) {
+        float3 l;
+        if (cell_light_fast(P, h, f, c / FW, c % FW, l)) {
+          acc[c].x += l.x;
+          acc[c].y += l.y;
+          acc[c].z += l.z;
+        }
+      }
+    };
+    for (uint32_t f = f0; f < f1; f += 32) {
+      const uint32_t kk = f + lane;
+      int leaf = -1;
+      if (kk < f1) {
+        uint32_t a = n0, b = n1 - 1;  // first node whose leaves reach past kk
+        while (a < b) {
+          const uint32_t mid = (a + b) >> 1;
+          if (pend[mid] > kk) b = mid;
+          else a = mid + 1;
+        }
+        const int node = pool[a];
+        const int d = L - node_level(node);
+        const uint32_t start = a > n0 ? pend[a - 1] : 0u;
+        leaf = (int)((((long long)node + 1) << d) - 1 + (kk - start));
+        if (node_excluded(P, S.box[leaf])) leaf = -1;
+      }
+      unsigned keep = __ballot_sync(0xffffffffu, leaf >= 0);
+      while (keep) {
+        const int src = __ffs(keep) - 1;
+        keep &= keep - 1;
+        const int lf = __shfl_sync(0xffffffffu, leaf, src);
+        int a0, a1;
+        node_range(S, lf, a0, a1);
+        for (int qb = a0; qb < a1; qb += 32) {
+          const int q = qb + lane;
+          float st = 0.f, sp = 0.f;
+          const bool in = q < a1 && star_test(P, S, q, st, sp);
+          const unsigned ball = __ballot_sync(0xffffffffu, in);
+          if (!ball) continue;
+          any = 1;
+          if (in) {
+            const int at = qn + __popc(ball & ((1u << lane) - 1u));
+            sh_q[w][at] = q;
+            sh_qpos[w][at] = make_float2(st, sp);
+          }
+          qn += __popc(ball);
+          if (qn >= 32) {
+            __syncwarp();
+            splat_queued(lane);
+            __syncwarp();
+            if (lane < qn - 32) {
+              sh_q[w][lane] = sh_q[w][lane + 32];
+              sh_qpos[w][lane] = sh_qpos[w][lane + 32];
+            }
+            qn -= 32;
+            __syncwarp();
+          }
+        }
+      }
+    }
+    __syncwarp();
+    if (lane < qn) splat_queued(lane);
+    __syncwarp();
+    float* out = partial + (size_t)u * (FW2 * 3);
+#pragma unroll
+    for (int c = 0; c < FW2; c++) {
+      float x = acc[c].x, y = acc[c].y, z = acc[c].z;
+      for (int o = 16; o > 0; o >>= 1) {
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+        y += __shfl_xor_sync(0xffffffffu, y, o);
+        z += __shfl_xor_sync(0xffffffffu, z, o);
+      }
+      if (lane == 0) {
+        out[3 * c] = x;
+        out[3 * c + 1] = y;
+        out[3 * c + 2] = z;
+      }
+    }
+    if (lane == 0) uany[u] = any ? 1 : 0;
+  }
+}
+
+// Pass 5, one warp per deferred pixel with units: its cells are the sums of
+// its units' slots in unit order (lane c adds component c), its flag whether
+// any unit splatted a star.
+template <int kStep>
+__global__ void k_star_units_sum(const uint32_t* __restrict__ heavy,
+                                 const uint32_t* __restrict__ hc,
+                                 const uint32_t* __restrict__ uoff,
+                                 const float* __restrict__ partial,
+                                 const uint8_t* __restrict__ uany, float* __restrict__ cells,
+                                 uint8_t* __restrict__ flag) {
+  constexpr int FW = 2 * kStep + 1, C = FW * FW * 3;
+  const uint32_t n = hc[kHcDeferred];
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); k < n; k += warps) {
+    const uint32_t u0 = uoff[k], u1 = uoff[k + 1];
+    if (u0 == u1) continue;  // no candidates, or a fallback pixel
+    int a = 0;
+    for (uint32_t u = u0 + lane; u < u1; u += 32) a |= uany[u];
+    const bool any = __any_sync(0xffffffffu, a != 0);
+    const uint32_t ij = heavy[k];
+    if (any)
+      for (int c = lane; c < C; c += 32) {
+        float v = 0.f;
+        for (uint32_t u = u0; u < u1; u++) v += partial[(size_t)u * C + c];
+        cells[(size_t)ij * C + c] = v;
+      }
+    if (lane == 0) flag[ij] = any ? 1 : 0;
+  }
+}
+
+// Deferred pixels that did not fit the unit path's node pool, one block at a
+// time each, taken from the queues by a shared counter; kThreads-thread
+// blocks.  Thread 0
 // walks the kd-tree (in passes of kHeavyNodes emitted nodes) into shared
 // memory with a prefix sum of the number of leaves under each node.  The
 // block then takes that flat range of candidate leaves kHeavyBatch at a time:
@@ -532,6 +833,75 @@ __global__ void k_blackbody_tables_1k(float4* __restrict__ bb) {
 // Threads per block of k_star_heavy; the launch fills the SMs with as many
 // blocks as are resident at once.
 constexpr int kHeavyThreads = 512;
+
+// Buffers of the unit path (lazy): per-pixel counts and offsets, the node
+// pool (max(2^21, N*M) entries) and the unit slots (max(2^18, N*M/8) units
+// of (2s+1)^2 cells), sized for splat width fw.
+static int ensure_units(MapScratch& Sc, int fw) {
+  const size_t np = (size_t)Sc.M * Sc.N;
+  if (Sc.hv_ctl && Sc.hv_fw >= fw) return BT_OK;
+  cudaFree(Sc.hv_nn); cudaFree(Sc.hv_nl); cudaFree(Sc.hv_noff); cudaFree(Sc.hv_uoff);
+  cudaFree(Sc.hv_pool); cudaFree(Sc.hv_pend); cudaFree(Sc.hv_partial); cudaFree(Sc.hv_uany);
+  cudaFree(Sc.hv_ctl);
+  Sc.hv_nn = Sc.hv_nl = Sc.hv_noff = Sc.hv_uoff = Sc.hv_pend = Sc.hv_ctl = nullptr;
+  Sc.hv_pool = nullptr;
+  Sc.hv_partial = nullptr;
+  Sc.hv_uany = nullptr;
+  Sc.hv_fw = 0;
+  if (!Sc.hv_node_cap) Sc.hv_node_cap = std::max<size_t>((size_t)1 << 21, np);
+  if (!Sc.hv_unit_cap) Sc.hv_unit_cap = std::max<size_t>((size_t)1 << 18, np / 8);
+  cudaError_t e = cudaSuccess;
+#define HV_ALLOC(p, bytes) \
+  if (e == cudaSuccess) e = cudaMalloc((void**)&(p), (bytes));
+  HV_ALLOC(Sc.hv_nn, np * sizeof(uint32_t));
+  HV_ALLOC(Sc.hv_nl, np * sizeof(uint32_t));
+  HV_ALLOC(Sc.hv_noff, (np + 1) * sizeof(uint32_t));
+  HV_ALLOC(Sc.hv_uoff, (np + 1) * sizeof(uint32_t));
+  HV_ALLOC(Sc.hv_pool, Sc.hv_node_cap * sizeof(int));
+  HV_ALLOC(Sc.hv_pend, Sc.hv_node_cap * sizeof(uint32_t));
+  HV_ALLOC(Sc.hv_partial, Sc.hv_unit_cap * fw * fw * 3 * sizeof(float));
+  HV_ALLOC(Sc.hv_uany, Sc.hv_unit_cap);
+  HV_ALLOC(Sc.hv_ctl, kHvWords * sizeof(uint32_t));
+#undef HV_ALLOC
+  if (e != cudaSuccess) {
+    set_error("star unit scratch allocation failed: %s", cudaGetErrorString(e));
+    return BT_ERR_NOMEM;
+  }
+  Sc.hv_fw = fw;
+  return BT_OK;
+}
+
+// Capacities of the unit path (0: the defaults); its buffers are released
+// and reserved again at the next frame.
+int map_set_star_capacity(MapScratch& Sc, size_t nodes, size_t units) {
+  BT_CUDA_TRY(cudaDeviceSynchronize());
+  cudaFree(Sc.hv_nn); cudaFree(Sc.hv_nl); cudaFree(Sc.hv_noff); cudaFree(Sc.hv_uoff);
+  cudaFree(Sc.hv_pool); cudaFree(Sc.hv_pend); cudaFree(Sc.hv_partial); cudaFree(Sc.hv_uany);
+  cudaFree(Sc.hv_ctl);
+  Sc.hv_nn = Sc.hv_nl = Sc.hv_noff = Sc.hv_uoff = Sc.hv_pend = Sc.hv_ctl = nullptr;
+  Sc.hv_pool = nullptr;
+  Sc.hv_partial = nullptr;
+  Sc.hv_uany = nullptr;
+  Sc.hv_fw = 0;
+  Sc.hv_node_cap = nodes;
+  Sc.hv_unit_cap = units;
+  return BT_OK;
+}
+
+template <int kStep>
+void launch_units(MapScratch& Sc, const MapFrame& F, const StarSet& SS, cudaStream_t s) {
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_star_units<kStep>, 256, 0);
+    if (per_sm < 1) per_sm = 1;
+  }
+  k_star_units<kStep><<<sm_count() * per_sm, 256, 0, s>>>(
+      Sc.thphi, Sc.bh, SS, F.cam, Sc.M, F.view, F.lr, Sc.area, Sc.heavy_list, Sc.heavy_count,
+      Sc.hv_noff, Sc.hv_uoff, Sc.hv_pool, Sc.hv_pend, Sc.hv_ctl, Sc.hv_partial, Sc.hv_uany);
+  k_star_units_sum<kStep><<<sm_count() * 4, 256, 0, s>>>(
+      Sc.heavy_list, Sc.heavy_count, Sc.hv_uoff, Sc.hv_partial, Sc.hv_uany, (float*)Sc.cells,
+      Sc.flag);
+}
 
 template <int kStep>
 void launch_heavy(MapScratch& Sc, const MapFrame& F, const StarSet& SS, cudaStream_t s) {
@@ -1009,19 +1379,31 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   const int M = Sc.M, N = Sc.N;
   const StarSet SS = stars_for_frame(F.stars, F.bb_table);
   const int fw = 2 * F.step + 1;
-  const size_t np = (size_t)M * N;
-  if (int rc = ensure_cells(Sc, fw)) return rc;
   if (F.step > 2) {
     set_error("star splat step > 2 is not supported");
     return BT_ERR_ARG;
   }
+  if (int rc = ensure_cells(Sc, fw)) return rc;
+  if (int rc = ensure_units(Sc, fw)) return rc;
   BT_CUDA_TRY(cudaMemsetAsync(Sc.heavy_count, 0, kHcWords * sizeof(uint32_t), s));
   k_star_cells<<<grid2(M, N), dim3(TX, TY), 0, s>>>(
       Sc.thphi, Sc.bh, SS, F.cam, M, N, F.step, F.view, F.lr, Sc.area,
       Sc.cells, Sc.flag, Sc.heavy_list, Sc.heavy_count + kHcDeferred);
-  k_heavy_plan<<<sm_count() * 2, 128, 0, s>>>(
-      Sc.thphi, Sc.bh, SS, F.cam, M, F.step, F.view, F.lr, Sc.area, Sc.heavy_list,
-      Sc.heavy_count, Sc.heavy_order, (uint32_t)np);
+  // deferred pixels: in units of candidate leaves, the pixels past the node
+  // pool in k_star_heavy
+  k_hv_count<<<sm_count() * 2, 128, 0, s>>>(Sc.thphi, Sc.bh, SS, F.cam, M, F.step, F.view,
+                                            F.lr, Sc.area, Sc.heavy_list, Sc.heavy_count,
+                                            Sc.hv_nn, Sc.hv_nl);
+  k_hv_scan<<<1, 1024, 0, s>>>(Sc.heavy_list, Sc.heavy_count, Sc.hv_nn, Sc.hv_nl, Sc.hv_noff,
+                               Sc.hv_uoff, Sc.heavy_order, Sc.hv_ctl,
+                               (uint32_t)std::min<size_t>(Sc.hv_node_cap, 0xffffffffu),
+                               (uint32_t)std::min<size_t>(Sc.hv_unit_cap, 0xffffffffu));
+  k_hv_nodes<<<sm_count() * 2, 128, 0, s>>>(Sc.thphi, Sc.bh, SS, F.cam, M, F.step, F.view,
+                                            F.lr, Sc.area, Sc.heavy_list, Sc.heavy_count,
+                                            Sc.hv_noff, Sc.hv_pool, Sc.hv_pend);
+  if (F.step == 0) launch_units<0>(Sc, F, SS, s);
+  else if (F.step == 1) launch_units<1>(Sc, F, SS, s);
+  else launch_units<2>(Sc, F, SS, s);
   if (F.step == 0) launch_heavy<0>(Sc, F, SS, s);
   else if (F.step == 1) launch_heavy<1>(Sc, F, SS, s);
   else launch_heavy<2>(Sc, F, SS, s);

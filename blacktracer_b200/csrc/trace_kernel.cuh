@@ -13,6 +13,7 @@
 #pragma once
 
 #include "bt_internal.h"
+#include "kerr_plain.cuh"
 
 namespace bt {
 
@@ -46,9 +47,68 @@ __device__ __forceinline__ int queue_grid(const uint32_t* __restrict__ qoff, int
   return lo;
 }
 
-// Traces the listed vertices of G grids into their lattices.  Queue entry k
-// is vertex trace[k - qoff[g]] of grid g; each grid's rays use that grid's
-// camera and spin (D[g].p).
+// Vertex key of queue entry k: the front segment (n_hot entries) of grid
+// g's trace list, then its back one.
+__device__ __forceinline__ uint32_t queue_key(const GridDesc& d, uint32_t r) {
+  const uint32_t nh = *(volatile const uint32_t*)&d.ctr->n_hot;
+  return r < nh ? d.trace[r] : d.trace[(uint32_t)d.L.N * (uint32_t)d.L.M - 1u - (r - nh)];
+}
+
+// Set-up pass of a level: the set-up and capture test of every listed ray
+// (ray_setup + checkCelest, BT/Grid.h:524-552), one thread each, so that the
+// trace kernel's lanes only integrate.  A ray that must be integrated leaves
+// its start in the grid's T-vertex buffers (free until the T-vertex fix
+// runs): (p_r, p_theta) in X[0], (b, q) in X[1], and its photon-orbit radius
+// as float in its steps slot (overwritten when it finishes); any other ray
+// (captured, Newton cap, maxstp 0) is final here and marked traced.
+template <class Policy>
+__global__ void __launch_bounds__(128)
+k_setup_lattice(const GridDesc* __restrict__ D, int G, const uint32_t* __restrict__ qoff) {
+  const uint32_t n = qoff[G];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += gridDim.x * blockDim.x) {
+    const int g = queue_grid(qoff, G, k);
+    const GridDesc& d = D[g];
+    const uint32_t key = queue_key(d, k - qoff[g]);
+    double th, ph, to, po;
+    int32_t s;
+    uint8_t ss;
+    lattice_seed(d.L, key, th, ph);
+    plain::RayStart rs;
+    const bool go = plain::setup_ray(d.p, th, ph, rs, to, po, s, ss);
+    if (go && d.p.maxstp > 0) {
+      d.X[0][key] = make_double2(rs.pR, rs.pTheta);
+      d.X[1][key] = make_double2(rs.b, rs.q);
+      reinterpret_cast<float*>(d.L.steps)[key] = (float)rs.r0;
+    } else {
+      if (go) {  // maxstp 0: odeint1's loop does not run (BT/Metric.h:283)
+        typename Policy::State st;
+        Policy::start(d.p, rs, st);
+        Policy::finish(d.p, st, to, po, s, ss);
+      }
+      d.L.thphi[key] = make_double2(to, po);
+      d.L.steps[key] = s;
+      d.L.vstat[key] = ss;
+      d.L.vflag[key] = 1;
+    }
+  }
+}
+
+// The start a set-up pass left for the ray of vertex key.
+__device__ __forceinline__ plain::RayStart lattice_start(const GridDesc& d, uint32_t key) {
+  const double2 a = d.X[0][key], b = d.X[1][key];
+  plain::RayStart rs;
+  rs.pR = a.x;
+  rs.pTheta = a.y;
+  rs.b = b.x;
+  rs.q = b.y;
+  rs.r0 = (double)reinterpret_cast<const float*>(d.L.steps)[key];
+  return rs;
+}
+
+// Traces the listed vertices of G grids into their lattices, after their
+// set-up pass.  Queue entry k is vertex trace[k - qoff[g]] of grid g; each
+// grid's rays use that grid's camera and spin (D[g].p).
 template <class Policy, int kThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
 k_trace_lattice(const GridDesc* __restrict__ D, int G,
@@ -74,26 +134,11 @@ k_trace_lattice(const GridDesc* __restrict__ D, int G,
         if (k < n) {
           g = queue_grid(qoff, G, k);
           const GridDesc& d = D[g];
-          // the front segment (n_hot entries), then the back one
-          const uint32_t r = k - qoff[g];
-          const uint32_t nh = *(volatile const uint32_t*)&d.ctr->n_hot;
-          key = r < nh ? d.trace[r]
-                       : d.trace[(uint32_t)d.L.N * (uint32_t)d.L.M - 1u - (r - nh)];
-          double th, ph, to, po;
-          int32_t s;
-          uint8_t ss;
-          lattice_seed(d.L, key, th, ph);
-          // a ray past the capture test takes its attempts (none when
-          // maxstp is 0: odeint1's loop, BT/Metric.h:283, does not run)
-          const bool go = Policy::begin(d.p, th, ph, st, to, po, s, ss);
-          if (go && d.p.maxstp > 0) {
+          key = queue_key(d, k - qoff[g]);
+          // rays the set-up pass finished need nothing more
+          if (d.L.vflag[key] != 1) {
+            Policy::start(d.p, lattice_start(d, key), st);
             slot = k;
-          } else {
-            if (go) Policy::finish(d.p, st, to, po, s, ss);
-            d.L.thphi[key] = make_double2(to, po);
-            d.L.steps[key] = s;
-            d.L.vstat[key] = ss;
-            d.L.vflag[key] = 1;
           }
         } else {
           slot = kLaneDone;
@@ -118,8 +163,8 @@ k_trace_lattice(const GridDesc* __restrict__ D, int G,
   }
 }
 
-// Launch of k_trace_lattice: one block per SM times the requested (or the
-// largest resident) number of blocks.  128-thread blocks come in three
+// Launch of a level's set-up pass and of k_trace_lattice: one block per SM
+// times the requested (or the largest resident) number of blocks.  128-thread blocks come in three
 // register budgets -- as compiled (3 blocks per SM), capped for 4 and for 5
 // resident blocks (with a few spills) -- picked by blocks_per_sm 0-3, 4, 5+.
 template <class Policy>
@@ -134,6 +179,7 @@ int launch_trace_shape(const GridDesc* D, int G, const uint32_t* qoff,
     }
     int per_sm = per_sm_max;
     if (shape.blocks_per_sm > 0 && shape.blocks_per_sm < per_sm) per_sm = shape.blocks_per_sm;
+    k_setup_lattice<Policy><<<sm_count() * 8, 128, 0, s>>>(D, G, qoff);
     kernel<<<sm_count() * per_sm, threads, 0, s>>>(D, G, qoff, qfetch);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

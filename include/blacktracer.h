@@ -459,6 +459,17 @@ int bt_psf_airy(int size, float first_zero, uint8_t* rgb);
 int bt_psf_levels(const uint8_t* psf_rgb, int psf_size, int level, int16_t* offsets,
                   float* values, int capacity, int* count);
 
+/* Diagnostic: the capacities of the star pass's deferred-pixel units (no
+ * counterpart in the reference).  Pixels whose stars exceed the per-pixel
+ * budget of the main star pass are cut into units of candidate kd-tree
+ * leaves that all SMs share; `nodes` (default max(2^21, W*H)) bounds the
+ * kd-tree nodes of those pixels' searches held at once, `units` (default
+ * max(2^18, W*H/8), at least 2) the units, whose size grows to fit.
+ * Pixels past either bound are rendered one block per pixel instead.  0
+ * keeps a default.  Synchronises the device; no frame of m may be in
+ * flight. */
+int bt_map_set_star_capacity(bt_map* m, size_t nodes, size_t units);
+
 /* addDiffraction (BT/MakeImageKernel.cu:775-800) on a caller's star-light
  * buffer: light and out are DEVICE arrays of width*height*3 floats (the
  * renderer's size; the summed star light sumStarLight produces), different
