@@ -529,13 +529,15 @@ def ref_map_sat(bgr):
 
 def ref_map_frame_rows(grid_f2, grid_rows, grid_cols, gridlvl, view, width, height, cam7,
                        rows, sat=None, env_shape=None, stars=None, step=1, lr=True,
-                       nthreads=0):
+                       nthreads=0, area=None):
     """One frame through the reference's own map kernels on host threads
     (btref_map_frame_rows): corners, black-hole mask and smoothed solid angles
     of the whole frame, and the environment, star and composite colours of the
     listed rows.  sat = ref_map_sat(bgr) with env_shape = (rows, cols), or
-    None; stars = (pos, mag, tree, level) or None.  Returns dict(thphi, gap,
-    bh, area, env, stars, image) with the row images as (len(rows), W, 4)."""
+    None; stars = (pos, mag, tree, level) or None; area: (H*W,) smoothed solid
+    angles for the colour passes to use instead of the harness's own (the
+    returned `area` is the harness's).  Returns dict(thphi, gap, bh, area,
+    env, stars, image) with the row images as (len(rows), W, 4)."""
     lib = _refmaplib()
     M, N = width, height
     rows = np.ascontiguousarray(rows, dtype=np.int32)
@@ -562,7 +564,8 @@ def ref_map_frame_rows(grid_f2, grid_rows, grid_cols, gridlvl, view, width, heig
     thphi = np.zeros(((N + 1) * (M + 1), 2), np.float32)
     gap = np.zeros((N + 1) * (M + 1), np.int32)
     bh = np.zeros(N * M, np.uint8)
-    area = np.zeros(N * M, np.float32)
+    area_out = np.zeros(N * M, np.float32)
+    area_keep = None if area is None else np.ascontiguousarray(area, np.float32).reshape(-1)
     env = np.zeros((nr, M, 4), np.uint8) if sat is not None else None
     simg = np.zeros((nr, M, 4), np.uint8) if stars is not None else None
     img = np.zeros((nr, M, 4), np.uint8) if (sat is not None and stars is not None) else None
@@ -570,7 +573,7 @@ def ref_map_frame_rows(grid_f2, grid_rows, grid_cols, gridlvl, view, width, heig
     lib.btref_map_frame_rows.argtypes = [
         _f32p, C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int, vp, C.c_int, C.c_int,
         vp, vp, C.c_int, vp, C.c_int, _f32p, C.c_int, C.c_int, _i32, C.c_int, C.c_int,
-        _f32p, _i32, _u8p, _f32p, vp, vp, vp]
+        _f32p, _i32, _u8p, _f32p, vp, vp, vp, vp]
     lib.btref_map_frame_rows.restype = C.c_int
     ptr = lambda a: None if a is None else C.c_void_p(a.ctypes.data)  # noqa: E731
     rc = lib.btref_map_frame_rows(
@@ -578,10 +581,12 @@ def ref_map_frame_rows(grid_f2, grid_rows, grid_cols, gridlvl, view, width, heig
         C.c_void_p(g.ctypes.data + pad * grid_cols * 8), grid_cols, grid_rows, gridlvl,
         sat_ptr, er, ec, sptr[0], sptr[1], sptr[2], sptr[3], sptr[4],
         np.ascontiguousarray(cam7, np.float32), step, int(lr), rows, nr, nthreads,
-        thphi, gap, bh, area, ptr(env), ptr(simg), ptr(img))
+        thphi, gap, bh, area_out,
+        None if area is None else C.c_void_p(area_keep.ctypes.data), ptr(env), ptr(simg),
+        ptr(img))
     if rc != 0:
         raise RuntimeError("reference frame rows failed (scratch reservation)")
-    return dict(thphi=thphi, gap=gap, bh=bh, area=area, env=env, stars=simg, image=img)
+    return dict(thphi=thphi, gap=gap, bh=bh, area=area_out, env=env, stars=simg, image=img)
 
 
 def ref_map_time(grid_f2, grid_rows, grid_cols, gridlvl, view, width, height, cam7, sat,

@@ -387,8 +387,9 @@ int btref_map_time(const float* view, int M, int N, const float* grid, int GM, i
 // distortEnvironmentMap, and distortStarMap over the rows within `step` of a
 // listed row followed by sumStarLight, makePix and addStarsAndBackground on
 // the listed rows.  env_rows / star_rows / img_rows: nr x M BGRA8 (any may be
-// NULL; img_rows needs both passes).  sat and grid are padded as for
-// btref_map_time.  Rows of the star pass run in chunks; chunks next to each
+// NULL; img_rows needs both passes).  area_in (may be NULL): smoothed solid
+// angles the colour passes use instead of the ones computed here (area_out
+// still receives these).  sat and grid are padded as for btref_map_time.  Rows of the star pass run in chunks; chunks next to each
 // other never run at the same time, so searchTree's writes past a pixel's
 // slots (into the next pixel's) land where only the same thread reads.
 // Returns 0, or -1 if scratch memory could not be reserved.
@@ -398,8 +399,8 @@ int btref_map_frame_rows(const float* view, int M, int N, const float* grid, int
                          int treeLevel, const float* cam7, int step, int lr,
                          const int* rows, int nr, int nthreads, float* thphi_out,
                          int* gap_out, unsigned char* bh_out, float* area_out,
-                         unsigned char* env_rows_out, unsigned char* star_rows_out,
-                         unsigned char* img_rows_out) {
+                         const float* area_in, unsigned char* env_rows_out,
+                         unsigned char* star_rows_out, unsigned char* img_rows_out) {
   if (nthreads > 0) omp_set_num_threads(nthreads);
   float2* thphi = (float2*)thphi_out;
 #pragma omp parallel for schedule(dynamic, 2)
@@ -431,6 +432,7 @@ int btref_map_frame_rows(const float* view, int M, int N, const float* grid, int
       at(i, j);
       smoothAreaV(areaS.data(), area_out, bh_out, gap_out, M, N);
     }
+  const float* area_use = area_in ? area_in : area_out;
   // distortEnvironmentMap writes out[ij]: a full-frame buffer reserved lazily
   Lazy<uchar4> env_img((size_t)N * M);
   if (!env_img.p) return -1;
@@ -441,7 +443,7 @@ int btref_map_frame_rows(const float* view, int M, int N, const float* grid, int
       for (int j = 0; j < M; j++) {
         at(rows[r], j);
         distortEnvironmentMap(thphi, env_img.p, bh_out, imsize, M, N, 0.f, (float4*)sat,
-                              cam7, 0, nullptr, area_out, (float2*)view, lr != 0);
+                              cam7, 0, nullptr, area_use, (float2*)view, lr != 0);
       }
     if (env_rows_out)
       for (int r = 0; r < nr; r++)
@@ -491,7 +493,7 @@ int btref_map_frame_rows(const float* view, int M, int N, const float* grid, int
             at(i, j);
             distortStarMap(scratch.p, thphi, bh_out, stars, tree, starSize, cam7, mag, treeLevel,
                            M, N, step, 0.f, search.p, searchNr, stCache.p, stnums.p, trail.p,
-                           trailnum, grad.p, 0, (const float2*)view, lr != 0, area_out);
+                           trailnum, grad.p, 0, (const float2*)view, lr != 0, area_use);
           }
     }
 #pragma omp parallel for schedule(dynamic, 1)

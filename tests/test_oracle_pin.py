@@ -114,3 +114,12 @@ def test_ref_frame_rows_equal_whole_frame(oracle_mod):
         assert np.array_equal(r["env"], ref["env"].reshape(H, W, 4)[sel])
         assert np.array_equal(r["stars"], ref["stars"].reshape(H, W, 4)[sel])
         assert np.array_equal(r["image"], ref["image"].reshape(H, W, 4)[sel])
+    # solid angles passed in are the ones the colour passes use
+    r2 = oracle_mod.ref_map_frame_rows(grid, rows, GM, ml, view, W, H, cam7, sel, sat=sat,
+                                       env_shape=bgr.shape[:2], stars=(pos, mg, tree, tl),
+                                       lr=True, nthreads=4, area=ref["area"])
+    assert np.array_equal(r2["image"], r["image"])
+    r3 = oracle_mod.ref_map_frame_rows(grid, rows, GM, ml, view, W, H, cam7, sel, sat=sat,
+                                       env_shape=bgr.shape[:2], lr=True, nthreads=4,
+                                       area=ref["area"] * np.float32(1.5))
+    assert not np.array_equal(r3["env"], r["env"])
