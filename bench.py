@@ -96,6 +96,53 @@ def batch_poses(bt, count=BATCH["count"], seed=BATCH["seed"]):
             for k in range(count)], [float(x) for x in a]
 
 
+def latency_floor(bt, torch, grid, d, cam, prec, reps=5):
+    """The build's latency floor: each refinement level waits for its longest
+    ray, so a level-synchronous build takes at least the sum over levels of
+    the time the level's longest ray takes alone.  Each such ray (the one
+    with the most steps among the level's integrated vertices; a vertex
+    belongs to the level at which its lattice position first appears) is
+    integrated alone through bt_integrate_rays, the best of `reps` runs."""
+    N, M = grid.N, grid.M
+    ml, sl = grid.MAXLEVEL, grid.STARTLVL
+    ii = torch.arange(N, device="cuda")[:, None].expand(N, M)
+    jj = torch.arange(M, device="cuda")[None, :].expand(N, M)
+
+    def tz(x):
+        t = torch.zeros_like(x)
+        for b in range(ml - sl):
+            t += ((x % (2 << b)) == 0).to(x.dtype)
+        return t
+    lvl = ml - torch.minimum(torch.minimum(tz(ii), tz(jj)), torch.full_like(ii, ml - sl))
+    live = (d["exists"] == 1) & (d["status"] != 1)
+    st = torch.where(live, d["steps"].to(torch.int64), torch.full_like(ii, -1))
+    stream = torch.cuda.current_stream()
+    levels, total_ms, attempts = [], 0.0, 0
+    for level in range(sl, ml + 1):
+        s_l = torch.where(lvl == level, st, torch.full_like(st, -1))
+        k = int(torch.argmax(s_l))
+        if int(s_l.view(-1)[k]) < 0:
+            continue
+        i, j = k // M, k % M
+        th = torch.tensor([i / (N - 1) * np.pi], dtype=torch.float64, device="cuda")
+        ph = torch.tensor([j / M * 2 * np.pi], dtype=torch.float64, device="cuda")
+        best = 1e30
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            bt.integrate_rays(cam, th, ph, opts=prec)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        n_att = int(s_l.view(-1)[k]) + 1
+        levels.append({"level": level, "attempts": n_att, "alone_ms": best})
+        total_ms += best
+        attempts += n_att
+    return {"floor_ms": total_ms, "critical_path_attempts": attempts,
+            "us_per_attempt_alone": total_ms * 1e3 / max(1, attempts), "levels": levels}
+
+
 def set_error_vs(Sp, Sm):
     """Per-vertex angular difference of a mixed set against the plain set
     (vertices both hold and both traced to the sky), p99 and max, and whether
@@ -507,6 +554,7 @@ def main():
     traced = int(grid.info().traced)
     flops_build = float(((st_all[integrated] + 1).sum().item()) * F_ATTEMPT_FORM[prec_main] +
                         traced * F_SETUP)
+    latency = latency_floor(bt, torch, grid, d, cam, prec_main)
     del d, steps, st_all, integrated
 
     for _ in range(args.warmup):
@@ -636,7 +684,13 @@ def main():
                                "(bt_probe_fp64_tflops); MEASURED_PEAKS.json has no FP64 entry",
                 "flops_per_build": flops_build, "trace_ms_per_build": trace_ms / args.steps,
                 "launches_per_build": launches / args.steps,
-                "avg_launch_ms": per_launch_ms}
+                "avg_launch_ms": per_launch_ms,
+                # one grid is bound by its levels' longest rays, not the FP64 pipe
+                "latency_roofline": {**latency,
+                                     "frac": latency["floor_ms"] / (trace_ms / args.steps),
+                                     "note": "sum over levels of the level's longest ray "
+                                             "integrated alone, over the trace time per "
+                                             "build"}}
 
     # resident environment (8192x4096) and star set (10^6 stars, tree level 14)
     env = sp = None
