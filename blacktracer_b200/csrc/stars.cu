@@ -288,6 +288,8 @@ enum { kHcDeferred = 0, kHcGiant = 1, kHcOther = 2, kHcNext = 3, kHcWords = 4 };
 // in unit order, so frames are reproducible.  Pixels whose nodes do not fit
 // the node pool go to the block-per-pixel kernel (k_star_heavy).
 enum { kHvUnits = 0, kHvUnitLeaves = 1, kHvFetch = 2, kHvWords = 4 };
+// Rounds of 32 leaves per unit, at least (more when the unit slots run out).
+constexpr int kUnitRounds = 1;
 
 // Pass 1, one thread per deferred pixel: the nodes its search emits and the
 // leaves under them.
@@ -384,7 +386,8 @@ k_hv_scan(const uint32_t* __restrict__ heavy, uint32_t* hc, const uint32_t* __re
     if (k < n && k >= ok) order[k - ok] = heavy[k];
   }
   const unsigned long long slots = 32ull * (unit_cap - ok);  // ok <= unit_cap / 2
-  const unsigned long long U = 32ull * (kept > slots ? (kept + slots - 1) / slots : 1ull);
+  const unsigned long long R = kept > slots ? (kept + slots - 1) / slots : 1ull;
+  const unsigned long long U = 32ull * (R > (unsigned long long)kUnitRounds ? R : kUnitRounds);
   unsigned long long ubase = 0;
   for (uint32_t c = 0; c < n; c += blockDim.x) {
     const uint32_t k = c + threadIdx.x;
