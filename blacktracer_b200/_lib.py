@@ -152,6 +152,8 @@ _SIGS = {
     "bt_grid_set_timing": (C.c_int, [_vp, C.c_int]),
     "bt_grid_set_graph": (C.c_int, [_vp, C.c_int]),
     "bt_grid_set_tfix_passes": (C.c_int, [_vp, C.c_int]),
+    "bt_grid_set_flow": (C.c_int, [_vp, C.c_int]),
+    "bt_batch_set_flow": (C.c_int, [_vp, C.c_int]),
     "bt_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),
     "bt_batch_destroy": (None, [_vp]),
     "bt_batch_build": (C.c_int, [_vp, C.POINTER(bt_camera), C.POINTER(C.c_double), C.c_int,

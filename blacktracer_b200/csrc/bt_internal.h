@@ -130,6 +130,14 @@ int launch_trace_mixed(const GridDesc* D, int G, const uint32_t* qoff,
 int launch_trace_fast(const GridDesc* D, int G, const uint32_t* qoff,
                       uint32_t* qfetch, TraceShape shape, cudaStream_t s);
 
+// The refinement levels of a set as one persistent launch (grid_flow.cuh):
+// the flow's queues and sync words, its control block, and its launch per
+// form (integrate.cu, mixed.cu).
+struct FlowArgs;
+int launch_flow_plain(const FlowArgs& A, cudaStream_t s);
+int launch_flow_mixed(const FlowArgs& A, cudaStream_t s);
+int launch_flow_fast(const FlowArgs& A, cudaStream_t s);
+
 // Map grid of a built grid into a caller's buffer (grid.cu).
 int grid_map_export_into(const bt_grid* g, float* dst, cudaStream_t s);
 

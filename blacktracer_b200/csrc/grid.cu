@@ -41,6 +41,7 @@
 #include <new>
 
 #include "bt_internal.h"
+#include "grid_flow.cuh"
 
 namespace bt {
 
@@ -112,6 +113,13 @@ struct bt_batch {
   // Jacobi passes of the T-vertex fix per level (kMaxTfixPasses unless a
   // test lowers it with bt_grid_set_tfix_passes)
   int tfix_passes;
+  // the refinement levels as one persistent launch (bt_batch_set_flow): its
+  // check queue (G*NM slots), block counters (G*NM bytes) and control block;
+  // the set-up and trace queues and the sync words reuse the block lists
+  int flow, exec_flow;
+  uint32_t* flow_q;
+  uint8_t* flow_bw;
+  bt::FlowCtl* flow_ctl;
 };
 
 namespace bt {
@@ -636,6 +644,79 @@ __global__ void k_tfix_check(const GridDesc* __restrict__ D, int G, int passes) 
   ctr->tfix_flags[1] = 1;
 }
 
+// ------------------------------------------------------------ flow
+// Sync words of the first n grids' vertices: traced where the seed level
+// traced them (and the pole copies), else nothing yet.
+__global__ void k_flow_sync(const GridDesc* __restrict__ D, size_t total, uint32_t NM,
+                            uint32_t* __restrict__ vsync) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t g = (uint32_t)(t / NM), key = (uint32_t)(t % NM);
+    vsync[t] = D[g].L.vflag[key] == 1 ? kVTraced : 0u;
+  }
+}
+
+// The start level's blocks of grid blockIdx.y (its check list) onto the
+// check queue: their corners are all traced.
+__global__ void k_flow_checks(const GridDesc* __restrict__ D, uint32_t NM,
+                              uint32_t* __restrict__ q, FlowCtl* ctl) {
+  const uint32_t g = blockIdx.y;
+  const GridDesc& d = D[g];
+  const uint32_t n = d.ctr->n_check;
+  const unsigned lane = threadIdx.x & 31u;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const uint32_t t = base + threadIdx.x;
+    const bool valid = t < n;
+    const unsigned m = __ballot_sync(0xffffffffu, valid);
+    unsigned long long at = 0;
+    if (lane == 0 && m) {
+      at = atomicAdd(&ctl->tail[kFqCheck], (unsigned long long)__popc(m));
+      atomicAdd(&ctl->live, (unsigned long long)__popc(m));
+    }
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (valid) q[at + __popc(m & ((1u << lane) - 1u))] = g * NM + d.list[0][t];
+  }
+}
+
+// After the flow, one block per grid: its leaves (tagged with their level)
+// sorted by level into the leaf list with the per-level offsets the T-vertex
+// fix reads (the order within a level does not matter to it), the rays it
+// traced counted, and the flow's error flags.
+__global__ void k_flow_leaves(const GridDesc* __restrict__ D, int span,
+                              const FlowCtl* __restrict__ ctl) {
+  const GridDesc& d = D[blockIdx.x];
+  GridCounters* ctr = d.ctr;
+  const uint32_t n = ctr->n_leaf;
+  __shared__ uint32_t cnt[16], off[16];
+  if (threadIdx.x < 16) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t* tmp = d.trace;  // free once the flow has ended
+  for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+    const uint32_t v = d.leaves[t];
+    tmp[t] = v;
+    atomicAdd(&cnt[v >> kFlowKeyBits], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int s = 0; s < 16; s++) {
+      off[s] = acc;
+      if (s <= span) ctr->leaf_off[s] = acc;
+      acc += cnt[s];
+    }
+    const uint64_t tr = ((uint64_t)ctr->traced_hi << 32 | ctr->traced_lo) + ctr->n_trace;
+    ctr->traced_lo = (uint32_t)tr;
+    ctr->traced_hi = (uint32_t)(tr >> 32);
+    ctr->n_trace = 0;
+    ctr->err |= ctl->err;
+  }
+  __syncthreads();
+  for (uint32_t t = threadIdx.x; t < n; t += blockDim.x) {
+    const uint32_t v = tmp[t];
+    d.leaves[atomicAdd(&off[v >> kFlowKeyBits], 1u)] = v & ((1u << kFlowKeyBits) - 1u);
+  }
+}
+
 // ------------------------------------------------------------ exports
 // makeGrid (BT/MakeImageKernel.cu:369-384) from the dense lattice: float2
 // values, (-2,-2) where no vertex exists; with sym the lower hemisphere is
@@ -854,8 +935,9 @@ void batch_free(bt_batch* b) {
     }
     delete[] b->grids;
   }
-  void* ptrs[] = {b->thphi, b->steps, b->vflag, b->vstat, b->blevel, b->lists,
-                  b->X,     b->ctr,   b->D,     b->qoff,  b->qfetch};
+  void* ptrs[] = {b->thphi, b->steps,   b->vflag,  b->vstat,   b->blevel, b->lists,
+                  b->X,     b->ctr,     b->D,      b->qoff,    b->qfetch, b->flow_q,
+                  b->flow_bw, b->flow_ctl};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (b->ctr_host) cudaFreeHost(b->ctr_host);
@@ -957,6 +1039,11 @@ GridDesc member_desc(bt_batch* b, int g, int startlevel, const RayParams& p) {
   return d;
 }
 
+// The flow is used when switched on and its items fit in 28 bits.
+static bool flow_usable(const bt_batch* b, int n) {
+  return b->flow && b->flow_q && (uint64_t)n * b->NM < (1ull << kFlowKeyBits);
+}
+
 // The launch sequence of one build of the whole set (no host
 // synchronisation).  Returns the number of kernels launched in *launches.
 int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_t s,
@@ -998,6 +1085,48 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
   k_advance<<<ga, 128, 0, s>>>(b->D, G, 1, 0);
   BT_CUDA_TRY(cudaGetLastError());
   nk += 2;
+  if (flow_usable(b, G) && startlevel < b->maxlevel) {
+    // the refinement levels as one persistent launch
+    const size_t GNM = (size_t)G * NM, gnm_full = (size_t)b->G * NM;
+    uint32_t* vsync = b->lists + 1 * gnm_full;
+    uint32_t* qsetup = b->lists + 0 * gnm_full;  // the check lists, once read
+    uint32_t* qtrace = b->lists + 2 * gnm_full;  // the trace lists, free now
+    BT_CUDA_TRY(cudaMemsetAsync(b->flow_ctl, 0, sizeof(FlowCtl), s));
+    BT_CUDA_TRY(cudaMemsetAsync(b->flow_bw, 0, GNM, s));
+    BT_CUDA_TRY(cudaMemsetAsync(b->flow_q, 0xff, GNM * sizeof(uint32_t), s));
+    k_flow_sync<<<sm_count() * 8, 256, 0, s>>>(b->D, GNM, (uint32_t)NM, vsync);
+    k_flow_checks<<<dim3(set_blocks(NM / 4, 256, G), G), 256, 0, s>>>(b->D, (uint32_t)NM,
+                                                                      b->flow_q, b->flow_ctl);
+    BT_CUDA_TRY(cudaMemsetAsync(qsetup, 0xff, GNM * sizeof(uint32_t), s));
+    BT_CUDA_TRY(cudaMemsetAsync(qtrace, 0xff, GNM * sizeof(uint32_t), s));
+    FlowArgs A;
+    A.D = b->D;
+    A.G = G;
+    A.NM = (uint32_t)NM;
+    A.M = (uint32_t)b->M;
+    A.maxlevel = b->maxlevel;
+    A.startlevel = startlevel;
+    A.q[kFqCheck] = b->flow_q;
+    A.q[kFqSetup] = qsetup;
+    A.q[kFqTrace] = qtrace;
+    for (int k = 0; k < kFq; k++) A.cap[k] = GNM;
+    A.vsync = vsync;
+    A.bwait = b->flow_bw;
+    A.ctl = b->flow_ctl;
+    const bool t = timing && b->timing && b->n_ev + 2 <= 2 * 16;
+    if (t) BT_CUDA_TRY(cudaEventRecord(b->ev[b->n_ev], s));
+    const int rc = precision == BT_PRECISION_MIXED ? launch_flow_mixed(A, s)
+                   : precision == BT_PRECISION_FAST ? launch_flow_fast(A, s)
+                                                    : launch_flow_plain(A, s);
+    if (rc) return rc;
+    if (t) {
+      BT_CUDA_TRY(cudaEventRecord(b->ev[b->n_ev + 1], s));
+      b->n_ev += 2;
+    }
+    k_flow_leaves<<<G, 256, 0, s>>>(b->D, b->maxlevel - startlevel, b->flow_ctl);
+    BT_CUDA_TRY(cudaGetLastError());
+    nk += 5;
+  } else {
   int cur = 0;
   for (int level = startlevel; level < b->maxlevel; level++) {
     k_refine<<<dim3(set_blocks(NM / 4, 256, G), G), 256, 0, s>>>(b->D, level, cur);
@@ -1012,6 +1141,7 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
   k_finalize<<<dim3(set_blocks(NM / 4, 256, G), G), 256, 0, s>>>(b->D, cur);
   BT_CUDA_TRY(cudaGetLastError());
   nk++;
+  }
   // T-vertex fix, level by level (coarse to fine)
   const unsigned nb = set_blocks(NM / 16, 128, G);
   for (int level = startlevel; level < b->maxlevel; level++) {
@@ -1067,6 +1197,7 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int n,
     const bool same = b->exec && b->exec_n == G && b->exec_startlevel == startlevel &&
                       b->exec_precision == precision &&
                       b->exec_tfix_passes == b->tfix_passes &&
+                      b->exec_flow == b->flow &&
                       b->exec_shape.threads == b->shape.threads &&
                       b->exec_shape.blocks_per_sm == b->shape.blocks_per_sm;
     if (!same) {
@@ -1096,6 +1227,7 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int n,
       b->exec_startlevel = startlevel;
       b->exec_precision = precision;
       b->exec_tfix_passes = b->tfix_passes;
+      b->exec_flow = b->flow;
       b->exec_shape = b->shape;
       b->launches = launches;
     }
@@ -1120,6 +1252,28 @@ float batch_trace_ms(const bt_batch* b) {
     if (cudaEventElapsedTime(&ms, b->ev[k], b->ev[k + 1]) == cudaSuccess) total += ms;
   }
   return total;
+}
+
+// The flow's buffers, reserved when it is switched on.
+int batch_set_flow(bt_batch* b, int on) {
+  if (on && !b->flow_q) {
+    const size_t GNM = (size_t)b->G * b->NM;
+    cudaError_t e = cudaMalloc((void**)&b->flow_q, GNM * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->flow_bw, GNM);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->flow_ctl, sizeof(FlowCtl));
+    if (e != cudaSuccess) {
+      cudaFree(b->flow_q);
+      cudaFree(b->flow_bw);
+      cudaFree(b->flow_ctl);
+      b->flow_q = nullptr;
+      b->flow_bw = nullptr;
+      b->flow_ctl = nullptr;
+      set_error("flow buffers (%zu vertices) failed: %s", GNM, cudaGetErrorString(e));
+      return BT_ERR_NOMEM;
+    }
+  }
+  b->flow = on ? 1 : 0;
+  return BT_OK;
 }
 
 int batch_set_timing(bt_batch* b, int on) {
@@ -1210,7 +1364,8 @@ int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream) {
   info->trace_launches = g->set->n_ev / 2;
   if (info->flags) {
     set_error("grid build flags 0x%x (1: T-vertex fix did not converge, "
-              "2: fix stack overflow, 4: work list overflow)", info->flags);
+              "2: fix stack overflow, 4: work list overflow, 8: the flow gave up waiting)",
+              info->flags);
     return BT_ERR_NUMERIC;
   }
   return BT_OK;
@@ -1225,6 +1380,12 @@ int bt_grid_set_graph(bt_grid* g, int on) {
   BT_ARG_CHECK(g != nullptr, "NULL grid");
   g->set->graph = on ? 1 : 0;
   return BT_OK;
+}
+
+int bt_grid_set_flow(bt_grid* g, int on) {
+  clear_error();
+  BT_ARG_CHECK(g != nullptr, "NULL grid");
+  return batch_set_flow(g->set, on);
 }
 
 int bt_grid_set_tfix_passes(bt_grid* g, int passes) {
@@ -1365,6 +1526,12 @@ int bt_batch_set_graph(bt_batch* b, int on) {
   BT_ARG_CHECK(b != nullptr, "NULL set");
   b->graph = on ? 1 : 0;
   return BT_OK;
+}
+
+int bt_batch_set_flow(bt_batch* b, int on) {
+  clear_error();
+  BT_ARG_CHECK(b != nullptr, "NULL set");
+  return batch_set_flow(b, on);
 }
 
 int bt_batch_set_timing(bt_batch* b, int on) {

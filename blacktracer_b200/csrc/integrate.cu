@@ -9,6 +9,7 @@
 #include "bt_internal.h"
 #include "kerr_plain.cuh"
 #include "trace_kernel.cuh"
+#include "grid_flow.cuh"
 
 namespace bt {
 
@@ -123,6 +124,10 @@ struct PlainPolicy {
 int launch_trace_plain(const GridDesc* D, int G, const uint32_t* qoff,
                        uint32_t* qfetch, TraceShape shape, cudaStream_t s) {
   return launch_trace_shape<PlainPolicy>(D, G, qoff, qfetch, shape, s);
+}
+
+int launch_flow_plain(const FlowArgs& A, cudaStream_t s) {
+  return launch_flow<PlainPolicy>(A, s);
 }
 
 int sm_count() {

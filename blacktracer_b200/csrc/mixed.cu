@@ -8,6 +8,7 @@
 #include "kerr_fast.cuh"
 #include "kerr_mixed.cuh"
 #include "trace_kernel.cuh"
+#include "grid_flow.cuh"
 
 namespace bt {
 
@@ -78,6 +79,14 @@ int launch_integrate_fast(const RayParams& p, const double* th, const double* ph
 int launch_trace_fast(const GridDesc* D, int G, const uint32_t* qoff,
                       uint32_t* qfetch, TraceShape shape, cudaStream_t s) {
   return launch_trace_shape<FastPolicy>(D, G, qoff, qfetch, shape, s);
+}
+
+int launch_flow_fast(const FlowArgs& A, cudaStream_t s) {
+  return launch_flow<FastPolicy>(A, s);
+}
+
+int launch_flow_mixed(const FlowArgs& A, cudaStream_t s) {
+  return launch_flow<MixedPolicy>(A, s);
 }
 
 }  // namespace bt

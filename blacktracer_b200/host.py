@@ -239,6 +239,11 @@ class Grid:
         """Capture later builds once into a CUDA graph and replay it."""
         L.check(L.lib().bt_grid_set_graph(self._h, 1 if on else 0))
 
+    def set_flow(self, on=True):
+        """Run the refinement levels of later builds as one persistent launch
+        (blocks checked as soon as their corners are traced; same grids)."""
+        L.check(L.lib().bt_grid_set_flow(self._h, 1 if on else 0))
+
     def set_tfix_passes(self, passes: int):
         """Jacobi passes of the T-vertex fix per level of later builds (1..8;
         default 8).  A level still changing at its last pass is reported as
@@ -385,6 +390,10 @@ class GridSet:
 
     def set_timing(self, on=True):
         L.check(L.lib().bt_batch_set_timing(self._h, 1 if on else 0))
+
+    def set_flow(self, on=True):
+        """Run the refinement levels of later builds as one persistent launch."""
+        L.check(L.lib().bt_batch_set_flow(self._h, 1 if on else 0))
 
     def set_shape(self, threads=128, blocks_per_sm=0):
         s = L.bt_trace_shape(threads, blocks_per_sm)

@@ -193,6 +193,17 @@ int bt_grid_set_timing(bt_grid* g, int on);
  * the reference (its build is host-driven). */
 int bt_grid_set_graph(bt_grid* g, int on);
 
+/* on = 1: later builds run the refinement levels as one persistent launch
+ * instead of one trace launch per level.  A block is checked (refineCheck,
+ * BT/Grid.h:410-445) as soon as its own four corners are traced and a new
+ * vertex is traced as soon as a check creates it, so no level waits for the
+ * previous level's longest rays.  The grids are the same bit for bit.
+ * Reserves 5 bytes per lattice vertex of the set; used when the set's
+ * lattices hold fewer than 2^28 vertices in all (otherwise builds take the
+ * level form).  No counterpart in the reference (its build is host-driven,
+ * level by level). */
+int bt_grid_set_flow(bt_grid* g, int on);
+
 /* Diagnostic: the number of Jacobi passes of the T-vertex fix per level of
  * later builds, 1..8 (default 8, the most any grid needs; 2-3 is typical).
  * A level whose last pass still changed a vertex is reported as not
@@ -274,9 +285,10 @@ int bt_batch_build_first(bt_batch* b, int n, const bt_camera* cams,
 /* Member k (0 <= k < count), or NULL. */
 bt_grid* bt_batch_grid(bt_batch* b, int k);
 
-/* As bt_grid_set_graph / bt_grid_set_timing, for the whole set. */
+/* As bt_grid_set_graph / bt_grid_set_timing / bt_grid_set_flow, for the whole set. */
 int bt_batch_set_graph(bt_batch* b, int on);
 int bt_batch_set_timing(bt_batch* b, int on);
+int bt_batch_set_flow(bt_batch* b, int on);
 
 /* Launch shape of the persistent ray-tracing kernel: threads per block
  * (64, 128 or 256) and resident blocks per SM (0 = as many as fit). */

@@ -118,3 +118,30 @@ def test_member_misuse(bt, cuda):
         S.grids[0].build(cams[0], spins[0])
     bt.lib().bt_grid_destroy(S.grids[1]._h)  # ignored for members
     assert S.grids[1].traced > 0
+
+
+@pytest.mark.parametrize("prec", ["plain", "fast", "mixed"])
+def test_flow_builds_equal_level_builds(bt, cuda, prec):
+    """The refinement levels run as one persistent launch (bt_batch_set_flow:
+    a block is checked as soon as its corners are traced) give the grids of
+    the level-by-level build, bit for bit: a set of poses (and one member
+    replayed from a CUDA graph), and the C2 grid L6 -> L10 alone."""
+    cams, spins = cameras(bt, POSES)
+    lvl = bt.GridSet(ML, SL, True, len(cams), opts=prec)
+    lvl.build(cams, spins)
+    flo = bt.GridSet(ML, SL, True, len(cams), opts=prec)
+    flo.set_flow(True)
+    for graph in (False, True):
+        flo.set_graph(graph)
+        flo.build(cams, spins)
+        assert flo.info().flags == 0
+        for k in range(len(cams)):
+            assert_same(dense(flo.grids[k]), dense(lvl.grids[k]), f"{prec} flow member {k}")
+            assert flo.grids[k].traced == lvl.grids[k].traced
+    cam = bt.Camera(math.pi / 2, 0.0, 5.0, 0.0, 0.0, 1.0, a=0.999)
+    a = bt.Grid(10, 6, True, cam, opts=prec)
+    b = bt.Grid(10, 6, True, cam, opts=prec)
+    b.set_flow(True)
+    b.build()
+    assert b.info().flags == 0 and b.traced == a.traced
+    assert_same(dense(b), dense(a), f"{prec} flow C2 L10")
