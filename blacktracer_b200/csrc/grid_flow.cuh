@@ -36,8 +36,9 @@
 // level-by-level build gives, bit for bit; only the order of work differs.
 // The launch ends when no queued or running item is left (a count of items
 // pushed and not finished).  Every wait is bounded: a warp that finds no
-// work sleeps and retries, and gives up (error flag 8) after about ten
-// seconds without progress anywhere; a queue slot taken before its producer
+// work sleeps and retries, and gives up (error flag 8) after about two
+// seconds without progress anywhere (the longest legitimate wait, one ray
+// alone, is a few milliseconds); a queue slot taken before its producer
 // wrote it is waited for the same way.
 #pragma once
 
@@ -54,7 +55,7 @@ enum { kFqCheck = 0, kFqSetup = 1, kFqTrace = 2, kFq = 3 };
 // check item carries (level - startlevel) in its top four bits.
 constexpr uint32_t kFlowKeyBits = 28;
 constexpr int kFlowThreads = 256;  // one manager warp and seven tracer warps
-constexpr long long kFlowIdleCap = 40000000;  // ~10 s of 256 ns sleeps
+constexpr long long kFlowIdleCap = 8000000;  // ~2 s of 256 ns sleeps
 
 struct FlowCtl {
   unsigned long long head[kFq];
