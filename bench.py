@@ -626,6 +626,36 @@ def main():
         del dp, dm, gm
     del ref_dense
 
+    # the refinement levels as one persistent launch (set_flow): the same grid,
+    # timed like the forms above, against the level-by-level headline build
+    flow_grid = {}
+    head = grid.dense()
+    for bps in (1, 2):
+        gf = bt.Grid(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam, opts=prec_main)
+        gf.set_flow(True, blocks_per_sm=bps)
+        for _ in range(3):
+            gf.build()
+        torch.cuda.synchronize()
+        t_f = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            gf.build()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_f += e0.elapsed_time(e1)
+        df = gf.dense()
+        flow_grid[f"{bps}_blocks_per_sm"] = {
+            "ms_per_build": t_f / args.steps,
+            "level_build_ms": total_ms / args.steps,
+            "speed_vs_level": (total_ms / args.steps) / (t_f / args.steps),
+            "same_grid": bool(all(torch.equal(head[k], df[k]) for k in head)),
+            "flags": int(gf.info().flags)}
+        del gf, df
+    del head
+
     # end to end through the C ABI with host buffers: build + compact export
     # (CamToCel / steps / blockLevels) into pinned host memory every step
     ex = grid.export()
@@ -828,6 +858,24 @@ def main():
                     "bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
                     "frac": ach / peak if peak else None, "flops_per_set": fl,
                     "note": "whole set build time (all kernels), FP64 peak as the headline's"}
+            if prec == "fast":
+                # the same set as one persistent launch per build
+                Sb.set_flow(True, blocks_per_sm=2)
+                for _ in range(3):
+                    Sb.build(cams_b, spins_b)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                for _ in range(nb_steps):
+                    Sb.build(cams_b, spins_b)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms_f = e0.elapsed_time(e1) / nb_steps
+                res[prec]["one_launch"] = {"ms_per_set": ms_f, "value": rays / (ms_f / 1e3),
+                                           "speed_vs_level": ms / ms_f, "blocks_per_sm": 2,
+                                           "flags": int(Sb.info().flags)}
+                Sb.set_flow(False)
             sets[prec] = Sb
         for prec in ("fast", "mixed"):
             p99, mx, topo = set_error_vs(sets["plain"], sets[prec])
@@ -925,6 +973,9 @@ def main():
             "serving": serving,
             "full_frame_8k": full,
             "integration_seam": seam,
+            "one_launch_build": {"workload": "the headline grid built with set_flow: every "
+                                             "refinement level in one persistent launch",
+                                 **flow_grid},
             "batched": batched,
             "frames_4k": frames,
             **other,

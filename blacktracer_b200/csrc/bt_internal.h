@@ -130,6 +130,11 @@ int launch_trace_mixed(const GridDesc* D, int G, const uint32_t* qoff,
 int launch_trace_fast(const GridDesc* D, int G, const uint32_t* qoff,
                       uint32_t* qfetch, TraceShape shape, cudaStream_t s);
 
+// A new vertex is hot when its parent block has a corner whose ray took at
+// least kHotSteps attempts (its own ray is then likely slow too): both build
+// forms start hot rays first.
+constexpr int32_t kHotSteps = 100;
+
 // The refinement levels of a set as one persistent launch (grid_flow.cuh):
 // the flow's queues and sync words, its control block, and its launch per
 // form (integrate.cu, mixed.cu).

@@ -113,9 +113,10 @@ struct bt_batch {
   // Jacobi passes of the T-vertex fix per level (kMaxTfixPasses unless a
   // test lowers it with bt_grid_set_tfix_passes)
   int tfix_passes;
-  // the refinement levels as one persistent launch (bt_batch_set_flow): its
-  // check queue (G*NM slots), block counters (G*NM bytes) and control block;
-  // the set-up and trace queues and the sync words reuse the block lists
+  // the refinement levels as one persistent launch (bt_batch_set_flow; flow =
+  // its blocks per SM, 0 = off): its check, hot-trace and hot-set-up queues
+  // (G*NM slots each), block counters (G*NM bytes) and control block; the
+  // set-up and trace queues and the sync words reuse the block lists
   int flow, exec_flow;
   uint32_t* flow_q;
   uint8_t* flow_bw;
@@ -238,12 +239,10 @@ __global__ void k_queue(const GridDesc* __restrict__ D, int G, uint32_t* qoff,
 }
 
 // ------------------------------------------------------------ refinement
-// A new vertex goes to the front of the trace list when its parent block
-// has a corner whose ray took at least kHotSteps attempts (its own ray is
-// then likely slow too), else to the back: the trace kernel takes the front
-// first, so the longest rays of a level start first instead of whenever a
-// lane happens to reach them.  The order changes no result.
-constexpr int32_t kHotSteps = 100;
+// A hot new vertex (kHotSteps) goes to the front of the trace list, else to
+// the back: the trace kernel takes the front first, so the longest rays of a
+// level start first instead of whenever a lane happens to reach them.  The
+// order changes no result.
 
 __device__ __forceinline__ void claim_vertex(const LatticeView& L, uint32_t i,
                                              uint32_t j, uint32_t* trace,
@@ -670,8 +669,8 @@ __global__ void k_flow_checks(const GridDesc* __restrict__ D, uint32_t NM,
     const unsigned m = __ballot_sync(0xffffffffu, valid);
     unsigned long long at = 0;
     if (lane == 0 && m) {
-      at = atomicAdd(&ctl->tail[kFqCheck], (unsigned long long)__popc(m));
-      atomicAdd(&ctl->live, (unsigned long long)__popc(m));
+      atomicAdd(&ctl->live.v, (unsigned long long)__popc(m));
+      at = atomicAdd(&ctl->tail[kFqCheck].v, (unsigned long long)__popc(m));
     }
     at = __shfl_sync(0xffffffffu, at, 0);
     if (valid) q[at + __popc(m & ((1u << lane) - 1u))] = g * NM + d.list[0][t];
@@ -1093,7 +1092,7 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
     uint32_t* qtrace = b->lists + 2 * gnm_full;  // the trace lists, free now
     BT_CUDA_TRY(cudaMemsetAsync(b->flow_ctl, 0, sizeof(FlowCtl), s));
     BT_CUDA_TRY(cudaMemsetAsync(b->flow_bw, 0, GNM, s));
-    BT_CUDA_TRY(cudaMemsetAsync(b->flow_q, 0xff, GNM * sizeof(uint32_t), s));
+    BT_CUDA_TRY(cudaMemsetAsync(b->flow_q, 0xff, 3 * GNM * sizeof(uint32_t), s));
     k_flow_sync<<<sm_count() * 8, 256, 0, s>>>(b->D, GNM, (uint32_t)NM, vsync);
     k_flow_checks<<<dim3(set_blocks(NM / 4, 256, G), G), 256, 0, s>>>(b->D, (uint32_t)NM,
                                                                       b->flow_q, b->flow_ctl);
@@ -1109,10 +1108,13 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
     A.q[kFqCheck] = b->flow_q;
     A.q[kFqSetup] = qsetup;
     A.q[kFqTrace] = qtrace;
+    A.q[kFqHot] = b->flow_q + GNM;
+    A.q[kFqSetupHot] = b->flow_q + 2 * GNM;
     for (int k = 0; k < kFq; k++) A.cap[k] = GNM;
     A.vsync = vsync;
     A.bwait = b->flow_bw;
     A.ctl = b->flow_ctl;
+    A.blocks_per_sm = b->flow;
     const bool t = timing && b->timing && b->n_ev + 2 <= 2 * 16;
     if (t) BT_CUDA_TRY(cudaEventRecord(b->ev[b->n_ev], s));
     const int rc = precision == BT_PRECISION_MIXED ? launch_flow_mixed(A, s)
@@ -1258,7 +1260,7 @@ float batch_trace_ms(const bt_batch* b) {
 int batch_set_flow(bt_batch* b, int on) {
   if (on && !b->flow_q) {
     const size_t GNM = (size_t)b->G * b->NM;
-    cudaError_t e = cudaMalloc((void**)&b->flow_q, GNM * sizeof(uint32_t));
+    cudaError_t e = cudaMalloc((void**)&b->flow_q, 3 * GNM * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMalloc((void**)&b->flow_bw, GNM);
     if (e == cudaSuccess) e = cudaMalloc((void**)&b->flow_ctl, sizeof(FlowCtl));
     if (e != cudaSuccess) {
@@ -1272,7 +1274,7 @@ int batch_set_flow(bt_batch* b, int on) {
       return BT_ERR_NOMEM;
     }
   }
-  b->flow = on ? 1 : 0;
+  b->flow = on > 0 ? on : 0;
   return BT_OK;
 }
 

@@ -18,6 +18,9 @@ import numpy as np
 
 from . import _lib as L
 
+# Blocks of 256 threads per SM of the one-launch build (set_flow).
+FLOW_BLOCKS_PER_SM = 2
+
 _current_spin = 0.0  # metric::a after the last BlackHole / setA
 
 
@@ -239,10 +242,11 @@ class Grid:
         """Capture later builds once into a CUDA graph and replay it."""
         L.check(L.lib().bt_grid_set_graph(self._h, 1 if on else 0))
 
-    def set_flow(self, on=True):
+    def set_flow(self, on=True, blocks_per_sm=FLOW_BLOCKS_PER_SM):
         """Run the refinement levels of later builds as one persistent launch
-        (blocks checked as soon as their corners are traced; same grids)."""
-        L.check(L.lib().bt_grid_set_flow(self._h, 1 if on else 0))
+        (blocks checked as soon as their corners are traced; same grids) of
+        `blocks_per_sm` blocks of 256 threads per SM."""
+        L.check(L.lib().bt_grid_set_flow(self._h, blocks_per_sm if on else 0))
 
     def set_tfix_passes(self, passes: int):
         """Jacobi passes of the T-vertex fix per level of later builds (1..8;
@@ -391,9 +395,10 @@ class GridSet:
     def set_timing(self, on=True):
         L.check(L.lib().bt_batch_set_timing(self._h, 1 if on else 0))
 
-    def set_flow(self, on=True):
-        """Run the refinement levels of later builds as one persistent launch."""
-        L.check(L.lib().bt_batch_set_flow(self._h, 1 if on else 0))
+    def set_flow(self, on=True, blocks_per_sm=FLOW_BLOCKS_PER_SM):
+        """Run the refinement levels of later builds as one persistent launch
+        of `blocks_per_sm` blocks of 256 threads per SM."""
+        L.check(L.lib().bt_batch_set_flow(self._h, blocks_per_sm if on else 0))
 
     def set_shape(self, threads=128, blocks_per_sm=0):
         s = L.bt_trace_shape(threads, blocks_per_sm)

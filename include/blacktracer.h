@@ -193,15 +193,16 @@ int bt_grid_set_timing(bt_grid* g, int on);
  * the reference (its build is host-driven). */
 int bt_grid_set_graph(bt_grid* g, int on);
 
-/* on = 1: later builds run the refinement levels as one persistent launch
- * instead of one trace launch per level.  A block is checked (refineCheck,
- * BT/Grid.h:410-445) as soon as its own four corners are traced and a new
- * vertex is traced as soon as a check creates it, so no level waits for the
- * previous level's longest rays.  The grids are the same bit for bit.
- * Reserves 5 bytes per lattice vertex of the set; used when the set's
- * lattices hold fewer than 2^28 vertices in all (otherwise builds take the
- * level form).  No counterpart in the reference (its build is host-driven,
- * level by level). */
+/* on >= 1: later builds run the refinement levels as one persistent launch
+ * of `on` blocks of 256 threads per SM (capped by the occupancy limit, 2)
+ * instead of one trace launch per level; 0 = off.  A block is checked
+ * (refineCheck, BT/Grid.h:410-445) as soon as its own four corners are
+ * traced and a new vertex is traced as soon as a check creates it, so no
+ * level waits for the previous level's longest rays.  The grids are the same
+ * bit for bit.  Reserves 13 bytes per lattice vertex of the set; used when the
+ * set's lattices hold fewer than 2^28 vertices in all (otherwise builds take
+ * the level form).  No counterpart in the reference (its build is
+ * host-driven, level by level). */
 int bt_grid_set_flow(bt_grid* g, int on);
 
 /* Diagnostic: the number of Jacobi passes of the T-vertex fix per level of

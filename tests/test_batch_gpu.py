@@ -141,7 +141,8 @@ def test_flow_builds_equal_level_builds(bt, cuda, prec):
     cam = bt.Camera(math.pi / 2, 0.0, 5.0, 0.0, 0.0, 1.0, a=0.999)
     a = bt.Grid(10, 6, True, cam, opts=prec)
     b = bt.Grid(10, 6, True, cam, opts=prec)
-    b.set_flow(True)
-    b.build()
-    assert b.info().flags == 0 and b.traced == a.traced
-    assert_same(dense(b), dense(a), f"{prec} flow C2 L10")
+    for bps in (1, 2):  # launch shapes: blocks of 256 threads per SM
+        b.set_flow(True, blocks_per_sm=bps)
+        b.build()
+        assert b.info().flags == 0 and b.traced == a.traced
+        assert_same(dense(b), dense(a), f"{prec} flow C2 L10, {bps} blocks per SM")
