@@ -228,27 +228,22 @@ k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
       }
     }
   };
-  for (int px = 0; px < 32; px++) {
-    const int n = __shfl_sync(0xffffffffu, nleaf, px);
-    if (n == 0) continue;
-    PixelStars P;
-    stars_of(sh_core[w][px], step, P);
-    for (int k = 0; k < n; k++) {
-      int a0, a1;
-      node_range(S, sh_leaf[w][k][px], a0, a1);
-      for (int base = a0; base < a1; base += 32) {
-        const int q = base + lane;
-        float st = 0.f, sp = 0.f;
-        const bool in = q < a1 && star_test(P, S, q, st, sp);
-        const unsigned ball = __ballot_sync(0xffffffffu, in);
-        if (!ball) continue;
-        const int cnt = __popc(ball);
-        if (qn + cnt > 32) {
-          __syncwarp();
-          drain(qn);
-          __syncwarp();
-          qn = 0;
-        }
+  // One loop over the warp's pixels, leaves and star steps with the drain at
+  // a single call site (the kernel's hot code is what bounds it; a second
+  // inlined copy of the drain for the last hits doubled it).  A step whose
+  // hits would not fit waits in registers while the queue drains.
+  PixelStars P;
+  int px = -1, n = 0, k = 0;  // pixel, its leaves, the next leaf
+  int base = 0, a1 = 0;       // star range left of the current leaf
+  bool pend = false, in = false;  // a tested step waiting for room; its lane result
+  int q = 0, cnt = 0;
+  unsigned ball = 0;
+  float st = 0.f, sp = 0.f;
+  for (;;) {
+    bool done = false;
+    for (;;) {
+      if (pend) {
+        if (qn + cnt > 32) break;  // drain first
         if (in) {
           const int at = qn + __popc(ball & ((1u << lane) - 1u));
           sh_hq[w][at] = q;
@@ -256,12 +251,37 @@ k_star_cells(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
           sh_hpx[w][at] = (uint8_t)px;
         }
         qn += cnt;
+        pend = false;
+      }
+      if (base < a1) {
+        q = base + lane;
+        base += 32;
+        st = 0.f;
+        sp = 0.f;
+        in = q < a1 && star_test(P, S, q, st, sp);
+        ball = __ballot_sync(0xffffffffu, in);
+        cnt = __popc(ball);
+        pend = cnt != 0;
+      } else if (k < n) {
+        node_range(S, sh_leaf[w][k][px], base, a1);
+        k++;
+      } else if (px < 31) {
+        px++;
+        n = __shfl_sync(0xffffffffu, nleaf, px);
+        k = 0;
+        if (n) stars_of(sh_core[w][px], step, P);
+      } else {
+        done = true;
+        break;
       }
     }
-  }
-  if (qn) {
-    __syncwarp();
-    drain(qn);
+    if (qn) {
+      __syncwarp();
+      drain(qn);
+      __syncwarp();
+      qn = 0;
+    }
+    if (done) break;
   }
   flush_cells();
   // heavy pixels are written 0 here and flagged again by k_star_heavy
@@ -448,8 +468,11 @@ __global__ void k_hv_nodes(const float2* __restrict__ thphi, const uint8_t* __re
 // survivors' stars 32 at a time, queues the hits and splats them 32 at a
 // time, one per lane, into the lane's cell registers (the per-star form of
 // the brightness, star_fast); the warp's sums go to the unit's slot.
+// Three blocks per SM (85 registers, a few spilled): the kernel is bound by
+// instruction fetch and more resident warps hide it (13.7 -> 13.2 ms per 4K
+// frame against two blocks; four blocks spilled too much to gain more).
 template <int kStep>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 k_star_units(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh, StarSet S,
              Cam7 cam, int M, const float2* __restrict__ view, int lr,
              const float* __restrict__ area, const uint32_t* __restrict__ heavy,
@@ -495,42 +518,22 @@ k_star_units(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh, S
       const int q = sh_q[w][q_at];
       const float2 pos = sh_qpos[w][q_at];
       const StarHit h = star_hit(P, S, q, pos.x, pos.y);
-      const StarFast f = star_fast(P, S, h);
-#pragma unroll
-      for (int c = 0; c < FW2; c++) {
-        float3 l;
-        if (cell_light_fast(P, h, f, c / FW, c % FW, l)) {
-          acc[c].x += l.x;
-          acc[c].y += l.y;
-          acc[c].z += l.z;
-        }
-      }
+      splat_cells<kStep>(P, h, star_fast(P, S, h), acc);
     };
-    for (uint32_t f = f0; f < f1; f += 32) {
-      const uint32_t kk = f + lane;
-      int leaf = -1;
-      if (kk < f1) {
-        uint32_t a = n0, b = n1 - 1;  // first node whose leaves reach past kk
-        while (a < b) {
-          const uint32_t mid = (a + b) >> 1;
-          if (pend[mid] > kk) b = mid;
-          else a = mid + 1;
-        }
-        const int node = pool[a];
-        const int d = L - node_level(node);
-        const uint32_t start = a > n0 ? pend[a - 1] : 0u;
-        leaf = (int)((((long long)node + 1) << d) - 1 + (kk - start));
-        if (node_excluded(P, S.box[leaf])) leaf = -1;
-      }
-      unsigned keep = __ballot_sync(0xffffffffu, leaf >= 0);
-      while (keep) {
-        const int src = __ffs(keep) - 1;
-        keep &= keep - 1;
-        const int lf = __shfl_sync(0xffffffffu, leaf, src);
-        int a0, a1;
-        node_range(S, lf, a0, a1);
-        for (int qb = a0; qb < a1; qb += 32) {
+    // One loop that tests until 32 hits are queued (or the unit is done) and
+    // then splats them, so that the splat has a single call site: the kernel
+    // is bound by instruction fetch, and a second inlined copy of the splat
+    // for the last hits doubled its hot code.
+    uint32_t f = f0;     // next batch of 32 candidate leaves
+    unsigned keep = 0;   // batch lanes whose leaf survived the box test
+    int leaf = -1;       // this lane's leaf of the batch
+    int qb = 0, a1 = 0;  // star range left of the current leaf
+    for (;;) {
+      bool done = false;
+      while (qn < 32) {
+        if (qb < a1) {
           const int q = qb + lane;
+          qb += 32;
           float st = 0.f, sp = 0.f;
           const bool in = q < a1 && star_test(P, S, q, st, sp);
           const unsigned ball = __ballot_sync(0xffffffffu, in);
@@ -542,23 +545,49 @@ k_star_units(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh, S
             sh_qpos[w][at] = make_float2(st, sp);
           }
           qn += __popc(ball);
-          if (qn >= 32) {
-            __syncwarp();
-            splat_queued(lane);
-            __syncwarp();
-            if (lane < qn - 32) {
-              sh_q[w][lane] = sh_q[w][lane + 32];
-              sh_qpos[w][lane] = sh_qpos[w][lane + 32];
+        } else if (keep) {
+          const int src = __ffs(keep) - 1;
+          keep &= keep - 1;
+          node_range(S, __shfl_sync(0xffffffffu, leaf, src), qb, a1);
+        } else if (f < f1) {
+          const uint32_t kk = f + lane;
+          f += 32;
+          leaf = -1;
+          if (kk < f1) {
+            uint32_t a = n0, b = n1 - 1;  // first node whose leaves reach past kk
+            while (a < b) {
+              const uint32_t mid = (a + b) >> 1;
+              if (pend[mid] > kk) b = mid;
+              else a = mid + 1;
             }
-            qn -= 32;
-            __syncwarp();
+            const int node = pool[a];
+            const int d = L - node_level(node);
+            const uint32_t start = a > n0 ? pend[a - 1] : 0u;
+            leaf = (int)((((long long)node + 1) << d) - 1 + (kk - start));
+            if (node_excluded(P, S.box[leaf])) leaf = -1;
           }
+          keep = __ballot_sync(0xffffffffu, leaf >= 0);
+        } else {
+          done = true;
+          break;
         }
       }
+      if (qn == 0) break;
+      __syncwarp();
+      if (lane < qn) splat_queued(lane);
+      __syncwarp();
+      if (qn > 32) {
+        if (lane < qn - 32) {
+          sh_q[w][lane] = sh_q[w][lane + 32];
+          sh_qpos[w][lane] = sh_qpos[w][lane + 32];
+        }
+        qn -= 32;
+      } else {
+        qn = 0;
+      }
+      __syncwarp();
+      if (done && qn == 0) break;
     }
-    __syncwarp();
-    if (lane < qn) splat_queued(lane);
-    __syncwarp();
     float* out = partial + (size_t)u * (FW2 * 3);
 #pragma unroll
     for (int c = 0; c < FW2; c++) {
@@ -670,16 +699,7 @@ k_star_heavy(const float2* __restrict__ thphi, const uint8_t* __restrict__ bh,
       const int q = sh_q[w][k];
       const float2 pos = sh_qpos[w][k];
       const StarHit h = star_hit(P, S, q, pos.x, pos.y);
-      const StarFast f = star_fast(P, S, h);
-#pragma unroll
-      for (int c = 0; c < FW2; c++) {
-        float3 l;
-        if (cell_light_fast(P, h, f, c / FW, c % FW, l)) {
-          acc[c].x += l.x;
-          acc[c].y += l.y;
-          acc[c].z += l.z;
-        }
-      }
+      splat_cells<kStep>(P, h, star_fast(P, S, h), acc);
     };
     for (;;) {
       if (tid == 0) {

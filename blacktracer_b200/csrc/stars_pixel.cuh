@@ -107,6 +107,8 @@ BT_HD void in_pixel(float t0, float t1, float t2, float t3, float p0,
   float midT = (t0 + t1 + t2 + t3) * .25f;
   float midP = (p0 + p1 + p2 + p3) * .25f;
   float y = 0.5f, x = 0.5f, perc = 0.5f;
+  // kept rolled: the star kernels are bound by instruction fetch
+#pragma unroll 1
   for (int q = 0; q < 10; q++) {
     if ((fabsf(st - midT) < error) && (fabsf(sp - midP) < error)) break;
     const float h01T = (t0 + t1) * .5f, h23T = (t2 + t3) * .5f;
@@ -522,7 +524,7 @@ BT_HD StarFast star_fast(const PixelStars& P, const StarSet& S, const StarHit& h
 }
 
 // cell_light kept out of line for the rare stars star_fast does not cover,
-// so that the unrolled cell loops around cell_light_fast stay small.
+// so that the unrolled cell loops stay small.
 #ifdef __CUDA_ARCH__
 __device__ __noinline__
 #else
@@ -535,9 +537,6 @@ bool cell_light_slow(int step, float maxDistSq, float frac, float st, float sp, 
 
 BT_HD bool cell_light_fast(const PixelStars& P, const StarHit& h, const StarFast& f,
                            int u, int v, float3& out) {
-  if (!f.ok)
-    return cell_light_slow(P.step, P.maxDistSq, P.frac, h.st, h.sp, h.part, h.hsp.x,
-                           h.hsp.y, h.hsp.z, u, v, out);
   const float dist = dist_sq(-P.step + u + .5f, h.st, -P.step + v + .5f, h.sp);
   if (dist > P.maxDistSq) return false;
   // gaussian(dist) = exp(-dist / (2 sigma^2)) / (sigma sqrt(2 pi)), sigma = 0.4
@@ -550,6 +549,38 @@ BT_HD bool cell_light_fast(const PixelStars& P, const StarHit& h, const StarFast
   const float r = f.r0 * b, g = f.g0 * b, bl = f.bl0 * b;
   out = make_float3(r * r, g * g, bl * bl);
   return true;
+}
+
+// A star's (2 kStep + 1)^2 cells added into acc: the per-star form where it
+// applies (f.ok), else cell_light.  Two separate unrolled loops, so that the
+// hot one carries none of the rare one's call set-up (the star kernels are
+// bound by instruction fetch).
+template <int kStep>
+BT_HD void splat_cells(const PixelStars& P, const StarHit& h, const StarFast& f,
+                       float3* acc) {
+  constexpr int FW = 2 * kStep + 1, FW2 = FW * FW;
+  if (f.ok) {
+#pragma unroll
+    for (int c = 0; c < FW2; c++) {
+      float3 l;
+      if (cell_light_fast(P, h, f, c / FW, c % FW, l)) {
+        acc[c].x += l.x;
+        acc[c].y += l.y;
+        acc[c].z += l.z;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int c = 0; c < FW2; c++) {
+      float3 l;
+      if (cell_light_slow(P.step, P.maxDistSq, P.frac, h.st, h.sp, h.part, h.hsp.x,
+                          h.hsp.y, h.hsp.z, c / FW, c % FW, l)) {
+        acc[c].x += l.x;
+        acc[c].y += l.y;
+        acc[c].z += l.z;
+      }
+    }
+  }
 }
 
 #undef BT_HD
