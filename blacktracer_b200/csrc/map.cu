@@ -488,27 +488,51 @@ __global__ void k_env(const float2* __restrict__ thphi, uchar4* __restrict__ out
 }
 
 // Adds the per-column differences d of 32 consecutive columns (one per lane,
-// `n` of them valid, lane order = column order) to `color` one after the
-// other, as the reference's sequential loop does; every lane ends with the
-// same color.
-__device__ __forceinline__ void add_in_order(float4& color, float4 d, int n) {
-  for (int b = 0; b < n; b++) {
-    color.x += __shfl_sync(0xffffffffu, d.x, b);
-    color.y += __shfl_sync(0xffffffffu, d.y, b);
-    color.z += __shfl_sync(0xffffffffu, d.z, b);
-    color.w += __shfl_sync(0xffffffffu, d.w, b);
+// lane order = column order; lanes [first, last] valid) to `color` one after
+// the other, as the reference's sequential loop does; every lane ends with
+// the same color.  The values pass through the warp's 32 float4 of shared
+// memory (one broadcast load per column instead of four shuffles; the
+// kernel is bound by issue, and this sum is most of its instructions).
+__device__ __forceinline__ void add_in_order(float4& color, float4 d, int first, int last,
+                                             float4* sh) {
+  const int lane = threadIdx.x & 31;
+  __syncwarp();
+  sh[lane] = d;
+  __syncwarp();
+  if (first == 0 && last == 31) {
+#pragma unroll
+    for (int b = 0; b < 32; b++) {
+      const float4 v = sh[b];
+      color.x += v.x;
+      color.y += v.y;
+      color.z += v.z;
+      color.w += v.w;
+    }
+  } else {
+    for (int b = first; b <= last; b++) {
+      const float4 v = sh[b];
+      color.x += v.x;
+      color.y += v.y;
+      color.z += v.z;
+      color.w += v.w;
+    }
   }
 }
 
 // The wide pixels of k_env, one warp each: 32 columns per step, the running
 // theta extremes of the reference as a warp prefix max/min, column sums
 // added in column order (bit-identical to the per-thread loop).
-__global__ void k_env_wide(const float2* __restrict__ thphi, uchar4* __restrict__ out,
+constexpr int kEnvWideThreads = 256;
+
+__global__ void __launch_bounds__(kEnvWideThreads)
+k_env_wide(const float2* __restrict__ thphi, uchar4* __restrict__ out,
                            int rows, int cols, int M, const float4* __restrict__ sat,
                            Cam7 cam, const float* __restrict__ solidangle,
                            const float2* __restrict__ view, int lr,
                            const uint32_t* __restrict__ wide, const uint32_t* nwide) {
   const int lane = threadIdx.x & 31;
+  __shared__ float4 sh_d[kEnvWideThreads / 32][32];
+  float4* sh = sh_d[threadIdx.x >> 5];
   const uint32_t n = *nwide;
   const long total = (long)rows * cols;
   const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
@@ -565,14 +589,7 @@ __global__ void k_env_wide(const float2* __restrict__ thphi, uchar4* __restrict_
           d = make_float4(mx.x - mn.x, mx.y - mn.y, mx.z - mn.z, mx.w - mn.w);
         }
         // columns s >= 1 only: lane 0 of the first step holds boundary 0
-        const int first = s0 == 0 ? 1 : 0;
-        const int last = min(31, pixNum - s0);
-        for (int b = first; b <= last; b++) {
-          color.x += __shfl_sync(0xffffffffu, d.x, b);
-          color.y += __shfl_sync(0xffffffffu, d.y, b);
-          color.z += __shfl_sync(0xffffffffu, d.z, b);
-          color.w += __shfl_sync(0xffffffffu, d.w, b);
-        }
+        add_in_order(color, d, s0 == 0 ? 1 : 0, min(31, pixNum - s0), sh);
         cmax = __shfl_sync(0xffffffffu, lmax, 31);
         cmin = __shfl_sync(0xffffffffu, lmin, 31);
       }
@@ -590,7 +607,7 @@ __global__ void k_env_wide(const float2* __restrict__ thphi, uchar4* __restrict_
           const float4 mn = sat_lin(sat, thMinPix + col, total);
           d = make_float4(mx.x - mn.x, mx.y - mn.y, mx.z - mn.z, mx.w - mn.w);
         }
-        add_in_order(color, d, min(32, pixNum - q0));
+        add_in_order(color, d, 0, min(31, pixNum - q0 - 1), sh);
       }
     }
     const uchar4 px = env_finish(color, t, p, M, ind, cam, view, solidangle[ij], lr);
@@ -629,7 +646,7 @@ int map_run_envmap(MapScratch& S, const MapFrame& F, cudaStream_t s) {
     k_env<<<grid2(M, N), dim3(TX, TY), 0, s>>>(
         S.thphi, (uchar4*)F.out_bg, S.bh, F.env->rows, F.env->cols, M, N,
         F.env->sat, F.cam, S.area, F.view, F.lr, S.env_wide, S.env_wide_count);
-    k_env_wide<<<sm_count() * 8, 256, 0, s>>>(
+    k_env_wide<<<sm_count() * 8, kEnvWideThreads, 0, s>>>(
         S.thphi, (uchar4*)F.out_bg, F.env->rows, F.env->cols, M, F.env->sat, F.cam,
         S.area, F.view, F.lr, S.env_wide, S.env_wide_count);
     BT_CUDA_TRY(cudaGetLastError());
