@@ -36,8 +36,10 @@ __global__ void k_view_sphere(float2* view, int W, int H) {
 }
 
 // pixInterpolation, G = 1 (BT/MakeImageKernel.cu:458-515): celestial
-// (theta, phi) and block size at every pixel corner.
-__global__ void k_pixinterp(const float2* __restrict__ view, int M, int N,
+// (theta, phi) and block size at every pixel corner.  Bound by the latency
+// of its grid reads: six blocks per SM (40 registers) instead of three.
+__global__ void __launch_bounds__(TX * TY, 6)
+k_pixinterp(const float2* __restrict__ view, int M, int N,
                             GridRef G, int gridlvl, float hor, float ver,
                             float2* __restrict__ thphi, int* __restrict__ gap) {
   const int j = blockIdx.x * TX + threadIdx.x;
