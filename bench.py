@@ -825,7 +825,10 @@ def main():
         for prec in ("plain", "fast", "mixed"):
             Sb = bt.GridSet(BATCH["maxlevel"], BATCH["startlevel"], True, BATCH["count"],
                             opts=prec)
-            shape, _ = Sb.autotune(cams_b, spins_b, repeats=1)
+            tuned = Sb.tune(cams_b, spins_b, p99_target=1e-6, repeats=1)
+            if tuned["flow"]:
+                Sb.set_flow(True, blocks_per_sm=tuned["flow"])
+            shape = tuned["shape"]
             Sb.set_graph(True)
             for _ in range(3):
                 Sb.build(cams_b, spins_b)
@@ -842,7 +845,11 @@ def main():
             rays = Sb.traced
             res[prec] = {"value": rays / (ms / 1e3), "unit": "geodesics/s",
                          "ms_per_set": ms, "rays_per_set": rays,
-                         "trace_shape": {"threads": shape[0], "blocks_per_sm": shape[1]},
+                         "trace_shape": {"threads": shape[0], "blocks_per_sm": shape[1],
+                                         "refill": shape[2]},
+                         "tuner": {k: tuned[k] for k in ("flow", "level_ms", "flow_ms",
+                                                         "candidates", "fp64_band",
+                                                         "band_met", "band_p99_rad")},
                          "launches_per_set": int(Sb.info().launches)}
             if prec != "mixed":
                 # FP64 work of the set per build over the whole build time
@@ -872,10 +879,11 @@ def main():
                 e1.record(stream)
                 torch.cuda.synchronize()
                 ms_f = e0.elapsed_time(e1) / nb_steps
-                res[prec]["one_launch"] = {"ms_per_set": ms_f, "value": rays / (ms_f / 1e3),
-                                           "speed_vs_level": ms / ms_f, "blocks_per_sm": 2,
-                                           "flags": int(Sb.info().flags)}
-                Sb.set_flow(False)
+                res[prec]["one_launch"] = {
+                    "ms_per_set": ms_f, "value": rays / (ms_f / 1e3),
+                    "speed_vs_level": ms / ms_f if not tuned["flow"] else None,
+                    "blocks_per_sm": 2, "flags": int(Sb.info().flags)}
+                Sb.set_flow(bool(tuned["flow"]), blocks_per_sm=tuned["flow"] or 2)
             sets[prec] = Sb
         for prec in ("fast", "mixed"):
             p99, mx, topo = set_error_vs(sets["plain"], sets[prec])
@@ -884,7 +892,9 @@ def main():
         batched = {"workload": f"{BATCH['count']} poses, adaptive L6->L9 (512x1024 "
                                "equivalent), static cameras r in [4M,40M], theta in "
                                "[0.1, pi-0.1], a in [0, 0.999], seeded; one set per step, "
-                               "CUDA graph replay, launch shape from the autotuner",
+                               "CUDA graph replay, configuration from the autotuner "
+                               "(bt_batch_tune: trace shape x refill, level or one-launch "
+                               "build; the mixed form's FP64 band by a 1e-6 rad p99 target)",
                    "plain": res["plain"], "fast": res["fast"], "mixed": res["mixed"],
                    "speedup_vs_plain_set": {
                        k: res[k]["value"] / res["plain"]["value"] for k in ("fast", "mixed")}}

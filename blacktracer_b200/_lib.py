@@ -54,7 +54,14 @@ class bt_grid_export_t(C.Structure):
 
 
 class bt_trace_shape(C.Structure):
-    _fields_ = [("threads", C.c_int32), ("blocks_per_sm", C.c_int32)]
+    _fields_ = [("threads", C.c_int32), ("blocks_per_sm", C.c_int32), ("refill", C.c_int32)]
+
+
+class bt_tune_result(C.Structure):
+    _fields_ = [("shape", bt_trace_shape), ("flow", C.c_int32), ("band_met", C.c_int32),
+                ("fp64_band", C.c_double), ("band_p99_rad", C.c_double),
+                ("best_ms", C.c_float), ("level_ms", C.c_float), ("flow_ms", C.c_float),
+                ("candidates", C.c_int32)]
 
 
 class bt_batch_info(C.Structure):
@@ -166,6 +173,9 @@ _SIGS = {
     "bt_batch_autotune": (C.c_int, [_vp, C.POINTER(bt_camera), C.POINTER(C.c_double), C.c_int,
                                     C.POINTER(bt_integ_opts), C.c_int,
                                     C.POINTER(bt_trace_shape), C.POINTER(C.c_float), _vp]),
+    "bt_batch_tune": (C.c_int, [_vp, C.POINTER(bt_camera), C.POINTER(C.c_double), C.c_int,
+                                C.POINTER(bt_integ_opts), C.c_double, C.c_int,
+                                C.POINTER(bt_tune_result), _vp]),
     "bt_probe_fp64_tflops": (C.c_int, [C.POINTER(C.c_double), _vp]),
     "bt_view_sphere": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "bt_env_create": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp), _vp]),

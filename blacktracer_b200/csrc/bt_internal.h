@@ -113,10 +113,12 @@ struct GridDesc {
 };
 
 // Launch shape of the ray-tracing kernel: threads per block (64, 128 or
-// 256) and resident blocks per SM (0 = as many as fit).
+// 256), resident blocks per SM (0 = as many as fit) and the number of idle
+// lanes a warp waits for before it refills them (0 = kRefillMin).
 struct TraceShape {
   int threads;
   int blocks_per_sm;
+  int refill;
 };
 
 // Traces the listed vertices of all G grids in one persistent launch: the

@@ -36,9 +36,11 @@
 //
 // Compiled with --fmad=false (the fix's FP64 Hermite must round like the
 // reference's host build).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "bt_internal.h"
 #include "grid_flow.cuh"
@@ -958,7 +960,7 @@ int batch_create(int maxlevel, int angle, int count, bt_batch** out) {
   b->eq = angle ? 1 : 0;
   b->maxlevel = maxlevel;
   b->NM = (size_t)N * M;
-  b->shape = TraceShape{128, 0};
+  b->shape = TraceShape{128, 0, 0};
   b->tfix_passes = bt::kMaxTfixPasses;
   b->grids = new (std::nothrow) bt_grid[count];
   if (!b->grids) {
@@ -1201,7 +1203,8 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int n,
                       b->exec_tfix_passes == b->tfix_passes &&
                       b->exec_flow == b->flow &&
                       b->exec_shape.threads == b->shape.threads &&
-                      b->exec_shape.blocks_per_sm == b->shape.blocks_per_sm;
+                      b->exec_shape.blocks_per_sm == b->shape.blocks_per_sm &&
+                      b->exec_shape.refill == b->shape.refill;
     if (!same) {
       if (b->exec) cudaGraphExecDestroy(b->exec);
       b->exec = nullptr;
@@ -1548,7 +1551,8 @@ int bt_batch_set_shape(bt_batch* b, const bt_trace_shape* shape) {
                "threads must be 64, 128 or 256");
   BT_ARG_CHECK(shape->blocks_per_sm >= 0 && shape->blocks_per_sm <= 32,
                "blocks_per_sm out of [0, 32]");
-  b->shape = TraceShape{shape->threads, shape->blocks_per_sm};
+  BT_ARG_CHECK(shape->refill >= 0 && shape->refill <= 32, "refill out of [0, 32]");
+  b->shape = TraceShape{shape->threads, shape->blocks_per_sm, shape->refill};
   return BT_OK;
 }
 
@@ -1570,6 +1574,7 @@ int bt_batch_query(bt_batch* b, bt_batch_info* info, void* stream) {
   info->graph = b->graph;
   info->shape.threads = b->shape.threads;
   info->shape.blocks_per_sm = b->shape.blocks_per_sm;
+  info->shape.refill = b->shape.refill;
   if (info->flags) {
     set_error("grid set build flags 0x%x", info->flags);
     return BT_ERR_NUMERIC;
@@ -1621,8 +1626,225 @@ int bt_batch_autotune(bt_batch* b, const bt_camera* cams, const double* spins, i
   if (best) {
     best->threads = best_s.threads;
     best->blocks_per_sm = best_s.blocks_per_sm;
+    best->refill = best_s.refill;
   }
   if (best_ms) *best_ms = best_t;
+  return BT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+constexpr double kTunePi = 3.14159265358979323846;
+
+// splitmix64: the tuner's seeded sample directions.
+uint64_t tune_mix(uint64_t& x) {
+  uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// p99 of max(|d theta|, |d phi| wrapped to [-pi, pi]) over the rays that
+// escaped in both runs; -1 when there are none.
+double tune_p99(const std::vector<double>& t0, const std::vector<double>& p0,
+                const std::vector<uint8_t>& s0, const std::vector<double>& t1,
+                const std::vector<double>& p1, const std::vector<uint8_t>& s1) {
+  std::vector<double> e;
+  e.reserve(t0.size());
+  for (size_t k = 0; k < t0.size(); k++) {
+    if (s0[k] != BT_RAY_ESCAPED || s1[k] != BT_RAY_ESCAPED) continue;
+    double dp = std::fabs(p0[k] - p1[k]);
+    dp = std::fmod(dp, 2 * kTunePi);
+    if (dp > kTunePi) dp = 2 * kTunePi - dp;
+    e.push_back(std::max(std::fabs(t0[k] - t1[k]), dp));
+  }
+  if (e.empty()) return -1;
+  const size_t at = std::min(e.size() - 1, (size_t)std::ceil(0.99 * (double)e.size()) - 1);
+  std::nth_element(e.begin(), e.begin() + at, e.end());
+  return e[at];
+}
+
+// The MIXED form's FP64 band by accuracy (see bt_batch_tune).
+int tune_band(const bt_camera* cams, const double* spins, int G, const bt_integ_opts& o,
+              double target, cudaStream_t s, double* band, double* p99, int* met) {
+  static const double cand[] = {0.05, 0.1, 0.2, 0.5, 1.0, 2.0, 5.0};
+  const int ncam = std::min(G, 8), per = 2048;
+  const size_t n = (size_t)ncam * per;
+  std::vector<double> th(n), ph(n);
+  uint64_t seed = 20261204;
+  for (size_t k = 0; k < n; k++) {
+    const double u = (double)(tune_mix(seed) >> 11) * 0x1.0p-53;
+    const double v = (double)(tune_mix(seed) >> 11) * 0x1.0p-53;
+    th[k] = std::acos(1 - 2 * u);
+    ph[k] = 2 * kTunePi * v;
+  }
+  double* d = nullptr;  // th, ph, theta out, phi out
+  int32_t* steps = nullptr;
+  uint8_t* st = nullptr;
+  cudaError_t e = cudaMalloc((void**)&d, 4 * n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&steps, n * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&st, n);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    cudaFree(steps);
+    set_error("tuner sample buffers: %s", cudaGetErrorString(e));
+    return BT_ERR_NOMEM;
+  }
+  int rc = BT_OK;
+  auto run = [&](const bt_integ_opts& oo, std::vector<double>& to, std::vector<double>& po,
+                 std::vector<uint8_t>& so) -> int {
+    for (int c = 0; c < ncam; c++) {
+      const size_t at = (size_t)c * per;
+      if (int r = bt_integrate_rays(&cams[c], spins[c], d + at, d + n + at, per, d + 2 * n + at,
+                                    d + 3 * n + at, steps + at, st + at, &oo, s))
+        return r;
+    }
+    to.resize(n);
+    po.resize(n);
+    so.resize(n);
+    if (cudaMemcpyAsync(to.data(), d + 2 * n, n * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(po.data(), d + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(so.data(), st, n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      set_error("tuner sample copies failed");
+      return BT_ERR_CUDA;
+    }
+    return BT_OK;
+  };
+  std::vector<double> t0, p0, t1, p1;
+  std::vector<uint8_t> s0, s1;
+  if (cudaMemcpyAsync(d, th.data(), n * sizeof(double), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(d + n, ph.data(), n * sizeof(double), cudaMemcpyHostToDevice, s) !=
+          cudaSuccess) {
+    set_error("tuner sample copies failed");
+    rc = BT_ERR_CUDA;
+  }
+  bt_integ_opts op = o;
+  op.precision = BT_PRECISION_PLAIN;
+  if (rc == BT_OK) rc = run(op, t0, p0, s0);
+  double best_e = 3.4e38;
+  *met = 0;
+  for (double c : cand) {
+    if (rc) break;
+    bt_integ_opts om = o;
+    om.fp64_band = c;
+    if ((rc = run(om, t1, p1, s1))) break;
+    const double q = tune_p99(t0, p0, s0, t1, p1, s1);
+    if (q >= 0 && q <= target) {
+      *band = c;
+      *p99 = q;
+      *met = 1;
+      break;
+    }
+    if (q >= 0 && q < best_e) {
+      best_e = q;
+      *band = c;
+      *p99 = q;
+    }
+  }
+  cudaFree(d);
+  cudaFree(steps);
+  cudaFree(st);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bt_batch_tune(bt_batch* b, const bt_camera* cams, const double* spins, int startlevel,
+                  const bt_integ_opts* o, double p99_target_rad, int repeats,
+                  bt_tune_result* out, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(b && cams && spins && out, "NULL pointer");
+  BT_ARG_CHECK(repeats >= 1 && repeats <= 100, "repeats out of [1, 100]");
+  BT_ARG_CHECK(p99_target_rad > 0, "p99 target must be positive");
+  cudaStream_t s = (cudaStream_t)stream;
+  bt_integ_opts opt;
+  if (o) opt = *o;
+  else bt_integ_opts_default(&opt);
+  std::memset(out, 0, sizeof(*out));
+  out->fp64_band = opt.fp64_band;
+  out->band_p99_rad = -1;
+  if (opt.precision == BT_PRECISION_MIXED) {
+    if (int rc = tune_band(cams, spins, b->G, opt, p99_target_rad, s, &out->fp64_band,
+                           &out->band_p99_rad, &out->band_met))
+      return rc;
+    opt.fp64_band = out->fp64_band;
+  }
+  // configurations: level builds (shape x refill), then one-launch builds
+  struct Conf {
+    TraceShape shape;
+    int flow;
+  };
+  std::vector<Conf> conf;
+  static const TraceShape shapes[] = {{128, 0, 0}, {128, 4, 0}, {128, 5, 0}, {64, 0, 0},
+                                      {256, 0, 0}};
+  for (const TraceShape& sh : shapes)
+    for (int r : {4, 8, 16}) conf.push_back({TraceShape{sh.threads, sh.blocks_per_sm, r}, 0});
+  for (int f : {1, 2}) conf.push_back({b->shape, f});
+  const TraceShape saved = b->shape;
+  const int saved_flow = b->flow, graph = b->graph;
+  b->graph = 0;  // time eager builds; the chosen configuration is captured later
+  cudaEvent_t e0, e1;
+  BT_CUDA_TRY(cudaEventCreate(&e0));
+  BT_CUDA_TRY(cudaEventCreate(&e1));
+  float best_t = 3.4e38f, best_level = 3.4e38f, best_flow = 3.4e38f;
+  Conf best = {saved, saved_flow};
+  int rc = BT_OK;
+  for (const Conf& c : conf) {
+    b->shape = c.shape;
+    if (c.flow) {
+      if (batch_set_flow(b, c.flow) != BT_OK) {  // no room for its buffers: skip
+        clear_error();
+        b->flow = 0;
+        continue;
+      }
+    } else {
+      b->flow = 0;
+    }
+    if ((rc = batch_build(b, cams, spins, b->G, startlevel, &opt, s))) break;  // warm-up
+    float t_min = 3.4e38f;
+    for (int r = 0; r < repeats && rc == BT_OK; r++) {
+      cudaEventRecord(e0, s);
+      rc = batch_build(b, cams, spins, b->G, startlevel, &opt, s);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = BT_ERR_CUDA;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < t_min) t_min = ms;
+    }
+    if (rc) break;
+    out->candidates++;
+    if (c.flow) best_flow = std::min(best_flow, t_min);
+    else best_level = std::min(best_level, t_min);
+    if (t_min < best_t) {
+      best_t = t_min;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->graph = graph;
+  if (rc) {
+    b->shape = saved;
+    b->flow = saved_flow;
+    return rc;
+  }
+  b->shape = best.shape;
+  b->flow = best.flow;
+  out->shape.threads = best.shape.threads;
+  out->shape.blocks_per_sm = best.shape.blocks_per_sm;
+  out->shape.refill = best.shape.refill;
+  out->flow = best.flow;
+  out->best_ms = best_t;
+  out->level_ms = best_level < 3.4e38f ? best_level : 0.f;
+  out->flow_ms = best_flow < 3.4e38f ? best_flow : 0.f;
   return BT_OK;
 }
 

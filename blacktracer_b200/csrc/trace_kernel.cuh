@@ -112,7 +112,7 @@ __device__ __forceinline__ plain::RayStart lattice_start(const GridDesc& d, uint
 template <class Policy, int kThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks)
 k_trace_lattice(const GridDesc* __restrict__ D, int G,
-                const uint32_t* __restrict__ qoff, uint32_t* qfetch) {
+                const uint32_t* __restrict__ qoff, uint32_t* qfetch, int refill) {
   const uint32_t n = qoff[G];
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -124,7 +124,7 @@ k_trace_lattice(const GridDesc* __restrict__ D, int G,
     const bool need = slot == kLaneIdle;
     const unsigned m = __ballot_sync(0xffffffffu, need);
     const unsigned busy = __ballot_sync(0xffffffffu, slot < kLaneDone);
-    if (m && (__popc(m) >= kRefillMin || !busy)) {
+    if (m && (__popc(m) >= refill || !busy)) {
       const int leader = __ffs(m) - 1;
       uint32_t base = 0;
       if ((int)lane == leader) base = atomicAdd(qfetch, (uint32_t)__popc(m));
@@ -180,7 +180,8 @@ int launch_trace_shape(const GridDesc* D, int G, const uint32_t* qoff,
     int per_sm = per_sm_max;
     if (shape.blocks_per_sm > 0 && shape.blocks_per_sm < per_sm) per_sm = shape.blocks_per_sm;
     k_setup_lattice<Policy><<<sm_count() * 8, 128, 0, s>>>(D, G, qoff);
-    kernel<<<sm_count() * per_sm, threads, 0, s>>>(D, G, qoff, qfetch);
+    const int refill = shape.refill > 0 ? shape.refill : kRefillMin;
+    kernel<<<sm_count() * per_sm, threads, 0, s>>>(D, G, qoff, qfetch, refill);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
       set_error("trace launch: %s", cudaGetErrorString(e));

@@ -400,9 +400,34 @@ class GridSet:
         of `blocks_per_sm` blocks of 256 threads per SM."""
         L.check(L.lib().bt_batch_set_flow(self._h, blocks_per_sm if on else 0))
 
-    def set_shape(self, threads=128, blocks_per_sm=0):
-        s = L.bt_trace_shape(threads, blocks_per_sm)
+    def set_shape(self, threads=128, blocks_per_sm=0, refill=0):
+        """Trace launch shape of level builds: threads per block, resident
+        blocks per SM (0: as many as fit), idle lanes a warp refills at once
+        (0: 8)."""
+        s = L.bt_trace_shape(threads, blocks_per_sm, refill)
         L.check(L.lib().bt_batch_set_shape(self._h, C.byref(s)))
+
+    def tune(self, cameras, spins, p99_target=1e-6, repeats=2):
+        """The full autotuner (bt_batch_tune): for the mixed form the FP64
+        band by accuracy against the plain form, then the fastest of the level
+        builds (trace shape x refill size) and the one-launch builds; the set
+        keeps it, and a mixed set's options take the chosen band.  Returns a
+        dict of the choice."""
+        cams, a = self._arrays(cameras, spins)
+        r = L.bt_tune_result()
+        L.check(L.lib().bt_batch_tune(self._h, cams, a, self.STARTLVL, self.opts.ref,
+                                      float(p99_target), int(repeats), C.byref(r),
+                                      _stream_ptr(self._stream)))
+        for g in self.grids:
+            g._info, g._map = None, None
+        self._info = None
+        if self.opts._o.precision == L.PRECISION_MIXED:
+            self.opts._o.fp64_band = r.fp64_band
+        return {"shape": (r.shape.threads, r.shape.blocks_per_sm, r.shape.refill),
+                "flow": int(r.flow), "fp64_band": float(r.fp64_band),
+                "band_met": bool(r.band_met), "band_p99_rad": float(r.band_p99_rad),
+                "best_ms": float(r.best_ms), "level_ms": float(r.level_ms),
+                "flow_ms": float(r.flow_ms), "candidates": int(r.candidates)}
 
     def autotune(self, cameras, spins, repeats=2):
         """Times the candidate trace launch shapes on these cameras, keeps

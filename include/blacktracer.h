@@ -294,8 +294,9 @@ int bt_batch_set_flow(bt_batch* b, int on);
 /* Launch shape of the persistent ray-tracing kernel: threads per block
  * (64, 128 or 256) and resident blocks per SM (0 = as many as fit). */
 typedef struct bt_trace_shape {
-  int32_t threads;
-  int32_t blocks_per_sm;
+  int32_t threads;        /* 64, 128 or 256                                 */
+  int32_t blocks_per_sm;  /* 0: as many as fit                             */
+  int32_t refill;         /* idle lanes a warp refills at once (0: 8)      */
 } bt_trace_shape;
 int bt_batch_set_shape(bt_batch* b, const bt_trace_shape* shape);
 
@@ -317,6 +318,36 @@ int bt_batch_query(bt_batch* b, bt_batch_info* info, void* stream);
 int bt_batch_autotune(bt_batch* b, const bt_camera* cams, const double* spins,
                       int startlevel, const bt_integ_opts* o, int repeats,
                       bt_trace_shape* best, float* best_ms, void* stream);
+
+typedef struct bt_tune_result {
+  bt_trace_shape shape;  /* level builds: trace launch shape and refill size  */
+  int32_t flow;          /* 0: level builds; k >= 1: one launch, k blocks/SM  */
+  int32_t band_met;      /* MIXED: 1 when fp64_band meets the p99 target      */
+  double fp64_band;      /* MIXED: the band chosen; otherwise the option's    */
+  double band_p99_rad;   /* MIXED: its p99 error against PLAIN on the sample
+                            rays; otherwise -1                                */
+  float best_ms;         /* per build of the set, chosen configuration        */
+  float level_ms;        /* fastest level-build configuration                 */
+  float flow_ms;         /* fastest one-launch configuration (0: none ran)    */
+  int32_t candidates;    /* configurations timed                              */
+} bt_tune_result;
+
+/* The full autotuner.  For the MIXED form it first picks the FP64 band
+ * (fp64_band, the FP64-fallback threshold around the photon orbit): the
+ * narrowest of 0.05, 0.1, 0.2, 0.5, 1, 2, 5 M whose p99 angular error
+ * against the PLAIN form, on 2048 seeded directions of each of the first
+ * (up to) 8 cameras, is at most p99_target_rad; when none is, the one with
+ * the smallest error (band_met = 0).  Then it times `repeats` builds of the
+ * set with that band for every configuration: level builds over the trace
+ * launch shapes of bt_batch_autotune and refill sizes 4, 8 and 16 (the rays
+ * per warp step that a warp waits to start together; each lane holds one
+ * ray), and one-launch builds (bt_batch_set_flow) of 1 and 2 blocks per SM.
+ * The set keeps the fastest (shape, refill and form); pass out->fp64_band
+ * in the options of later MIXED builds.  Synchronises `stream`.  No
+ * counterpart in the reference. */
+int bt_batch_tune(bt_batch* b, const bt_camera* cams, const double* spins, int startlevel,
+                  const bt_integ_opts* o, double p99_target_rad, int repeats,
+                  bt_tune_result* out, void* stream);
 
 /* ------------------------------------------------------- per-pixel map */
 

@@ -98,6 +98,39 @@ def test_autotune_keeps_results(bt, cuda):
         assert_same(dense(S.grids[k]), ref[k], f"tuned member {k}")
 
 
+def test_full_tuner(bt, cuda):
+    """bt_batch_tune: the configuration it keeps (level shape with refill size,
+    or one launch) builds the same grids; for the mixed form the FP64 band is
+    picked by its error against the plain form: the narrowest band meets a
+    loose target, none meets an impossible one (the smallest-error band is
+    reported), and the error reported is the one of the band chosen."""
+    cams, spins = cameras(bt, POSES)
+    S = bt.GridSet(ML, SL, True, len(cams), opts="fast")
+    S.build(cams, spins)
+    ref = [dense(g) for g in S.grids]
+    r = S.tune(cams, spins, repeats=1)
+    assert r["candidates"] == 17 and r["best_ms"] > 0 and r["level_ms"] > 0
+    assert r["flow_ms"] > 0 and r["best_ms"] == min(r["level_ms"], r["flow_ms"])
+    assert r["band_p99_rad"] == -1.0
+    sh = S.info().shape
+    if r["flow"] == 0:
+        assert (sh.threads, sh.blocks_per_sm, sh.refill) == r["shape"]
+        assert r["shape"][2] in (4, 8, 16)
+    S.build(cams, spins)
+    assert S.info().flags == 0
+    for k in range(len(cams)):
+        assert_same(dense(S.grids[k]), ref[k], f"tuned member {k}")
+    M = bt.GridSet(ML, SL, True, len(cams), opts="mixed")
+    loose = M.tune(cams, spins, p99_target=1.0, repeats=1)
+    assert loose["band_met"] and loose["fp64_band"] == 0.05
+    assert 0 <= loose["band_p99_rad"] <= 1.0
+    tight = M.tune(cams, spins, p99_target=1e-15, repeats=1)
+    assert not tight["band_met"] and tight["fp64_band"] in (0.05, 0.1, 0.2, 0.5, 1.0, 2.0, 5.0)
+    assert tight["band_p99_rad"] <= loose["band_p99_rad"]
+    assert M.opts._o.fp64_band == tight["fp64_band"]
+    print(f"tuned: fast {r}; mixed band {tight['fp64_band']} p99 {tight['band_p99_rad']:.2e}")
+
+
 def test_lone_grid_graph_replay(bt, cuda):
     cams, spins = cameras(bt, POSES)
     ref, _ = alone(bt, cams[1], spins[1])
