@@ -556,6 +556,8 @@ def main():
                         traced * F_SETUP)
     latency = latency_floor(bt, torch, grid, d, cam, prec_main)
     del d, steps, st_all, integrated
+    # the launch configuration from the project's autotuner (not timed)
+    tuned_main = grid.tune(repeats=3)
 
     for _ in range(args.warmup):
         grid.build()
@@ -590,6 +592,7 @@ def main():
     ref_dense = None
     for prec in [p_ for p_ in ("plain", "fast", "mixed") if p_ != prec_main]:
         gm = bt.Grid(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam, opts=prec)
+        tuned_o = gm.tune(repeats=3)
         for _ in range(3):
             gm.build()
         torch.cuda.synchronize()
@@ -618,7 +621,9 @@ def main():
             "p99_rad_vs_plain": float(torch.quantile(err, 0.99)) if err.numel() else None,
             "max_rad_vs_plain": float(err.max()) if err.numel() else None,
             "topology_exact": bool(torch.equal(dp["exists"], dm["exists"]) and
-                                   torch.equal(dp["blevel"], dm["blevel"]))}
+                                   torch.equal(dp["blevel"], dm["blevel"])),
+            "tuned": {"shape": tuned_o["shape"], "flow": tuned_o["flow"],
+                      "fp64_band": tuned_o["fp64_band"] if prec == "mixed" else None}}
         if prec != "plain":
             other[prec]["error_vs"] = "plain"
         else:
@@ -970,6 +975,11 @@ def main():
                                       "plain": "FP64, reference operation order, no FMA",
                                       "mixed": "FP32 bulk, FP64 guards"}[prec_main],
                        "rays_per_build": traced, "l2": "flushed (256 MB write) before every step",
+                       "launch": {"from": "bt_grid_tune (the project's autotuner), before timing",
+                                  "threads": tuned_main["shape"][0],
+                                  "blocks_per_sm": tuned_main["shape"][1],
+                                  "refill": tuned_main["shape"][2],
+                                  "one_launch_build": tuned_main["flow"]},
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
             "e2e": {"value": e2e_value, "unit": "geodesics/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,

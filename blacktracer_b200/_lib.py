@@ -176,6 +176,9 @@ _SIGS = {
     "bt_batch_tune": (C.c_int, [_vp, C.POINTER(bt_camera), C.POINTER(C.c_double), C.c_int,
                                 C.POINTER(bt_integ_opts), C.c_double, C.c_int,
                                 C.POINTER(bt_tune_result), _vp]),
+    "bt_grid_set_shape": (C.c_int, [_vp, C.POINTER(bt_trace_shape)]),
+    "bt_grid_tune": (C.c_int, [_vp, C.POINTER(bt_integ_opts), C.c_double, C.c_int,
+                               C.POINTER(bt_tune_result), _vp]),
     "bt_probe_fp64_tflops": (C.c_int, [C.POINTER(C.c_double), _vp]),
     "bt_view_sphere": (C.c_int, [_vp, C.c_int, C.c_int, _vp]),
     "bt_env_create": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(_vp), _vp]),

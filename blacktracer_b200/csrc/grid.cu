@@ -1393,6 +1393,24 @@ int bt_grid_set_flow(bt_grid* g, int on) {
   return batch_set_flow(g->set, on);
 }
 
+int bt_grid_set_shape(bt_grid* g, const bt_trace_shape* shape) {
+  clear_error();
+  BT_ARG_CHECK(g != nullptr, "NULL grid");
+  return bt_batch_set_shape(g->set, shape);
+}
+
+int bt_grid_tune(bt_grid* g, const bt_integ_opts* o, double p99_target_rad, int repeats,
+                 bt_tune_result* out, void* stream) {
+  clear_error();
+  BT_ARG_CHECK(g != nullptr, "NULL grid");
+  BT_ARG_CHECK(g->set->standalone, "a member of a set: tune the set");
+  BT_ARG_CHECK(g->built, "grid not built");
+  const bt_camera cam = g->cam;
+  const double a = g->a;
+  return bt_batch_tune(g->set, &cam, &a, g->L.startlevel, o, p99_target_rad, repeats, out,
+                       stream);
+}
+
 int bt_grid_set_tfix_passes(bt_grid* g, int passes) {
   clear_error();
   BT_ARG_CHECK(g != nullptr, "NULL grid");
@@ -1783,8 +1801,10 @@ int bt_batch_tune(bt_batch* b, const bt_camera* cams, const double* spins, int s
     int flow;
   };
   std::vector<Conf> conf;
+  // as many blocks as fit, the capped register budgets, and fewer warps per
+  // SM (a lone grid's longest rays run faster on lightly loaded SMs)
   static const TraceShape shapes[] = {{128, 0, 0}, {128, 4, 0}, {128, 5, 0}, {64, 0, 0},
-                                      {256, 0, 0}};
+                                      {256, 0, 0}, {128, 2, 0}, {128, 1, 0}};
   for (const TraceShape& sh : shapes)
     for (int r : {4, 8, 16}) conf.push_back({TraceShape{sh.threads, sh.blocks_per_sm, r}, 0});
   for (int f : {1, 2}) conf.push_back({b->shape, f});

@@ -165,6 +165,14 @@ def grid_dims(maxlevel: int, angle: bool = True):
     return N.value, M.value
 
 
+def _tune_dict(r) -> dict:
+    return {"shape": (r.shape.threads, r.shape.blocks_per_sm, r.shape.refill),
+            "flow": int(r.flow), "fp64_band": float(r.fp64_band),
+            "band_met": bool(r.band_met), "band_p99_rad": float(r.band_p99_rad),
+            "best_ms": float(r.best_ms), "level_ms": float(r.level_ms),
+            "flow_ms": float(r.flow_ms), "candidates": int(r.candidates)}
+
+
 class Grid:
     """BT/Grid.h:605: Grid(maxLevelPrec, startLevel, angle, camera, bh).
 
@@ -247,6 +255,23 @@ class Grid:
         (blocks checked as soon as their corners are traced; same grids) of
         `blocks_per_sm` blocks of 256 threads per SM."""
         L.check(L.lib().bt_grid_set_flow(self._h, blocks_per_sm if on else 0))
+
+    def set_shape(self, threads=128, blocks_per_sm=0, refill=0):
+        """Trace launch shape of later level builds (as GridSet.set_shape)."""
+        s = L.bt_trace_shape(threads, blocks_per_sm, refill)
+        L.check(L.lib().bt_grid_set_shape(self._h, C.byref(s)))
+
+    def tune(self, p99_target=1e-6, repeats=2):
+        """The full autotuner (bt_grid_tune) on this grid's camera and spin;
+        keeps the fastest configuration, a mixed grid's options take the band
+        chosen.  Returns a dict of the choice (as GridSet.tune)."""
+        r = L.bt_tune_result()
+        L.check(L.lib().bt_grid_tune(self._h, self.opts.ref, float(p99_target), int(repeats),
+                                     C.byref(r), _stream_ptr(self._stream)))
+        self._info, self._map = None, None
+        if self.opts._o.precision == L.PRECISION_MIXED:
+            self.opts._o.fp64_band = r.fp64_band
+        return _tune_dict(r)
 
     def set_tfix_passes(self, passes: int):
         """Jacobi passes of the T-vertex fix per level of later builds (1..8;
@@ -423,11 +448,7 @@ class GridSet:
         self._info = None
         if self.opts._o.precision == L.PRECISION_MIXED:
             self.opts._o.fp64_band = r.fp64_band
-        return {"shape": (r.shape.threads, r.shape.blocks_per_sm, r.shape.refill),
-                "flow": int(r.flow), "fp64_band": float(r.fp64_band),
-                "band_met": bool(r.band_met), "band_p99_rad": float(r.band_p99_rad),
-                "best_ms": float(r.best_ms), "level_ms": float(r.level_ms),
-                "flow_ms": float(r.flow_ms), "candidates": int(r.candidates)}
+        return _tune_dict(r)
 
     def autotune(self, cameras, spins, repeats=2):
         """Times the candidate trace launch shapes on these cameras, keeps

@@ -339,7 +339,8 @@ typedef struct bt_tune_result {
  * (up to) 8 cameras, is at most p99_target_rad; when none is, the one with
  * the smallest error (band_met = 0).  Then it times `repeats` builds of the
  * set with that band for every configuration: level builds over the trace
- * launch shapes of bt_batch_autotune and refill sizes 4, 8 and 16 (the rays
+ * launch shapes of bt_batch_autotune plus 128 threads at 1 and 2 blocks per
+ * SM, and refill sizes 4, 8 and 16 (the rays
  * per warp step that a warp waits to start together; each lane holds one
  * ray), and one-launch builds (bt_batch_set_flow) of 1 and 2 blocks per SM.
  * The set keeps the fastest (shape, refill and form); pass out->fp64_band
@@ -348,6 +349,13 @@ typedef struct bt_tune_result {
 int bt_batch_tune(bt_batch* b, const bt_camera* cams, const double* spins, int startlevel,
                   const bt_integ_opts* o, double p99_target_rad, int repeats,
                   bt_tune_result* out, void* stream);
+
+/* As bt_batch_set_shape / bt_batch_tune for a lone grid (bt_grid_create),
+ * on its last build's camera, spin and start level; the tuned configuration
+ * is kept for later builds. */
+int bt_grid_set_shape(bt_grid* g, const bt_trace_shape* shape);
+int bt_grid_tune(bt_grid* g, const bt_integ_opts* o, double p99_target_rad, int repeats,
+                 bt_tune_result* out, void* stream);
 
 /* ------------------------------------------------------- per-pixel map */
 

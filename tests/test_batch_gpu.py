@@ -109,7 +109,7 @@ def test_full_tuner(bt, cuda):
     S.build(cams, spins)
     ref = [dense(g) for g in S.grids]
     r = S.tune(cams, spins, repeats=1)
-    assert r["candidates"] == 17 and r["best_ms"] > 0 and r["level_ms"] > 0
+    assert r["candidates"] == 23 and r["best_ms"] > 0 and r["level_ms"] > 0
     assert r["flow_ms"] > 0 and r["best_ms"] == min(r["level_ms"], r["flow_ms"])
     assert r["band_p99_rad"] == -1.0
     sh = S.info().shape
@@ -129,6 +129,23 @@ def test_full_tuner(bt, cuda):
     assert tight["band_p99_rad"] <= loose["band_p99_rad"]
     assert M.opts._o.fp64_band == tight["fp64_band"]
     print(f"tuned: fast {r}; mixed band {tight['fp64_band']} p99 {tight['band_p99_rad']:.2e}")
+
+
+def test_lone_grid_tuner(bt, cuda):
+    """bt_grid_tune on a lone grid keeps a configuration that builds the same
+    grid; tuning a member of a set is refused."""
+    cams, spins = cameras(bt, POSES)
+    g = bt.Grid(ML, SL, True, cams[0], opts="fast")
+    ref = dense(g)
+    r = g.tune(repeats=1)
+    assert r["candidates"] == 23 and r["best_ms"] > 0
+    g.build()
+    assert g.info().flags == 0
+    assert_same(dense(g), ref, "tuned lone grid")
+    S = bt.GridSet(ML, SL, True, 2, opts="fast")
+    S.build(cams[:2], spins[:2])
+    with pytest.raises(bt.BtError):
+        S.grids[0].tune(repeats=1)
 
 
 def test_lone_grid_graph_replay(bt, cuda):
