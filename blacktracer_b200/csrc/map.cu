@@ -162,6 +162,9 @@ __global__ void k_pixinterp2(const float2* __restrict__ view, int M, int N, Grid
     if (centerdist <= (bhBorderNew.x - center.x) * (bhBorderNew.x - center.x) +
                           (bhBorderNew.y - center.y) * (bhBorderNew.y - center.y)) {
       thphi[q] = {-1, -1};
+      // the reference returns here without writing gapsave (an earlier
+      // frame's value, or uninitialised memory); 0 keeps frames reproducible
+      gap[q] = 0;
       return;
     }
     const float tStoB = (center.x - stretchRad * sinf(angle) - bhBorderNew.x);
