@@ -507,6 +507,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fast", choices=["fast", "plain", "mixed"],
                     help="integrator form of the headline value")
+    ap.add_argument("--launch", default=None,
+                    help="THREADS,BLOCKS_PER_SM,REFILL for the headline grid's trace launch "
+                         "instead of the autotuner's choice (for reproducible profiles)")
     ap.add_argument("--no-batch", dest="batch", action="store_false",
                     help="skip the 64-pose batched-grid measurement")
     ap.add_argument("--no-c5", dest="c5", action="store_false",
@@ -556,8 +559,14 @@ def main():
                         traced * F_SETUP)
     latency = latency_floor(bt, torch, grid, d, cam, prec_main)
     del d, steps, st_all, integrated
-    # the launch configuration from the project's autotuner (not timed)
-    tuned_main = grid.tune(repeats=3)
+    # the launch configuration from the project's autotuner (not timed), or a
+    # fixed one
+    if args.launch:
+        t_, b_, r_ = (int(x) for x in args.launch.split(","))
+        grid.set_shape(t_, b_, r_)
+        tuned_main = {"shape": (t_, b_, r_), "flow": 0}
+    else:
+        tuned_main = grid.tune(repeats=3)
 
     for _ in range(args.warmup):
         grid.build()
@@ -975,7 +984,8 @@ def main():
                                       "plain": "FP64, reference operation order, no FMA",
                                       "mixed": "FP32 bulk, FP64 guards"}[prec_main],
                        "rays_per_build": traced, "l2": "flushed (256 MB write) before every step",
-                       "launch": {"from": "bt_grid_tune (the project's autotuner), before timing",
+                       "launch": {"from": "--launch" if args.launch else
+                                  "bt_grid_tune (the project's autotuner), before timing",
                                   "threads": tuned_main["shape"][0],
                                   "blocks_per_sm": tuned_main["shape"][1],
                                   "refill": tuned_main["shape"][2],
