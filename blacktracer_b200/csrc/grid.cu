@@ -36,6 +36,8 @@
 //
 // Compiled with --fmad=false (the fix's FP64 Hermite must round like the
 // reference's host build).
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -120,6 +122,8 @@ struct bt_batch {
   // (G*NM slots each), block counters (G*NM bytes) and control block; the
   // set-up and trace queues and the sync words reuse the block lists
   int flow, exec_flow;
+  // set-wide "changed" flag per T-vertex pass of k_tfix_level (16 words)
+  uint32_t* tfix_changed;
   uint32_t* flow_q;
   uint8_t* flow_bw;
   bt::FlowCtl* flow_ctl;
@@ -645,6 +649,84 @@ __global__ void k_tfix_check(const GridDesc* __restrict__ D, int G, int passes) 
   ctr->tfix_flags[1] = 1;
 }
 
+// The T-vertex fix of one level for every grid of the set in one cooperative
+// launch (blockIdx.y = grid): the Jacobi passes of k_tfix_pass separated by
+// grid-wide barriers, stopping after the first pass in which no grid changed
+// (at most `passes`), then k_tfix_commit and k_tfix_check.  The same passes
+// and values as the launches it replaces, which cost a launch each even
+// after convergence (40 launches and ~0.5 ms of a C2 build).  set_changed
+// (16 words, zero on entry and left zero) is the set-wide "changed" flag per
+// pass.
+__global__ void __launch_bounds__(128)
+k_tfix_level(const GridDesc* __restrict__ D, int level, int lo_slot, int hi_slot, int passes,
+             uint32_t* set_changed) {
+  cooperative_groups::grid_group grid = cooperative_groups::this_grid();
+  const GridDesc& d = D[blockIdx.y];
+  GridCounters* ctr = d.ctr;
+  const uint32_t lo = ctr->leaf_off[lo_slot], hi = ctr->leaf_off[hi_slot];
+  const LatticeView& L = d.L;
+  const uint32_t M = L.M;
+  const uint32_t g = pow2u(L.maxlevel - level);
+  const uint64_t n4 = 4ull * (hi - lo);
+  int pass = 1;
+  for (; pass <= passes; pass++) {
+    // a grid that did not change in the previous pass is converged
+    if (pass == 1 || *(volatile uint32_t*)&ctr->tfix_flags[pass - 1] != 0) {
+      const TfixArgs A = tfix_args(d, level, pass, lo_slot, hi_slot);
+      bool changed = false;
+      for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n4;
+           u += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t key = A.leaves[lo + (uint32_t)(u >> 2)];
+        const int e = (int)(u & 3u);
+        const uint32_t i = key / M, j = key % M;
+        if (L.thphi[key].y < 0) continue;  // BT/Grid.h:107
+        const uint32_t k = i + g, l = (j + g) % M;
+        const Edge E = e == 0   ? Edge{i, j, 1, g, rank_of(i, j, 0)}
+                       : e == 1 ? Edge{i, j, 0, g, rank_of(i, j, 1)}
+                       : e == 2 ? Edge{i, l, 1, g, rank_of(i, j, 2)}
+                                : Edge{k, j, 0, g, rank_of(i, j, 3)};
+        changed |= fix_edge(A, E);
+      }
+      if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) {
+        atomicOr(&ctr->tfix_flags[pass], 1u);
+        atomicOr(&set_changed[pass], 1u);
+      }
+    }
+    grid.sync();
+    // the same decision in every block: stop when no grid changed
+    if (pass > 1 && *(volatile uint32_t*)&set_changed[pass] == 0) break;
+  }
+  // commit (the values of the last pass; passes after a grid converged left
+  // both buffers equal on every vertex it writes)
+  const double2* X = d.X[passes & 1];
+  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n4;
+       u += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t key = d.leaves[lo + (uint32_t)(u >> 2)];
+    const int e = (int)(u & 3u);
+    const uint32_t i = key / M, j = key % M;
+    if (L.thphi[key].y < 0) continue;
+    const uint32_t k = i + g, l = (j + g) % M;
+    const uint32_t si = e == 3 ? k : i, sj = e == 2 ? l : j;
+    const int ud = (e == 0 || e == 2) ? 1 : 0;
+    for (uint32_t o = 1; o < g; o++) {
+      const uint32_t ip = si + ud * o, jp = sj + (1 - ud) * o;
+      const size_t id = (size_t)ip * M + jp;
+      if (L.vflag[id] == 1) L.thphi[id] = X[id];
+    }
+  }
+  grid.sync();
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    bool conv = false;
+    for (int t = 2; t <= passes; t++)
+      if (ctr->tfix_flags[t] == 0) conv = true;
+    if (!conv) ctr->err |= 1u;
+    for (int t = 0; t < 16; t++) ctr->tfix_flags[t] = 0;
+    ctr->tfix_flags[1] = 1;
+    if (blockIdx.y == 0)
+      for (int t = 0; t < 16; t++) set_changed[t] = 0;
+  }
+}
+
 // ------------------------------------------------------------ flow
 // Sync words of the first n grids' vertices: traced where the seed level
 // traced them (and the pole copies), else nothing yet.
@@ -938,7 +1020,7 @@ void batch_free(bt_batch* b) {
   }
   void* ptrs[] = {b->thphi, b->steps,   b->vflag,  b->vstat,   b->blevel, b->lists,
                   b->X,     b->ctr,     b->D,      b->qoff,    b->qfetch, b->flow_q,
-                  b->flow_bw, b->flow_ctl};
+                  b->flow_bw, b->flow_ctl, b->tfix_changed};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (b->ctr_host) cudaFreeHost(b->ctr_host);
@@ -983,6 +1065,8 @@ int batch_create(int maxlevel, int angle, int count, bt_batch** out) {
   GALLOC(b->D, G * sizeof(GridDesc));
   GALLOC(b->qoff, (G + 1) * sizeof(uint32_t));
   GALLOC(b->qfetch, sizeof(uint32_t));
+  GALLOC(b->tfix_changed, 16 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemset(b->tfix_changed, 0, 16 * sizeof(uint32_t));
   for (size_t g = 0; g < G; g++) {
     bt_grid* m = &b->grids[g];
     GALLOC(m->rowv, (size_t)N * sizeof(uint32_t));
@@ -1146,11 +1230,31 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
   BT_CUDA_TRY(cudaGetLastError());
   nk++;
   }
-  // T-vertex fix, level by level (coarse to fine)
+  // T-vertex fix, level by level (coarse to fine): one cooperative launch per
+  // level when the set's blocks fit the device at once, else a launch per pass
   const unsigned nb = set_blocks(NM / 16, 128, G);
+  static int coop_per_sm = -1;
+  if (coop_per_sm < 0) {
+    int dev = 0, coop = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
+    coop_per_sm = 0;
+    if (coop) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&coop_per_sm, k_tfix_level, 128, 0);
+  }
+  const unsigned coop_x = std::min<unsigned>(nb, (unsigned)(coop_per_sm * sm_count()) / G);
   for (int level = startlevel; level < b->maxlevel; level++) {
-    const int lo = level - startlevel, hi = level - startlevel + 1;
-    const int passes = b->tfix_passes;
+    int lo = level - startlevel, hi = level - startlevel + 1;
+    int passes = b->tfix_passes;
+    if (coop_x >= 1) {
+      int lv = level;
+      uint32_t* changed = b->tfix_changed;
+      void* args[] = {(void*)&b->D, (void*)&lv, (void*)&lo, (void*)&hi, (void*)&passes,
+                      (void*)&changed};
+      BT_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)k_tfix_level, dim3(coop_x, G),
+                                              dim3(128), args, 0, s));
+      nk++;
+      continue;
+    }
     for (int pass = 1; pass <= passes; pass++)
       k_tfix_pass<<<dim3(nb, G), 128, 0, s>>>(b->D, level, pass, lo, hi);
     k_tfix_commit<<<dim3(nb, G), 128, 0, s>>>(b->D, level, lo, hi, passes);
