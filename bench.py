@@ -568,6 +568,21 @@ def main():
     else:
         tuned_main = grid.tune(repeats=3)
 
+    # the trace launches' device time per build (the roofline's kernel time),
+    # from eager builds with CUDA events around each trace launch
+    for _ in range(args.warmup):
+        grid.build()
+    n_eager = max(3, args.steps // 4)
+    trace_ms, launches = 0.0, 0
+    for _ in range(n_eager):
+        flush.zero_()
+        grid.build()
+        inf = grid.info()  # synchronises
+        trace_ms += float(inf.trace_ms)
+        launches += int(inf.trace_launches)
+    trace_ms_build, launches_build = trace_ms / n_eager, launches / n_eager
+    # the timed builds: each a replay of the build's CUDA graph
+    grid.set_graph(True)
     for _ in range(args.warmup):
         grid.build()
     torch.cuda.synchronize()
@@ -575,7 +590,7 @@ def main():
     clocks.start()
     barrier()
     torch.cuda.synchronize()
-    total_ms, trace_ms, launches, all_launches = 0.0, 0.0, 0, 0
+    total_ms, all_launches = 0.0, 0
     for _ in range(args.steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -585,8 +600,6 @@ def main():
         e1.record(stream)
         inf = grid.info()  # synchronises
         total_ms += e0.elapsed_time(e1)
-        trace_ms += float(inf.trace_ms)
-        launches += int(inf.trace_launches)
         all_launches += int(inf.launches)
     torch.cuda.synchronize()
     barrier()
@@ -602,6 +615,7 @@ def main():
     for prec in [p_ for p_ in ("plain", "fast", "mixed") if p_ != prec_main]:
         gm = bt.Grid(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam, opts=prec)
         tuned_o = gm.tune(repeats=3)
+        gm.set_graph(True)  # timed like the headline
         for _ in range(3):
             gm.build()
         torch.cuda.synchronize()
@@ -647,6 +661,7 @@ def main():
     for bps in (1, 2):
         gf = bt.Grid(WORKLOAD["maxlevel"], WORKLOAD["startlevel"], True, cam, opts=prec_main)
         gf.set_flow(True, blocks_per_sm=bps)
+        gf.set_graph(True)  # timed like the headline
         for _ in range(3):
             gf.build()
         torch.cuda.synchronize()
@@ -718,20 +733,21 @@ def main():
     pk = C.c_double()
     bt._lib.check(bt.lib().bt_probe_fp64_tflops(C.byref(pk), C.c_void_p(stream.cuda_stream)))
     peak = pk.value
-    per_launch_ms = trace_ms / max(1, launches)
-    achieved = flops_build / (trace_ms / args.steps / 1e3) / 1e12
+    per_launch_ms = trace_ms_build / max(1.0, launches_build)
+    achieved = flops_build / (trace_ms_build / 1e3) / 1e12
     roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak if peak else None,
                 "traffic": traffic_from_profiles(prec_main),
                 "kernel": "k_trace_lattice<%sPolicy>" % prec_main.capitalize(),
                 "peak_source": "measured in this run: independent-chain DFMA probe "
                                "(bt_probe_fp64_tflops); MEASURED_PEAKS.json has no FP64 entry",
-                "flops_per_build": flops_build, "trace_ms_per_build": trace_ms / args.steps,
-                "launches_per_build": launches / args.steps,
+                "flops_per_build": flops_build, "trace_ms_per_build": trace_ms_build,
+                "trace_ms_from": f"{n_eager} eager builds with events around the trace launches",
+                "launches_per_build": launches_build,
                 "avg_launch_ms": per_launch_ms,
                 # one grid is bound by its levels' longest rays, not the FP64 pipe
                 "latency_roofline": {**latency,
-                                     "frac": latency["floor_ms"] / (trace_ms / args.steps),
+                                     "frac": latency["floor_ms"] / trace_ms_build,
                                      "note": "sum over levels of the level's longest ray "
                                              "integrated alone, over the trace time per "
                                              "build"}}
@@ -984,6 +1000,7 @@ def main():
                                       "plain": "FP64, reference operation order, no FMA",
                                       "mixed": "FP32 bulk, FP64 guards"}[prec_main],
                        "rays_per_build": traced, "l2": "flushed (256 MB write) before every step",
+                       "graph": "each timed build replays the build's CUDA graph",
                        "launch": {"from": "--launch" if args.launch else
                                   "bt_grid_tune (the project's autotuner), before timing",
                                   "threads": tuned_main["shape"][0],
