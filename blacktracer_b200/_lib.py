@@ -159,6 +159,7 @@ _SIGS = {
     "bt_grid_set_timing": (C.c_int, [_vp, C.c_int]),
     "bt_grid_set_graph": (C.c_int, [_vp, C.c_int]),
     "bt_grid_set_tfix_passes": (C.c_int, [_vp, C.c_int]),
+    "bt_grid_set_tfix_launch": (C.c_int, [_vp, C.c_int]),
     "bt_grid_set_flow": (C.c_int, [_vp, C.c_int]),
     "bt_batch_set_flow": (C.c_int, [_vp, C.c_int]),
     "bt_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),

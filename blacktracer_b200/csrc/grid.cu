@@ -117,6 +117,9 @@ struct bt_batch {
   // Jacobi passes of the T-vertex fix per level (kMaxTfixPasses unless a
   // test lowers it with bt_grid_set_tfix_passes)
   int tfix_passes;
+  // 1: the fix of a level as one cooperative launch when the set fits the
+  // device at once (k_tfix_level); 0: a launch per pass (bt_grid_set_tfix_launch)
+  int tfix_coop, exec_tfix_coop;
   // the refinement levels as one persistent launch (bt_batch_set_flow; flow =
   // its blocks per SM, 0 = off): its check, hot-trace and hot-set-up queues
   // (G*NM slots each), block counters (G*NM bytes) and control block; the
@@ -1044,6 +1047,7 @@ int batch_create(int maxlevel, int angle, int count, bt_batch** out) {
   b->NM = (size_t)N * M;
   b->shape = TraceShape{128, 0, 0};
   b->tfix_passes = bt::kMaxTfixPasses;
+  b->tfix_coop = 1;
   b->grids = new (std::nothrow) bt_grid[count];
   if (!b->grids) {
     delete b;
@@ -1245,7 +1249,7 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
   for (int level = startlevel; level < b->maxlevel; level++) {
     int lo = level - startlevel, hi = level - startlevel + 1;
     int passes = b->tfix_passes;
-    if (coop_x >= 1) {
+    if (b->tfix_coop && coop_x >= 1) {
       int lv = level;
       uint32_t* changed = b->tfix_changed;
       void* args[] = {(void*)&b->D, (void*)&lv, (void*)&lo, (void*)&hi, (void*)&passes,
@@ -1305,6 +1309,7 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int n,
     const bool same = b->exec && b->exec_n == G && b->exec_startlevel == startlevel &&
                       b->exec_precision == precision &&
                       b->exec_tfix_passes == b->tfix_passes &&
+                      b->exec_tfix_coop == b->tfix_coop &&
                       b->exec_flow == b->flow &&
                       b->exec_shape.threads == b->shape.threads &&
                       b->exec_shape.blocks_per_sm == b->shape.blocks_per_sm &&
@@ -1336,6 +1341,7 @@ int batch_build(bt_batch* b, const bt_camera* cams, const double* spins, int n,
       b->exec_startlevel = startlevel;
       b->exec_precision = precision;
       b->exec_tfix_passes = b->tfix_passes;
+      b->exec_tfix_coop = b->tfix_coop;
       b->exec_flow = b->flow;
       b->exec_shape = b->shape;
       b->launches = launches;
@@ -1520,6 +1526,13 @@ int bt_grid_set_tfix_passes(bt_grid* g, int passes) {
   BT_ARG_CHECK(g != nullptr, "NULL grid");
   BT_ARG_CHECK(passes >= 1 && passes <= kMaxTfixPasses, "passes must be in [1, 8]");
   g->set->tfix_passes = passes;
+  return BT_OK;
+}
+
+int bt_grid_set_tfix_launch(bt_grid* g, int cooperative) {
+  clear_error();
+  BT_ARG_CHECK(g != nullptr, "NULL grid");
+  g->set->tfix_coop = cooperative ? 1 : 0;
   return BT_OK;
 }
 

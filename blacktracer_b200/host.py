@@ -279,6 +279,11 @@ class Grid:
         not converged by info() (flag 1, BtError BT_ERR_NUMERIC)."""
         L.check(L.lib().bt_grid_set_tfix_passes(self._h, int(passes)))
 
+    def set_tfix_launch(self, cooperative=True):
+        """Diagnostic: the T-vertex fix of later builds as one cooperative
+        launch per level (default) or a launch per pass."""
+        L.check(L.lib().bt_grid_set_tfix_launch(self._h, 1 if cooperative else 0))
+
     def export(self, out=None, pinned=True):
         """The grid as key-ordered lists (CamToCel, steps, blockLevels).
 

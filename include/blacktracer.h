@@ -213,6 +213,12 @@ int bt_grid_set_flow(bt_grid* g, int on);
  * counterpart in the reference (its fixTvertices is sequential). */
 int bt_grid_set_tfix_passes(bt_grid* g, int passes);
 
+/* Diagnostic: cooperative = 1 (default) runs the T-vertex fix of a level as
+ * one cooperative launch when the set's blocks fit the device at once;
+ * 0 launches each pass, the commit and the check separately (the path sets
+ * too large for one cooperative launch take).  Same grids either way. */
+int bt_grid_set_tfix_launch(bt_grid* g, int cooperative);
+
 /* Synchronises `stream` and reports the build.  Returns BT_ERR_NUMERIC when
  * a bounded loop (T-vertex fixed point) gave up. */
 int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream);

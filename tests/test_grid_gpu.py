@@ -110,16 +110,20 @@ def test_fast_grid_topology_matches_plain(bt, cuda, oracle_mod, ml, sl, camname)
     assert np.percentile(err, 99) <= 1e-6
 
 
-def test_tfix_nonconvergence_is_reported(bt, cuda, oracle_mod):
+@pytest.mark.parametrize("coop", [True, False])
+def test_tfix_nonconvergence_is_reported(bt, cuda, oracle_mod, coop):
     """With one T-vertex pass per level the fix cannot see a pass that
     changed nothing, so the build must report it as not converged: flag 1
     in bt_grid_info.flags and BT_ERR_NUMERIC from bt_grid_query.  The
-    default pass count converges on the same grid."""
+    default pass count converges on the same grid.  Both launch forms of
+    the fix (one cooperative launch per level, a launch per pass)."""
     import ctypes as C
 
     from blacktracer_b200 import _lib as L
     cam, a = oracle_camera(oracle_mod, "c2")
     g = bt.Grid(9, 6, True, bt.Camera.from_array(cam, a), opts="plain")
+    g.set_tfix_launch(coop)
+    g.build()
     assert g.info().flags == 0
     g.set_tfix_passes(1)
     g.build()
@@ -135,3 +139,20 @@ def test_tfix_nonconvergence_is_reported(bt, cuda, oracle_mod):
     assert g.info().flags == 0
     with pytest.raises(L.BtError):
         g.set_tfix_passes(0)
+
+
+@pytest.mark.parametrize("prec", ["plain", "fast"])
+def test_tfix_launch_forms_agree(bt, cuda, oracle_mod, prec):
+    """The T-vertex fix as one cooperative launch per level and as a launch
+    per pass give the same grid, bit for bit (C2 camera, L6 -> L10)."""
+    cam, a = oracle_camera(oracle_mod, "c2")
+    c = bt.Camera.from_array(cam, a)
+    g1 = bt.Grid(10, 6, True, c, opts=prec)
+    g2 = bt.Grid(10, 6, True, c, opts=prec)
+    g2.set_tfix_launch(False)
+    g2.build()
+    d1 = {k: v.cpu().numpy() for k, v in g1.dense().items()}
+    d2 = {k: v.cpu().numpy() for k, v in g2.dense().items()}
+    for k in d1:
+        np.testing.assert_array_equal(d1[k], d2[k], err_msg=k)
+    assert g1.info().flags == 0 and g2.info().flags == 0
