@@ -45,7 +45,7 @@ void map_free(bt_map* m) {
                   m->S.heavy_list, m->S.heavy_order, m->S.heavy_count, m->S.env_wide,
                   m->S.env_wide_count, m->tmp_img, m->S.hv_nn, m->S.hv_nl, m->S.hv_noff,
                   m->S.hv_uoff, m->S.hv_pool, m->S.hv_pend, m->S.hv_partial, m->S.hv_uany,
-                  m->S.hv_ctl};
+                  m->S.hv_ctl, m->S.hv_slab};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (m->side) {

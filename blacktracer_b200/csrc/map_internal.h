@@ -47,6 +47,11 @@ struct MapScratch {
   float* hv_partial;
   uint8_t* hv_uany;
   uint32_t* hv_ctl;
+  // the first pass's emitted nodes, kHvSlab per deferred pixel for the first
+  // hv_slab_pixels pixels, so that the second pass copies instead of
+  // searching again
+  int* hv_slab;
+  uint32_t hv_slab_pixels;
   size_t hv_node_cap, hv_unit_cap;  // 0: the defaults
   int hv_fw;
 };

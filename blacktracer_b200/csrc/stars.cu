@@ -310,6 +310,10 @@ enum { kHcDeferred = 0, kHcGiant = 1, kHcOther = 2, kHcNext = 3, kHcWords = 4 };
 enum { kHvUnits = 0, kHvUnitLeaves = 1, kHvFetch = 2, kHvWords = 4 };
 // Rounds of 32 leaves per unit, at least (more when the unit slots run out).
 constexpr int kUnitRounds = 1;
+// Emitted nodes per deferred pixel the first pass keeps (a 4K frame's
+// deferred pixels emit up to ~570); a pixel that emits more is searched
+// again by the second pass.
+constexpr uint32_t kHvSlab = 1024;
 
 // Pass 1, one thread per deferred pixel: the nodes its search emits and the
 // leaves under them.
@@ -318,7 +322,8 @@ __global__ void k_hv_count(const float2* __restrict__ thphi, const uint8_t* __re
                            const float2* __restrict__ view, int lr,
                            const float* __restrict__ area, const uint32_t* __restrict__ heavy,
                            const uint32_t* __restrict__ hc, uint32_t* __restrict__ nn,
-                           uint32_t* __restrict__ nl) {
+                           uint32_t* __restrict__ nl, int* __restrict__ slab,
+                           uint32_t slab_pixels) {
   const uint32_t n = hc[kHcDeferred];
   const int L = S.treeLevel;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
@@ -327,8 +332,10 @@ __global__ void k_hv_count(const float2* __restrict__ thphi, const uint8_t* __re
     PixelStars P;
     float mn[2], mx[2];
     uint32_t nodes = 0, leaves = 0;
+    int* keep = k < slab_pixels ? slab + (size_t)k * kHvSlab : nullptr;
     if (pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, ij / M, ij % M, P, mn, mx))
       tree_search(S, mn, mx, [&](int node) {
+        if (keep && nodes < kHvSlab) keep[nodes] = node;
         nodes++;
         leaves += 1u << (L - node_level(node));  // disjoint nodes: at most 2^L leaves
         return true;
@@ -440,26 +447,54 @@ __global__ void k_hv_nodes(const float2* __restrict__ thphi, const uint8_t* __re
                            const float2* __restrict__ view, int lr,
                            const float* __restrict__ area, const uint32_t* __restrict__ heavy,
                            const uint32_t* __restrict__ hc, const uint32_t* __restrict__ noff,
+                           const int* __restrict__ slab, uint32_t slab_pixels,
                            int* __restrict__ pool, uint32_t* __restrict__ pend) {
   const uint32_t n = hc[kHcDeferred];
   const int L = S.treeLevel;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += gridDim.x * blockDim.x) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n; k += warps) {
     const uint32_t b0 = noff[k], b1 = noff[k + 1];
     if (b0 == b1) continue;
-    const uint32_t ij = heavy[k];
-    PixelStars P;
-    float mn[2], mx[2];
-    pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, ij / M, ij % M, P, mn, mx);
-    uint32_t e = b0, cum = 0;
-    tree_search(S, mn, mx, [&](int node) {
-      if (e >= b1) return false;  // the same search as pass 1: never taken
-      cum += 1u << (L - node_level(node));
-      pool[e] = node;
-      pend[e] = cum;
-      e++;
-      return true;
-    });
+    if (k < slab_pixels && b1 - b0 <= kHvSlab) {
+      // the first pass kept them: copy, the leaves up to each node as a
+      // warp prefix sum
+      const int* src = slab + (size_t)k * kHvSlab;
+      uint32_t carry = 0;
+      for (uint32_t e0 = b0; e0 < b1; e0 += 32) {
+        const uint32_t e = e0 + lane;
+        const int node = e < b1 ? src[e - b0] : 0;
+        uint32_t c = e < b1 ? 1u << (L - node_level(node)) : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, c, o);
+          if (lane >= (unsigned)o) c += y;
+        }
+        if (e < b1) {
+          pool[e] = node;
+          pend[e] = carry + c;
+        }
+        carry += __shfl_sync(0xffffffffu, c, 31);
+      }
+      continue;
+    }
+    // more nodes than the slab holds (or past its pixels): lane 0 searches
+    // again while the warp waits, so that every lane stays on this pixel
+    if (lane == 0) {
+      const uint32_t ij = heavy[k];
+      PixelStars P;
+      float mn[2], mx[2];
+      pixel_setup(thphi, bh, cam.v, M, step, view, lr, area, ij / M, ij % M, P, mn, mx);
+      uint32_t e = b0, cum = 0;
+      tree_search(S, mn, mx, [&](int node) {
+        if (e >= b1) return false;  // the same search as pass 1: never taken
+        cum += 1u << (L - node_level(node));
+        pool[e] = node;
+        pend[e] = cum;
+        e++;
+        return true;
+      });
+    }
+    __syncwarp();
   }
 }
 
@@ -865,9 +900,10 @@ static int ensure_units(MapScratch& Sc, int fw) {
   if (Sc.hv_ctl && Sc.hv_fw >= fw) return BT_OK;
   cudaFree(Sc.hv_nn); cudaFree(Sc.hv_nl); cudaFree(Sc.hv_noff); cudaFree(Sc.hv_uoff);
   cudaFree(Sc.hv_pool); cudaFree(Sc.hv_pend); cudaFree(Sc.hv_partial); cudaFree(Sc.hv_uany);
-  cudaFree(Sc.hv_ctl);
+  cudaFree(Sc.hv_ctl); cudaFree(Sc.hv_slab);
   Sc.hv_nn = Sc.hv_nl = Sc.hv_noff = Sc.hv_uoff = Sc.hv_pend = Sc.hv_ctl = nullptr;
-  Sc.hv_pool = nullptr;
+  Sc.hv_pool = Sc.hv_slab = nullptr;
+  Sc.hv_slab_pixels = 0;
   Sc.hv_partial = nullptr;
   Sc.hv_uany = nullptr;
   Sc.hv_fw = 0;
@@ -885,6 +921,9 @@ static int ensure_units(MapScratch& Sc, int fw) {
   HV_ALLOC(Sc.hv_partial, Sc.hv_unit_cap * fw * fw * 3 * sizeof(float));
   HV_ALLOC(Sc.hv_uany, Sc.hv_unit_cap);
   HV_ALLOC(Sc.hv_ctl, kHvWords * sizeof(uint32_t));
+  const uint32_t slab_px = (uint32_t)std::min<size_t>(std::max<size_t>(np / 512, 4096), 32768);
+  HV_ALLOC(Sc.hv_slab, (size_t)slab_px * kHvSlab * sizeof(int));
+  if (e == cudaSuccess) Sc.hv_slab_pixels = slab_px;
 #undef HV_ALLOC
   if (e != cudaSuccess) {
     set_error("star unit scratch allocation failed: %s", cudaGetErrorString(e));
@@ -900,9 +939,10 @@ int map_set_star_capacity(MapScratch& Sc, size_t nodes, size_t units) {
   BT_CUDA_TRY(cudaDeviceSynchronize());
   cudaFree(Sc.hv_nn); cudaFree(Sc.hv_nl); cudaFree(Sc.hv_noff); cudaFree(Sc.hv_uoff);
   cudaFree(Sc.hv_pool); cudaFree(Sc.hv_pend); cudaFree(Sc.hv_partial); cudaFree(Sc.hv_uany);
-  cudaFree(Sc.hv_ctl);
+  cudaFree(Sc.hv_ctl); cudaFree(Sc.hv_slab);
   Sc.hv_nn = Sc.hv_nl = Sc.hv_noff = Sc.hv_uoff = Sc.hv_pend = Sc.hv_ctl = nullptr;
-  Sc.hv_pool = nullptr;
+  Sc.hv_pool = Sc.hv_slab = nullptr;
+  Sc.hv_slab_pixels = 0;
   Sc.hv_partial = nullptr;
   Sc.hv_uany = nullptr;
   Sc.hv_fw = 0;
@@ -1416,14 +1456,15 @@ int map_run_stars(MapScratch& Sc, const MapFrame& F, cudaStream_t s) {
   // pool in k_star_heavy
   k_hv_count<<<sm_count() * 2, 128, 0, s>>>(Sc.thphi, Sc.bh, SS, F.cam, M, F.step, F.view,
                                             F.lr, Sc.area, Sc.heavy_list, Sc.heavy_count,
-                                            Sc.hv_nn, Sc.hv_nl);
+                                            Sc.hv_nn, Sc.hv_nl, Sc.hv_slab, Sc.hv_slab_pixels);
   k_hv_scan<<<1, 1024, 0, s>>>(Sc.heavy_list, Sc.heavy_count, Sc.hv_nn, Sc.hv_nl, Sc.hv_noff,
                                Sc.hv_uoff, Sc.heavy_order, Sc.hv_ctl,
                                (uint32_t)std::min<size_t>(Sc.hv_node_cap, 0xffffffffu),
                                (uint32_t)std::min<size_t>(Sc.hv_unit_cap, 0xffffffffu));
   k_hv_nodes<<<sm_count() * 2, 128, 0, s>>>(Sc.thphi, Sc.bh, SS, F.cam, M, F.step, F.view,
                                             F.lr, Sc.area, Sc.heavy_list, Sc.heavy_count,
-                                            Sc.hv_noff, Sc.hv_pool, Sc.hv_pend);
+                                            Sc.hv_noff, Sc.hv_slab, Sc.hv_slab_pixels,
+                                            Sc.hv_pool, Sc.hv_pend);
   if (F.step == 0) launch_units<0>(Sc, F, SS, s);
   else if (F.step == 1) launch_units<1>(Sc, F, SS, s);
   else launch_units<2>(Sc, F, SS, s);
