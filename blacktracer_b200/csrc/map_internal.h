@@ -59,6 +59,10 @@ struct MapScratch {
 struct StarSet;
 const StarSet* stars_internal(const bt_stars* s);
 
+// Device bytes of the star unit path's scratch of an np-pixel frame with a
+// (fw x fw) splat (reserved at the first frame with stars).
+size_t map_star_scratch_bytes(size_t np, int fw);
+
 // One frame's inputs.
 struct MapFrame {
   const float2* grid;   // map grid GN x GM (rows = GN1 for half grids)

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "bt_internal.h"
+#include "map_internal.h"
 
 using bt::clear_error;
 using bt::set_error;
@@ -92,7 +93,8 @@ size_t map_bytes(int W, int H, int step) {
   const size_t np = (size_t)W * H, nc = (size_t)(W + 1) * (H + 1);
   const size_t fw = 2 * (size_t)step + 1;
   return nc * (8 + 4) + np * (1 + 4 + 4 + 12 + 12 + 4 + 1 + 4 + 4 + 4 + 4 + 4) +
-         np * fw * fw * 12 + np * 4 /* frame */ + (1 << 16);
+         np * fw * fw * 12 + np * 4 /* frame */ + bt::map_star_scratch_bytes(np, (int)fw) +
+         (1 << 16);
 }
 
 }  // namespace
@@ -314,6 +316,14 @@ void admit(bt_server* S) {
     key.v[12] = r.a;
     auto it = S->cache.find(key);
     Entry* e = it == S->cache.end() ? nullptr : it->second;
+    if (map_bytes(r.width, r.height, S->cfg.step) > S->cfg.render_bytes) {
+      // its frame can never fit the render budget: fail it instead of
+      // holding it (and every request behind it) forever
+      Request fail = q;
+      S->pending.pop_front();
+      complete(S, fail, BT_ERR_NOMEM, 0);
+      continue;
+    }
     if (!e && !grid_room(S, S->grid_bytes)) return;  // wait for grids to unpin
     Slot* sl = slot_for(S, r.width, r.height);
     if (!sl) return;  // wait for a slot

@@ -895,6 +895,23 @@ constexpr int kHeavyThreads = 512;
 // Buffers of the unit path (lazy): per-pixel counts and offsets, the node
 // pool (max(2^21, N*M) entries) and the unit slots (max(2^18, N*M/8) units
 // of (2s+1)^2 cells), sized for splat width fw.
+// The unit path's scratch for np pixels and a (2s+1)^2 splat: per-pixel
+// counts and offsets, the node pool, the units' cell sums and flags, the
+// first pass's slab.  Small frames get small floors (a frame's deferred
+// pixels that do not fit take the block-per-pixel kernel, and a pixel past
+// the slab is searched twice), so that a server can hold many of them.
+static size_t units_node_cap(size_t np) { return std::max<size_t>((size_t)1 << 18, np); }
+static size_t units_unit_cap(size_t np) { return std::max<size_t>((size_t)1 << 15, np / 8); }
+static uint32_t units_slab_pixels(size_t np) {
+  return (uint32_t)std::min<size_t>(std::max<size_t>(np / 512, 1024), 32768);
+}
+
+size_t map_star_scratch_bytes(size_t np, int fw) {
+  return 4 * (np + 1) * sizeof(uint32_t) + units_node_cap(np) * (sizeof(int) + sizeof(uint32_t)) +
+         units_unit_cap(np) * ((size_t)fw * fw * 3 * sizeof(float) + 1) +
+         (size_t)units_slab_pixels(np) * kHvSlab * sizeof(int) + kHvWords * sizeof(uint32_t);
+}
+
 static int ensure_units(MapScratch& Sc, int fw) {
   const size_t np = (size_t)Sc.M * Sc.N;
   if (Sc.hv_ctl && Sc.hv_fw >= fw) return BT_OK;
@@ -907,8 +924,8 @@ static int ensure_units(MapScratch& Sc, int fw) {
   Sc.hv_partial = nullptr;
   Sc.hv_uany = nullptr;
   Sc.hv_fw = 0;
-  if (!Sc.hv_node_cap) Sc.hv_node_cap = std::max<size_t>((size_t)1 << 21, np);
-  if (!Sc.hv_unit_cap) Sc.hv_unit_cap = std::max<size_t>((size_t)1 << 18, np / 8);
+  if (!Sc.hv_node_cap) Sc.hv_node_cap = units_node_cap(np);
+  if (!Sc.hv_unit_cap) Sc.hv_unit_cap = units_unit_cap(np);
   cudaError_t e = cudaSuccess;
 #define HV_ALLOC(p, bytes) \
   if (e == cudaSuccess) e = cudaMalloc((void**)&(p), (bytes));
@@ -921,7 +938,7 @@ static int ensure_units(MapScratch& Sc, int fw) {
   HV_ALLOC(Sc.hv_partial, Sc.hv_unit_cap * fw * fw * 3 * sizeof(float));
   HV_ALLOC(Sc.hv_uany, Sc.hv_unit_cap);
   HV_ALLOC(Sc.hv_ctl, kHvWords * sizeof(uint32_t));
-  const uint32_t slab_px = (uint32_t)std::min<size_t>(std::max<size_t>(np / 512, 4096), 32768);
+  const uint32_t slab_px = units_slab_pixels(np);
   HV_ALLOC(Sc.hv_slab, (size_t)slab_px * kHvSlab * sizeof(int));
   if (e == cudaSuccess) Sc.hv_slab_pixels = slab_px;
 #undef HV_ALLOC

@@ -91,6 +91,32 @@ def test_eviction_under_small_budget(bt, cuda, scene):
         assert np.array_equal(outs[k], ref[k]), f"request {k} differs under eviction"
 
 
+def test_request_that_cannot_fit_fails(bt, cuda, scene):
+    """A request whose frame needs more than the whole render budget fails
+    with BT_ERR_NOMEM instead of waiting forever (it used to hold every
+    request behind it, and the server's shutdown, which drains the queue);
+    a request that fits is served after it."""
+    import time
+
+    import torch
+
+    from blacktracer_b200 import _lib as L
+    env, sp, cams = scene
+    S = bt.Server(env=env, stars=sp, maxlevel=ML, startlevel=SL, precision="fast",
+                  render_bytes=24 << 20)
+    big, small = (1920, 960), SIZES[0]
+    bufs = [out_buf(torch, *big), out_buf(torch, *small)]
+    cam, a = cams[0]
+    S.submit(0, *big, cam, a, bufs[0])
+    S.submit(1, *small, cam, a, bufs[1])
+    got, t0 = [], time.time()
+    while len(got) < 2 and time.time() - t0 < 60.0:
+        got += S.poll(wait_ms=50)
+    st = {c["id"]: c["status"] for c in got}
+    assert st == {0: L.BT_ERR_NOMEM, 1: L.BT_OK}, st
+    S.close()  # returns: nothing is left waiting
+
+
 def test_backpressure_keeps_every_request(bt, cuda, scene):
     reqs = [(k % 5, SIZES[k % 3]) for k in range(24)]
     outs, comp, st = serve(bt, scene, reqs, max_inflight=2, max_build_batch=3,
