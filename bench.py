@@ -970,8 +970,8 @@ def main():
                                           f"Grid::integration_wrapper on 8 threads "
                                           f"({s8:.2f} s)"}
 
-    # the north star's speed target, like for like: the form that meets
-    # 1e-6 rad against the plain FP64 form on the same work
+    # the speed target of the path (at least 5x the plain FP64 form at <= 1e-6 rad
+    # p99), like for like: the form that meets 1e-6 rad against plain on the same work
     head = traced * args.steps / (total_ms / 1e3)
     plain_v = other["plain"]["value"] if "plain" in other else head
     target = {"form": prec_main, "goal": ">= 5x plain FP64 at <= 1e-6 rad p99",

@@ -47,7 +47,8 @@ void orc_integrate_rays(const orc_camera* cam, double a, const double* theta,
                         int nthreads);
 
 /* Integration with non-default tolerance / end point / cap (BT/Metric.h:276
- * odeint1 called directly, as BASELINE config 1's "rel tol" variant asks). */
+ * odeint1 called directly, as the relative-tolerance variant of the C1
+ * configuration uses). */
 void orc_integrate_rays_opts(const orc_camera* cam, double a,
                              const double* theta, const double* phi, size_t n,
                              double* theta_out, double* phi_out,

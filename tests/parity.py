@@ -3,7 +3,7 @@ import numpy as np
 
 TWO_PI = 2 * np.pi
 
-# Seeded synthetic cameras of the benchmark configurations (BASELINE configs):
+# Seeded synthetic cameras of the benchmark configurations:
 #   C1 static camera at r = 30M, theta = pi/2, a = 0.6      (Camera.h:27)
 #   C2 Keplerian orbit at r = 5M, theta = pi/2, a = 0.999  (Camera.h:40)
 #   C5 Keplerian orbit at r = 8M, theta = 1.2,  a = 0.99
