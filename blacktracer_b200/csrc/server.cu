@@ -461,6 +461,10 @@ int bt_server_create(const bt_server_config* cfg, bt_server** out) {
   S->grid_bytes = (size_t)S->grid_rows * S->grid_cols * sizeof(float2);
   BT_ARG_CHECK(S->grid_bytes <= cfg->grid_cache_bytes, "grid cache smaller than one grid");
   int rc = bt_batch_create(cfg->maxlevel, cfg->angle, cfg->max_build_batch, &S->set);
+  // the T-vertex fix as a launch per pass: builds share the device with
+  // frames on other streams, and a cooperative launch must wait until all of
+  // its blocks fit at once (p99 at 120 requests/s: 56-58 ms against 79-84)
+  if (rc == BT_OK) rc = bt_grid_set_tfix_launch(bt_batch_grid(S->set, 0), 0);
   cudaDeviceGetStreamPriorityRange(&S->prio_least, &S->prio_greatest);
   if (rc == BT_OK) {
     const size_t n = cfg->grid_cache_bytes / S->grid_bytes;
