@@ -192,6 +192,7 @@ _SIGS = {
     "bt_stars_blackbody": (C.c_int, [_vp, C.c_int, _vp, _vp, C.c_int, C.POINTER(C.c_int), _vp]),
     "bt_map_diffract": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "bt_map_set_star_capacity": (C.c_int, [_vp, C.c_size_t, C.c_size_t]),
+    "bt_map_set_star_slab": (C.c_int, [_vp, C.c_int]),
     "bt_blend_create": (C.c_int, [C.POINTER(_vp)]),
     "bt_blend_destroy": (None, [_vp]),
     "bt_blend_prepare": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp]),

@@ -262,6 +262,7 @@ int bt_map_create(int width, int height, bt_map** out) {
   MapScratch& S = m->S;
   S.M = width;
   S.N = height;
+  S.hv_slab_req = -1;  // the default slab for the frame size
   const size_t np = (size_t)width * height;
   const size_t nc = (size_t)(width + 1) * (height + 1);
   cudaError_t e = cudaSuccess;
@@ -355,6 +356,13 @@ int bt_map_set_star_capacity(bt_map* m, size_t nodes, size_t units) {
   BT_ARG_CHECK(units == 0 || units >= 2, "units must be 0 (default) or at least 2");
   BT_ARG_CHECK(nodes <= 0xffffffffu && units <= 0xffffffffu, "capacity above 2^32 - 1");
   return map_set_star_capacity(m->S, nodes, units);
+}
+
+int bt_map_set_star_slab(bt_map* m, int pixels) {
+  clear_error();
+  BT_ARG_CHECK(m != nullptr, "NULL renderer");
+  BT_ARG_CHECK(pixels <= 32768, "slab above 32768 pixels");
+  return map_set_star_slab(m->S, pixels);
 }
 
 int bt_map_diffract(bt_map* m, const bt_stars* stars, const float* light, float* out,

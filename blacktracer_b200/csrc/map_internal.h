@@ -52,6 +52,7 @@ struct MapScratch {
   // searching again
   int* hv_slab;
   uint32_t hv_slab_pixels;
+  int hv_slab_req;  // pixels the slab holds; < 0: the default for the frame size
   size_t hv_node_cap, hv_unit_cap;  // 0: the defaults
   int hv_fw;
 };
@@ -100,6 +101,7 @@ int map_diffract(MapScratch& S, const StarSet& SS, const float* light, float* ou
                  int psf_scale, const float2* view, const float* area, cudaStream_t s);
 // Capacities of the star pass's unit path (stars.cu; 0 = the defaults).
 int map_set_star_capacity(MapScratch& S, size_t nodes, size_t units);
+int map_set_star_slab(MapScratch& S, int pixels);
 // The same for a caller's light buffer with a star set's sprite, unscaled.
 int map_diffract_light(MapScratch& S, const bt_stars* stars, const float* light, float* out,
                        cudaStream_t s);

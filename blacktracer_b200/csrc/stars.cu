@@ -938,8 +938,8 @@ static int ensure_units(MapScratch& Sc, int fw) {
   HV_ALLOC(Sc.hv_partial, Sc.hv_unit_cap * fw * fw * 3 * sizeof(float));
   HV_ALLOC(Sc.hv_uany, Sc.hv_unit_cap);
   HV_ALLOC(Sc.hv_ctl, kHvWords * sizeof(uint32_t));
-  const uint32_t slab_px = units_slab_pixels(np);
-  HV_ALLOC(Sc.hv_slab, (size_t)slab_px * kHvSlab * sizeof(int));
+  const uint32_t slab_px = Sc.hv_slab_req < 0 ? units_slab_pixels(np) : (uint32_t)Sc.hv_slab_req;
+  if (slab_px) HV_ALLOC(Sc.hv_slab, (size_t)slab_px * kHvSlab * sizeof(int));
   if (e == cudaSuccess) Sc.hv_slab_pixels = slab_px;
 #undef HV_ALLOC
   if (e != cudaSuccess) {
@@ -947,6 +947,15 @@ static int ensure_units(MapScratch& Sc, int fw) {
     return BT_ERR_NOMEM;
   }
   Sc.hv_fw = fw;
+  return BT_OK;
+}
+
+// Deferred pixels whose first-pass nodes the slab keeps (< 0: the default);
+// the unit path's buffers are released and reserved again at the next frame.
+int map_set_star_slab(MapScratch& Sc, int pixels) {
+  const size_t nodes = Sc.hv_node_cap, units = Sc.hv_unit_cap;
+  if (int rc = map_set_star_capacity(Sc, nodes, units)) return rc;
+  Sc.hv_slab_req = pixels;
   return BT_OK;
 }
 

@@ -520,13 +520,20 @@ int bt_psf_levels(const uint8_t* psf_rgb, int psf_size, int level, int16_t* offs
 /* Diagnostic: the capacities of the star pass's deferred-pixel units (no
  * counterpart in the reference).  Pixels whose stars exceed the per-pixel
  * budget of the main star pass are cut into units of candidate kd-tree
- * leaves that all SMs share; `nodes` (default max(2^21, W*H)) bounds the
+ * leaves that all SMs share; `nodes` (default max(2^18, W*H)) bounds the
  * kd-tree nodes of those pixels' searches held at once, `units` (default
- * max(2^18, W*H/8), at least 2) the units, whose size grows to fit.
+ * max(2^15, W*H/8), at least 2) the units, whose size grows to fit.
  * Pixels past either bound are rendered one block per pixel instead.  0
  * keeps a default.  Synchronises the device; no frame of m may be in
  * flight. */
 int bt_map_set_star_capacity(bt_map* m, size_t nodes, size_t units);
+
+/* Diagnostic: the number of those pixels (up to 32768) whose first tree
+ * search keeps its emitted nodes (1024 at most each) for the second pass to
+ * copy; the others are searched twice.  Negative: the default
+ * (clamp(W*H/512, 1024, 32768)); 0: none.  Frames are the same either way.
+ * Synchronises the device; no frame of m may be in flight. */
+int bt_map_set_star_slab(bt_map* m, int pixels);
 
 /* addDiffraction (BT/MakeImageKernel.cu:775-800) on a caller's star-light
  * buffer: light and out are DEVICE arrays of width*height*3 floats (the

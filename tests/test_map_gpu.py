@@ -179,7 +179,9 @@ def test_deferred_pixels_fallback_and_unit_size(bt, cuda, oracle_mod):
     of candidate leaves shared by all SMs; pixels past the unit path's node
     pool or unit slots are rendered one block per pixel, and a small slot
     count makes the units larger.  All three give the reference's frame
-    within the map tolerances, and each is reproducible."""
+    within the map tolerances, and each is reproducible.  The second tree
+    pass over those pixels, copying the first pass's nodes or searching
+    again, gives the same frame."""
     import ctypes as C
     case = ("g_c2_l7s4", 128, 64, 128, 60000, 4)
     g, cam, grid, ref_grid, rows, GM, bgr, stars, W, H, tl = setup_case(bt, cuda, oracle_mod, case)
@@ -201,3 +203,14 @@ def test_deferred_pixels_fallback_and_unit_size(bt, cuda, oracle_mod):
         assert np.array_equal(a, b), f"{label}: frames must be reproducible"
     with pytest.raises(bt.BtError):
         L.check(L.lib().bt_map_set_star_capacity(R._h, 0, 1))
+    # the deferred pixels' second tree pass: nodes copied from the first
+    # pass's slab (default), searched again (no slab), or both in one frame
+    # (a slab of one pixel): the same frame, bit for bit
+    frames = []
+    for pixels in (-1, 0, 1):
+        R = bt.Renderer(W, H)
+        L.check(L.lib().bt_map_set_star_slab(R._h, pixels))
+        frames.append(R.render(grid, viewer, cam, stars=sp, lr=True).cpu().numpy())
+    assert np.array_equal(frames[0], frames[1]) and np.array_equal(frames[0], frames[2])
+    with pytest.raises(bt.BtError):
+        L.check(L.lib().bt_map_set_star_slab(R._h, 40000))
