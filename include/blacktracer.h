@@ -748,7 +748,9 @@ typedef struct bt_server_stats {
 /* The server uses the device current at creation; env and stars must
  * outlive it. */
 int bt_server_create(const bt_server_config* cfg, bt_server** out);
-/* Thread-safe, non-blocking.  r->out must stay valid until completion. */
+/* Thread-safe, non-blocking.  r->out must stay valid until completion.  A
+ * request whose frame needs more device memory than the whole render budget
+ * (render_bytes) completes with status BT_ERR_NOMEM instead of waiting. */
 int bt_server_submit(bt_server* s, const bt_request* r);
 /* Up to cap completions; waits up to wait_ms for the first one. */
 int bt_server_poll(bt_server* s, bt_completion* out, int cap, int* n, int wait_ms);
