@@ -160,6 +160,7 @@ _SIGS = {
     "bt_grid_set_graph": (C.c_int, [_vp, C.c_int]),
     "bt_grid_set_tfix_passes": (C.c_int, [_vp, C.c_int]),
     "bt_grid_set_tfix_launch": (C.c_int, [_vp, C.c_int]),
+    "bt_grid_set_flow_drop": (C.c_int, [_vp]),
     "bt_grid_set_flow": (C.c_int, [_vp, C.c_int]),
     "bt_batch_set_flow": (C.c_int, [_vp, C.c_int]),
     "bt_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(_vp)]),

@@ -125,6 +125,7 @@ struct bt_batch {
   // (G*NM slots each), block counters (G*NM bytes) and control block; the
   // set-up and trace queues and the sync words reuse the block lists
   int flow, exec_flow;
+  int flow_drop;  // diagnostic: the next flow build loses one ray (bt_grid_set_flow_drop)
   // set-wide "changed" flag per T-vertex pass of k_tfix_level (16 words)
   uint32_t* tfix_changed;
   uint32_t* flow_q;
@@ -1205,6 +1206,8 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
     A.bwait = b->flow_bw;
     A.ctl = b->flow_ctl;
     A.blocks_per_sm = b->flow;
+    A.drop = b->flow_drop;
+    b->flow_drop = 0;
     const bool t = timing && b->timing && b->n_ev + 2 <= 2 * 16;
     if (t) BT_CUDA_TRY(cudaEventRecord(b->ev[b->n_ev], s));
     const int rc = precision == BT_PRECISION_MIXED ? launch_flow_mixed(A, s)
@@ -1526,6 +1529,15 @@ int bt_grid_set_tfix_passes(bt_grid* g, int passes) {
   BT_ARG_CHECK(g != nullptr, "NULL grid");
   BT_ARG_CHECK(passes >= 1 && passes <= kMaxTfixPasses, "passes must be in [1, 8]");
   g->set->tfix_passes = passes;
+  return BT_OK;
+}
+
+int bt_grid_set_flow_drop(bt_grid* g) {
+  clear_error();
+  BT_ARG_CHECK(g != nullptr, "NULL grid");
+  BT_ARG_CHECK(g->set->flow, "the one-launch build is off (bt_grid_set_flow)");
+  BT_ARG_CHECK(!g->set->graph, "graph replay is on: the drop applies to one eager build");
+  g->set->flow_drop = 1;
   return BT_OK;
 }
 

@@ -90,6 +90,7 @@ struct FlowCtl {
   FlowCounter live;       // items pushed and not finished
   FlowCounter progress;   // tracer warps' heartbeats
   uint32_t err;
+  uint32_t dropped;       // diagnostic: the ray already lost (FlowArgs::drop)
 };
 
 struct FlowArgs {
@@ -103,6 +104,10 @@ struct FlowArgs {
   uint8_t* bwait;   // G * NM: untraced corners of the block at this origin
   FlowCtl* ctl;
   int blocks_per_sm;  // of the launch (capped by the occupancy limit)
+  // Diagnostic (bt_grid_set_flow_drop): the first ray to be traced is
+  // counted as live but never handed to a tracer, so that nothing can
+  // finish the flow and its bounded wait runs out (error flag 8).
+  int drop;
 };
 
 __device__ __forceinline__ unsigned long long flow_now() {
@@ -482,8 +487,13 @@ __device__ __forceinline__ void flow_worker(const FlowArgs& A, FlowIdle& w) {
     const uint32_t sk = si & kFlowKeyMask;
     const bool trace = si != kQEmpty && flow_setup<Policy>(A, sk);
     const bool hot = (si >> kFlowKeyBits) & 1u;
-    flow_push_warp(A, kFqHot, &sk, trace && hot ? 1u : 0u);
-    flow_push_warp(A, kFqTrace, &sk, trace && !hot ? 1u : 0u);
+    bool lose = false;
+    if (A.drop && trace && atomicCAS(&A.ctl->dropped, 0u, 1u) == 0u) {
+      atomicAdd(&A.ctl->live.v, 1ull);  // live for good: never pushed, never finished
+      lose = true;
+    }
+    flow_push_warp(A, kFqHot, &sk, trace && hot && !lose ? 1u : 0u);
+    flow_push_warp(A, kFqTrace, &sk, trace && !hot && !lose ? 1u : 0u);
     const unsigned done = __popc(__ballot_sync(0xffffffffu, ci != kQEmpty)) +
                           __popc(__ballot_sync(0xffffffffu, si != kQEmpty));
     flow_finished(A, done);

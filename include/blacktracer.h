@@ -219,6 +219,13 @@ int bt_grid_set_tfix_passes(bt_grid* g, int passes);
  * too large for one cooperative launch take).  Same grids either way. */
 int bt_grid_set_tfix_launch(bt_grid* g, int cooperative);
 
+/* Diagnostic for the one-launch build's failure path: the next build (flow
+ * on, eager) loses one ray -- counted as in flight, never traced -- so that
+ * nothing can end the flow; its warps give up after about two seconds
+ * without progress and the build reports flag 8 (BT_ERR_NUMERIC, "the flow
+ * gave up waiting").  The grid is then incomplete; later builds are normal. */
+int bt_grid_set_flow_drop(bt_grid* g);
+
 /* Synchronises `stream` and reports the build.  Returns BT_ERR_NUMERIC when
  * a bounded loop (T-vertex fixed point) gave up. */
 int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream);

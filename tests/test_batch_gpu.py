@@ -196,3 +196,35 @@ def test_flow_builds_equal_level_builds(bt, cuda, prec):
         b.build()
         assert b.info().flags == 0 and b.traced == a.traced
         assert_same(dense(b), dense(a), f"{prec} flow C2 L10, {bps} blocks per SM")
+
+
+def test_flow_gives_up_when_a_ray_is_lost(bt, cuda):
+    """The one-launch build's waits are bounded: with one ray lost on purpose
+    (counted as in flight, never traced; bt_grid_set_flow_drop) nothing can
+    end the flow, its warps give up after about two seconds without
+    progress, and the build reports flag 8 (BT_ERR_NUMERIC, "the flow gave up
+    waiting").  The context stays usable: the next build, with nothing lost,
+    gives the level build's grid."""
+    import time
+
+    from blacktracer_b200 import _lib as L
+    cam = bt.Camera(math.pi / 2, 0.0, 5.0, 0.0, 0.0, 1.0, a=0.999)
+    ref = bt.Grid(9, 6, True, cam, opts="fast")
+    g = bt.Grid(9, 6, True, cam, opts="fast")
+    g.set_flow(True)
+    L.check(L.lib().bt_grid_set_flow_drop(g._h))
+    import ctypes as C
+    t0 = time.time()
+    g.build()
+    inf = L.bt_grid_info()
+    rc = L.lib().bt_grid_query(g._h, C.byref(inf), None)
+    waited = time.time() - t0
+    assert rc == L.BT_ERR_NUMERIC and inf.flags & 8, (rc, inf.flags)
+    assert b"flow gave up" in L.lib().bt_last_error()
+    assert 1.5 < waited < 60, waited
+    g.build()
+    assert g.info().flags == 0
+    assert_same(dense(g), dense(ref), "flow after a lost ray")
+    g.set_graph(True)
+    with pytest.raises(L.BtError):
+        L.check(L.lib().bt_grid_set_flow_drop(g._h))
