@@ -232,6 +232,48 @@ class Grid {
   const bt_grid_info& info() const { return info_; }
   int64_t traced() const { return info_.traced; }
 
+  // Build this grid again for another camera at the same MAXLEVEL, start level
+  // and view, reusing its device buffers and its tuned trace configuration.
+  // The reference makes a new Grid per camera (BT/BlackTracer.cpp:252); this
+  // gives the same grid without the allocations.  Host copies (CamToCel,
+  // steps, blockLevels) are taken again on their next use.
+  void rebuild(const Camera* camera, const BlackHole* bh = nullptr,
+               const bt_integ_opts* opts = nullptr) {
+    if (!g_) throw Error(BT_ERR_STATE, "a grid loaded from a file cannot be built");
+    bt_camera c = camera->raw();
+    const double a = bh ? bh->a : camera->a;
+    check(bt_grid_build(g_, &c, a, STARTLVL, opts, stream_));
+    check(bt_grid_query(g_, &info_, stream_));
+    exported_ = false;
+    cam_to_cel_.clear();
+    block_levels_.clear();
+    steps_.clear();
+  }
+
+  // The autotuner on this grid's last build (bt_grid_tune): later builds and
+  // rebuild() use the fastest trace shape, refill size and build form found.
+  // For the MIXED form it also picks fp64_band for p99_target_rad; pass the
+  // result's fp64_band in the options of later MIXED builds.
+  bt_tune_result tune(const bt_integ_opts* opts = nullptr, double p99_target_rad = 1e-6,
+                      int repeats = 2) {
+    if (!g_) throw Error(BT_ERR_STATE, "a grid loaded from a file cannot be tuned");
+    bt_tune_result r;
+    std::memset(&r, 0, sizeof(r));
+    check(bt_grid_tune(g_, opts, p99_target_rad, repeats, &r, stream_));
+    return r;
+  }
+
+  // CUDA-graph replay of the level builds (bt_grid_set_graph) and the
+  // one-launch build at blocksPerSm blocks per SM, 0 for off (bt_grid_set_flow).
+  void setGraph(bool on) {
+    if (!g_) throw Error(BT_ERR_STATE, "a grid loaded from a file is not built");
+    check(bt_grid_set_graph(g_, on ? 1 : 0));
+  }
+  void setFlow(int blocksPerSm) {
+    if (!g_) throw Error(BT_ERR_STATE, "a grid loaded from a file is not built");
+    check(bt_grid_set_flow(g_, blocksPerSm));
+  }
+
   // BT/Grid.h:575, 577, 588 -- host copies, keyed i<<32|j like the reference.
   const std::unordered_map<uint64_t, Point2d>& CamToCel() { exportHost(); return cam_to_cel_; }
   const std::vector<int>& steps() { exportHost(); return steps_; }

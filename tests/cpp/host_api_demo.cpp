@@ -5,6 +5,7 @@
 //   host_api_demo grid             (GPU)
 //   host_api_demo frame            (GPU)
 //   host_api_demo files <dir>      (GPU: cache files, perspective view, G = 2)
+//   host_api_demo rebuild          (GPU: tune, graph replay, rebuild vs new Grid)
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -117,6 +118,31 @@ int main(int argc, char** argv) {
     d2.render(c0b.data(), 0.f, 0.f, 0.f);
     printf("%d %d %d %d %d\n", same ? 1 : 0, loaded[0].MAXLEVEL, sp2.starSize,
            c0 == c0b ? 1 : 0, c0 != c5 ? 1 : 0);
+    return 0;
+  }
+  if (!std::strcmp(mode, "rebuild")) {
+    // One grid tuned, switched to graph replay and built again for a second
+    // camera (twice: capture, then replay) must equal a new Grid of that camera.
+    Grid g(8, 5, true, &cam, &black);
+    const bt_tune_result t = g.tune(nullptr, 1e-6, 1);
+    g.setGraph(true);
+    Camera cam2(M_PI / 2, 0.3, 7.0, 0.0, 0.0, 1.0);
+    g.rebuild(&cam2, &black);
+    g.rebuild(&cam2, &black);
+    Grid fresh(8, 5, true, &cam2, &black);
+    const auto& a = g.CamToCel();
+    const auto& b = fresh.CamToCel();
+    bool same = a.size() == b.size();
+    for (const auto& e : a) {
+      auto it = b.find(e.first);
+      if (it == b.end() || std::memcmp(&it->second, &e.second, sizeof(Point2d))) {
+        same = false;
+        break;
+      }
+    }
+    same = same && g.steps() == fresh.steps() && g.blockLevels() == fresh.blockLevels();
+    printf("%d %d %lld %lld\n", same ? 1 : 0, t.candidates, (long long)g.traced(),
+           (long long)fresh.traced());
     return 0;
   }
   return 2;

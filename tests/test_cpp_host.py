@@ -70,3 +70,10 @@ def test_cpp_files_view_and_blend(demo, cuda, tmp_path):
     assert same == "1", "frame from the saved files differs"
     assert int(level) == 7 and int(nstars) == 1500
     assert repeat == "1" and blended == "1"
+
+
+@pytest.mark.gpu
+def test_cpp_tune_graph_and_rebuild(demo, cuda):
+    same, candidates, traced, traced_fresh = run(demo, "rebuild")[0].split()
+    assert same == "1", "a tuned, graph-replayed rebuild differs from a new Grid"
+    assert int(candidates) > 1 and traced == traced_fresh
