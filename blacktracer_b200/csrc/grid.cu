@@ -122,9 +122,12 @@ struct bt_batch {
   int tfix_coop, exec_tfix_coop;
   // the refinement levels as one persistent launch (bt_batch_set_flow; flow =
   // its blocks per SM, 0 = off): its check, hot-trace and hot-set-up queues
-  // (G*NM slots each), block counters (G*NM bytes) and control block; the
-  // set-up and trace queues and the sync words reuse the block lists
+  // (G*NM slots each), block bytes (G*NM per level below the max that blocks
+  // wait on, flow_bw_levels of them) and control block; the set-up and trace
+  // queues and the sync words reuse the block lists
   int flow, exec_flow;
+  int flow_bw_levels;
+  int flow_early;  // refine blocks early in the flow (on unless a test turns it off)
   int flow_drop;  // diagnostic: the next flow build loses one ray (bt_grid_set_flow_drop)
   // set-wide "changed" flag per T-vertex pass of k_tfix_level (16 words)
   uint32_t* tfix_changed;
@@ -1049,6 +1052,7 @@ int batch_create(int maxlevel, int angle, int count, bt_batch** out) {
   b->shape = TraceShape{128, 0, 0};
   b->tfix_passes = bt::kMaxTfixPasses;
   b->tfix_coop = 1;
+  b->flow_early = 1;
   b->grids = new (std::nothrow) bt_grid[count];
   if (!b->grids) {
     delete b;
@@ -1181,8 +1185,12 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
     uint32_t* vsync = b->lists + 1 * gnm_full;
     uint32_t* qsetup = b->lists + 0 * gnm_full;  // the check lists, once read
     uint32_t* qtrace = b->lists + 2 * gnm_full;  // the trace lists, free now
+    // early refinement when the waiter bits of every level fit a sync word
+    const int span = b->maxlevel - startlevel;
+    const bool early = b->flow_early && span <= kFlowEarlySpan && span - 1 <= b->flow_bw_levels;
+    const size_t bw_levels = early ? (size_t)(span - 1) : 1;
     BT_CUDA_TRY(cudaMemsetAsync(b->flow_ctl, 0, sizeof(FlowCtl), s));
-    BT_CUDA_TRY(cudaMemsetAsync(b->flow_bw, 0, GNM, s));
+    if (bw_levels) BT_CUDA_TRY(cudaMemsetAsync(b->flow_bw, 0, bw_levels * GNM, s));
     BT_CUDA_TRY(cudaMemsetAsync(b->flow_q, 0xff, 3 * GNM * sizeof(uint32_t), s));
     k_flow_sync<<<sm_count() * 8, 256, 0, s>>>(b->D, GNM, (uint32_t)NM, vsync);
     k_flow_checks<<<dim3(set_blocks(NM / 4, 256, G), G), 256, 0, s>>>(b->D, (uint32_t)NM,
@@ -1204,6 +1212,8 @@ int batch_enqueue(bt_batch* b, int n, int startlevel, int precision, cudaStream_
     for (int k = 0; k < kFq; k++) A.cap[k] = GNM;
     A.vsync = vsync;
     A.bwait = b->flow_bw;
+    A.bw_stride = early ? GNM : 0;
+    A.early = early ? 1 : 0;
     A.ctl = b->flow_ctl;
     A.blocks_per_sm = b->flow;
     A.drop = b->flow_drop;
@@ -1376,8 +1386,11 @@ float batch_trace_ms(const bt_batch* b) {
 int batch_set_flow(bt_batch* b, int on) {
   if (on && !b->flow_q) {
     const size_t GNM = (size_t)b->G * b->NM;
+    // block bytes for every level below the max that a build can have
+    // blocks wait on (start level 1 or more), at most the early-refinement span
+    const int lv = std::max(1, std::min(b->maxlevel - 2, kFlowBwLevels));
     cudaError_t e = cudaMalloc((void**)&b->flow_q, 3 * GNM * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&b->flow_bw, GNM);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->flow_bw, (size_t)lv * GNM);
     if (e == cudaSuccess) e = cudaMalloc((void**)&b->flow_ctl, sizeof(FlowCtl));
     if (e != cudaSuccess) {
       cudaFree(b->flow_q);
@@ -1389,6 +1402,7 @@ int batch_set_flow(bt_batch* b, int on) {
       set_error("flow buffers (%zu vertices) failed: %s", GNM, cudaGetErrorString(e));
       return BT_ERR_NOMEM;
     }
+    b->flow_bw_levels = lv;
   }
   b->flow = on > 0 ? on : 0;
   return BT_OK;
@@ -1482,7 +1496,8 @@ int bt_grid_query(bt_grid* g, bt_grid_info* info, void* stream) {
   info->trace_launches = g->set->n_ev / 2;
   if (info->flags) {
     set_error("grid build flags 0x%x (1: T-vertex fix did not converge, "
-              "2: fix stack overflow, 4: work list overflow, 8: the flow gave up waiting)",
+              "2: fix stack overflow, 4: work list overflow, 8: the flow gave up waiting, "
+              "16: the flow refined a block early that the level form would not)",
               info->flags);
     return BT_ERR_NUMERIC;
   }

@@ -22,16 +22,31 @@
 // Each block of the launch has a worker warp (checks first, then set-ups,
 // one per lane), a service warp that feeds the block's tracer lanes and
 // collects their rays, and tracer warps.  A finished vertex sets the traced
-// bit of its sync word and, for each child block that registered on it (one
-// waiter bit per corner position), decrements the block's count of untraced
-// corners; the decrement that reaches zero queues the block.  A child is
-// created with a count of five (four corners and a guard): it registers on
-// each corner, counts down the corners already traced, then drops the guard.
-// The traced bit and the waiter bits share one word, so exactly one of the
-// tracer and the registering block sees the other.  A vertex's waiters are
-// blocks of its native level (the level at which its lattice position first
-// appears): it is created by a refinement into that level, and blocks of
-// later levels are only created after it is traced.
+// bit of its sync word and, for each block that registered on it (a waiter
+// bit per corner position and level), sets that corner's bit in the block's
+// byte; the bit that completes the four queues the block's check.  A block
+// registers on each of its corners when it is created and sets the bits of
+// the corners already traced itself.  The traced bit and the waiter bits
+// share one word, so exactly one of the tracer and the registering block
+// sees the other.
+//
+// Early refinement: refineCheck refines a block when the larger of its two
+// diagonals' squared separations is above the threshold, so a traced
+// diagonal above it decides the block without its other two corners.  The
+// bit that completes a diagonal reads its two corners and, when they are far
+// enough apart, queues the block as refined at once: its children are
+// created, and their new rays start, while the block's slow corner is still
+// being integrated (a chain of slow rays no longer runs level after level).
+// The one case where the larger-of-two rule can differ from the diagonal
+// alone is a NaN separation on the (0, 3) diagonal when the (1, 2) diagonal
+// decided: std::max then keeps the NaN and the block is a leaf.  A block
+// refined early on (1, 2) is therefore checked again by whoever completes its
+// corners, and a disagreement is reported (error flag 16: rebuild in the
+// level form).  Blocks of several levels then wait on one vertex (a child can
+// exist before its parent's corners are traced), so the waiter bits carry
+// the level (four per level above the vertex's native one, 28 bits in all:
+// early refinement needs maxlevel - startlevel <= 7) and every level below
+// the max has its own array of block bytes.
 //
 // The manager's queues (checks, set-ups) hand out tickets: a lane reserves
 // the next slot with a fetch-and-add (one per warp) and polls that slot, its
@@ -46,7 +61,8 @@
 // grid's build.
 //
 // Decisions depend only on corner values, so the grids are the ones the
-// level-by-level build gives, bit for bit; only the order of work differs.
+// level-by-level build gives, bit for bit (flag 16 aside); only the order of
+// work differs.
 // The launch ends when no queued or running item is left (a count of items
 // pushed and not finished).  Every wait is bounded: a warp with nothing to do
 // backs off and looks again, and gives up (error flag 8) after two seconds in
@@ -64,10 +80,20 @@ constexpr uint32_t kVTraced = 0x80000000u;  // sync word: the vertex is final
 constexpr uint32_t kQEmpty = 0xffffffffu;   // queue slot not written yet
 enum { kFqCheck = 0, kFqSetup = 1, kFqTrace = 2, kFqHot = 3, kFqSetupHot = 4, kFq = 5 };
 // Items: grid g's vertex or block origin key as g * NM + key (< 2^28); a
-// check item carries (level - startlevel) in its top four bits, a set-up
+// check item carries (level - startlevel) in its top four bits (with early
+// refinement: bits 28-30, and bit 31 for a block refined early), a set-up
 // item the vertex's hot bit (kHotSteps) in bit 28.
 constexpr uint32_t kFlowKeyBits = 28;
 constexpr uint32_t kFlowKeyMask = (1u << kFlowKeyBits) - 1u;
+constexpr uint32_t kFlowEarly = 0x80000000u;
+// Early refinement: the most levels below the max that blocks wait on.
+constexpr int kFlowEarlySpan = 7;
+constexpr int kFlowBwLevels = kFlowEarlySpan - 1;
+// A block's byte: its corners traced (bit p = corner p: 0 origin, 1 right,
+// 2 below, 3 diagonal), checked or refined early, refined on (1, 2).
+constexpr uint32_t kBCorners = 0xfu;
+constexpr uint32_t kBDecided = 0x10u;
+constexpr uint32_t kBByDiag2 = 0x20u;
 // A block: one service warp, kFlowWorkers worker warps, kFlowSlots tracer warps.
 constexpr int kFlowWorkers = 1;
 constexpr int kFlowSlots = 6;  // tracer warps = tracer lanes per service lane
@@ -101,7 +127,11 @@ struct FlowArgs {
   uint32_t* q[kFq];
   unsigned long long cap[kFq];  // slots of each queue
   uint32_t* vsync;  // G * NM: traced bit + waiter bits
-  uint8_t* bwait;   // G * NM: untraced corners of the block at this origin
+  // block bytes: of level l at (l - startlevel - 1) * bw_stride + g * NM +
+  // origin; bw_stride 0 (early refinement off): one array for all levels
+  uint8_t* bwait;
+  size_t bw_stride;
+  int early;  // refine a block as soon as one diagonal decides it
   FlowCtl* ctl;
   int blocks_per_sm;  // of the launch (capped by the occupancy limit)
   // Diagnostic (bt_grid_set_flow_drop): the first ray to be traced is
@@ -288,56 +318,130 @@ __device__ __forceinline__ int native_level(const FlowArgs& A, uint32_t i, uint3
   return A.maxlevel - min(min(ti, tj), span);
 }
 
-// One of a block's untraced-corner count comes off; the one that empties it
-// queues the block's check (levels below the maximum only register).
+// Squared separation of two lattice values, rounded as refineCheck's
+// expression is without contraction (the level form's k_refine is compiled
+// with --fmad=false; the flow is also built into units that contract).
+__device__ __forceinline__ double flow_sep(const double2 u, const double2 v) {
+  const double dx = u.x - v.x, dy = u.y - v.y;
+  return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+}
+
+// refineCheck's threshold (BT/Grid.h:437-440).
+__device__ __forceinline__ bool flow_refines(double mx, int level) {
+  return (level < 6 && mx > 1E-10) || (mx > 0.015);
+}
+
+// refineCheck (BT/Grid.h:410-445) of the block at (i, j) with side gap: the
+// larger of its diagonals' squared separations against the threshold.
+__device__ __forceinline__ bool flow_rule(const LatticeView& L, uint32_t M, uint32_t i,
+                                          uint32_t j, uint32_t gap, int level) {
+  const uint32_t k = i + gap, l = (j + gap) % M;
+  const double diag = flow_sep(L.thphi[(size_t)i * M + j], L.thphi[(size_t)k * M + l]);
+  const double diag2 = flow_sep(L.thphi[(size_t)k * M + j], L.thphi[(size_t)i * M + l]);
+  const double mx = diag < diag2 ? diag2 : diag;  // std::max
+  return flow_refines(mx, level);
+}
+
+// The byte of the block of `level` (above the start level) at gk = g * NM +
+// origin: its aligned 32-bit word, and the byte's shift in it.
+__device__ __forceinline__ uint32_t* block_word(const FlowArgs& A, uint32_t gk, int level,
+                                                uint32_t& sh) {
+  const size_t lv = A.bw_stride ? (size_t)(level - A.startlevel - 1) : 0;
+  uint8_t* byte = A.bwait + lv * A.bw_stride + gk;
+  sh = (uint32_t)((uintptr_t)byte & 3) * 8;
+  return (uint32_t*)((uintptr_t)byte & ~(uintptr_t)3);
+}
+
+// Corner p of the block of `level` at origin (grid g) is traced.  The bit
+// that completes the four queues the block's check; with early refinement,
+// the bit that completes a diagonal whose separation alone refines the block
+// queues it as refined.  Exactly one of them decides (kBDecided).
 __device__ __forceinline__ void block_corner_done(const FlowArgs& A, uint32_t g,
-                                                  uint32_t origin, int level) {
+                                                  uint32_t origin, int level, int p) {
   const uint32_t gk = g * A.NM + origin;
-  uint32_t* word = (uint32_t*)((uintptr_t)(A.bwait + gk) & ~(uintptr_t)3);
-  const uint32_t sh = ((uintptr_t)(A.bwait + gk) & 3) * 8;
-  const uint32_t old = atomicSub(word, 1u << sh);
-  if (((old >> sh) & 0xffu) == 1u)
-    flow_push(A, kFqCheck, ((uint32_t)(level - A.startlevel) << kFlowKeyBits) | gk);
+  uint32_t sh;
+  uint32_t* word = block_word(A, gk, level, sh);
+  const uint32_t old = (atomicOr(word, (1u << p) << sh) >> sh) & 0xffu;
+  const uint32_t now = old | (1u << p);
+  const uint32_t tag = (uint32_t)(level - A.startlevel) << kFlowKeyBits;
+  const uint32_t M = A.M, i = origin / M, j = origin % M;
+  const uint32_t gap = 1u << (A.maxlevel - level);
+  if ((now & kBCorners) == kBCorners) {
+    uint32_t prev = old;
+    if (!(old & kBDecided)) {
+      prev = (atomicOr(word, kBDecided << sh) >> sh) & 0xffu;
+      if (!(prev & kBDecided)) {
+        flow_push(A, kFqCheck, tag | gk);
+        return;
+      }
+    }
+    // refined early on the (1, 2) diagonal: the full rule must agree (it
+    // does unless the (0, 3) separation is NaN)
+    if (prev & kBByDiag2) {
+      __threadfence();  // the corners' values after their traced bits
+      if (!flow_rule(A.D[g].L, M, i, j, gap, level)) atomicOr(&A.ctl->err, 16u);
+    }
+    return;
+  }
+  if (!A.early || (old & kBDecided)) return;
+  const bool d03 = (now & 9u) == 9u && (old & 9u) != 9u;
+  const bool d12 = (now & 6u) == 6u && (old & 6u) != 6u;
+  if (!d03 && !d12) return;
+  __threadfence();  // the corners' values after their traced bits
+  const LatticeView& L = A.D[g].L;
+  const uint32_t k = i + gap, l = (j + gap) % M;
+  const double sep = d03 ? flow_sep(L.thphi[(size_t)i * M + j], L.thphi[(size_t)k * M + l])
+                         : flow_sep(L.thphi[(size_t)k * M + j], L.thphi[(size_t)i * M + l]);
+  if (!flow_refines(sep, level)) return;
+  const uint32_t mark = kBDecided | (d03 ? 0u : kBByDiag2);
+  const uint32_t prev = (atomicOr(word, mark << sh) >> sh) & 0xffu;
+  if (prev & kBDecided) return;  // checked or refined meanwhile
+  flow_push(A, kFqCheck, kFlowEarly | tag | gk);
 }
 
 // Vertex key of grid g is final (its lattice values written): set its traced
-// bit and release the blocks that waited on it.
+// bit and release the blocks that waited on it (waiter bit 4 e + p: corner p
+// of a block e levels above the vertex's native one).
 __device__ __forceinline__ void vertex_done(const FlowArgs& A, uint32_t g, uint32_t key) {
   __threadfence();  // the vertex's values before its traced bit
   const uint32_t old = atomicOr(&A.vsync[g * A.NM + key], kVTraced);
-  const uint32_t waiters = old & 0xfu;
+  uint32_t waiters = old & ~kVTraced;
   if (!waiters) return;
   const uint32_t i = key / A.M, j = key % A.M;
-  const int level = native_level(A, i, j);
-  const uint32_t gap = 1u << (A.maxlevel - level);
-  for (int p = 0; p < 4; p++) {
-    if (!(waiters & (1u << p))) continue;
+  const int native = native_level(A, i, j);
+  while (waiters) {
+    const int b = __ffs((int)waiters) - 1;
+    waiters &= waiters - 1u;
+    const int level = native + (b >> 2), p = b & 3;
+    const uint32_t gap = 1u << (A.maxlevel - level);
     const uint32_t oi = (p & 2) ? i - gap : i;
     const uint32_t oj = (p & 1) ? (j + A.M - gap) % A.M : j;
-    block_corner_done(A, g, oi * A.M + oj, level);
+    block_corner_done(A, g, oi * A.M + oj, level, p);
   }
 }
 
-// A child block at `level` with origin (oi, oj) and side gap: counted to five,
-// registered on its corners, the traced ones counted down, the guard dropped.
+// A child block at `level` with origin (oi, oj) and side gap: registered on
+// its corners, the traced ones set at once.  Its byte is zero (its level's
+// array is cleared for each build; with one array, the checked parent at the
+// same origin cleared it).
 __device__ __forceinline__ void block_create(const FlowArgs& A, uint32_t g, uint32_t oi,
                                              uint32_t oj, uint32_t gap, int level) {
   const uint32_t origin = oi * A.M + oj;
-  {
-    const uint32_t gk = g * A.NM + origin;
-    uint32_t* word = (uint32_t*)((uintptr_t)(A.bwait + gk) & ~(uintptr_t)3);
-    const uint32_t sh = ((uintptr_t)(A.bwait + gk) & 3) * 8;
-    // the byte is zero (never used, or the finished parent's): add five
-    atomicAdd(word, 5u << sh);
-  }
   const uint32_t oj2 = (oj + gap) % A.M;
-  const uint32_t corner[4] = {origin, oi * A.M + oj2, (oi + gap) * A.M + oj,
-                              (oi + gap) * A.M + oj2};
+  const uint32_t ci[4] = {oi, oi, oi + gap, oi + gap}, cj[4] = {oj, oj2, oj, oj2};
   for (int p = 0; p < 4; p++) {
-    const uint32_t old = atomicOr(&A.vsync[g * A.NM + corner[p]], 1u << p);
-    if (old & kVTraced) block_corner_done(A, g, origin, level);
+    uint32_t* sw = &A.vsync[g * A.NM + ci[p] * A.M + cj[p]];
+    const int e = level - native_level(A, ci[p], cj[p]);
+    if (!A.early && e > 0) {
+      // without early refinement a corner of an older level was traced
+      // before the parent's check
+      if (*(volatile uint32_t*)sw & kVTraced) block_corner_done(A, g, origin, level, p);
+      else atomicOr(&A.ctl->err, 4u);
+      continue;
+    }
+    const uint32_t old = atomicOr(sw, 1u << (4 * e + p));
+    if (old & kVTraced) block_corner_done(A, g, origin, level, p);
   }
-  block_corner_done(A, g, origin, level);  // the guard
 }
 
 // claim_vertex of the level form for the flow: a vertex no block claimed yet
@@ -363,7 +467,9 @@ __device__ __forceinline__ bool flow_claim(const GridDesc& d, uint32_t M, uint32
 // set-up items go to `claimed` (at most five); their count is returned.
 __device__ __forceinline__ unsigned flow_check(const FlowArgs& A, uint32_t item,
                                               uint32_t* claimed) {
-  const int level = A.startlevel + (int)(item >> kFlowKeyBits);
+  const bool early = A.early && (item & kFlowEarly);
+  const int level =
+      A.startlevel + (int)((item >> kFlowKeyBits) & (A.early ? 7u : 15u));
   const uint32_t gk = item & kFlowKeyMask;
   const uint32_t g = gk / A.NM, key = gk % A.NM;
   const GridDesc& d = A.D[g];
@@ -372,15 +478,9 @@ __device__ __forceinline__ unsigned flow_check(const FlowArgs& A, uint32_t item,
   const uint32_t gap = 1u << (A.maxlevel - level);
   const uint32_t i = key / M, j = key % M;
   const uint32_t k = i + gap, l = (j + gap) % M;
-  const double2 v1 = L.thphi[(size_t)i * M + j];
-  const double2 v2 = L.thphi[(size_t)k * M + j];
-  const double2 v3 = L.thphi[(size_t)i * M + l];
-  const double2 v4 = L.thphi[(size_t)k * M + l];
-  const double diag = (v1.x - v4.x) * (v1.x - v4.x) + (v1.y - v4.y) * (v1.y - v4.y);
-  const double diag2 = (v2.x - v3.x) * (v2.x - v3.x) + (v2.y - v3.y) * (v2.y - v3.y);
-  const double mx = diag < diag2 ? diag2 : diag;  // std::max
-  const bool refine = (level < 6 && mx > 1E-10) || (mx > 0.015);
-  if (!refine) {
+  // refined early: a traced diagonal decided it (its other corners may still
+  // be in flight)
+  if (!early && !flow_rule(L, M, i, j, gap, level)) {
     L.blevel[key] = (int8_t)level;
     // leaves below the max level, tagged with their level for the T-vertex fix
     const uint32_t s = atomicAdd(&d.ctr->n_leaf, 1u);
@@ -388,15 +488,27 @@ __device__ __forceinline__ unsigned flow_check(const FlowArgs& A, uint32_t item,
     return 0;
   }
   const uint32_t h = gap / 2, kh = i + h, lh = j + h;
-  const int32_t smax = max(max(L.steps[(size_t)i * M + j], L.steps[(size_t)k * M + j]),
-                           max(L.steps[(size_t)i * M + l], L.steps[(size_t)k * M + l]));
-  const uint32_t hot = smax >= kHotSteps ? 1u << kFlowKeyBits : 0u;
+  // hot: a slow corner (a block refined early waits for one)
+  bool slow = early;
+  if (!early) {
+    const int32_t smax = max(max(L.steps[(size_t)i * M + j], L.steps[(size_t)k * M + j]),
+                             max(L.steps[(size_t)i * M + l], L.steps[(size_t)k * M + l]));
+    slow = smax >= kHotSteps;
+  }
+  const uint32_t hot = slow ? 1u << kFlowKeyBits : 0u;
   const uint32_t nv[5][2] = {{kh, j}, {kh, lh}, {i, lh}, {i + gap, lh}, {kh, (j + gap) % M}};
   unsigned n = 0;
   for (int v = 0; v < 5; v++)
     if (flow_claim(d, M, nv[v][0], nv[v][1]))
       claimed[n++] = hot | (g * A.NM + nv[v][0] * M + nv[v][1]);
   const int lc = level + 1;
+  if (!A.bw_stride && level > A.startlevel && lc < A.maxlevel) {
+    // one array of block bytes: the child at this origin takes this byte,
+    // and no corner of this block is left to set it
+    uint32_t sh;
+    uint32_t* word = block_word(A, gk, level, sh);
+    atomicAnd(word, ~(0xffu << sh));
+  }
   const uint32_t co[4][2] = {{i, j}, {kh, j}, {kh, lh}, {i, lh}};
   for (int c = 0; c < 4; c++) {
     if (lc == A.maxlevel) {

@@ -171,7 +171,12 @@ typedef struct bt_grid_info {
   int32_t N, M, maxlevel, startlevel, angle;
   int64_t traced;         /* rays integrated by the build            */
   int64_t n_leaf_blocks;  /* leaf blocks below the max level          */
-  uint32_t flags;         /* nonzero: a bounded iteration gave up    */
+  uint32_t flags;         /* nonzero: a bounded iteration gave up
+                             (1: T-vertex fix not converged, 2: fix
+                             stack, 4: work list overflow, 8: the
+                             one-launch build gave up waiting) or 16:
+                             an early refinement the level form would
+                             not make (bt_grid_set_flow)             */
   /* device pointers into the lattice (valid until the next build) */
   const double* thphi;    /* N*M (theta, phi) pairs                  */
   const int32_t* steps;   /* N*M                                     */
@@ -197,12 +202,16 @@ int bt_grid_set_graph(bt_grid* g, int on);
  * of `on` blocks of 256 threads per SM (capped by the occupancy limit, 2)
  * instead of one trace launch per level; 0 = off.  A block is checked
  * (refineCheck, BT/Grid.h:410-445) as soon as its own four corners are
- * traced and a new vertex is traced as soon as a check creates it, so no
- * level waits for the previous level's longest rays.  The grids are the same
- * bit for bit.  Reserves 13 bytes per lattice vertex of the set; used when the
- * set's lattices hold fewer than 2^28 vertices in all (otherwise builds take
- * the level form).  No counterpart in the reference (its build is
- * host-driven, level by level). */
+ * traced, or refined as soon as one traced diagonal alone is far enough
+ * apart (maxlevel - startlevel <= 7), and a new vertex is traced as soon as a
+ * check creates it, so no level waits for the previous level's longest rays.
+ * The grids are the same bit for bit, except where a block refined on its
+ * (1, 2) diagonal has a NaN separation on the other, which refineCheck's
+ * std::max turns into a leaf: that build reports flag 16 (rebuild in the
+ * level form).  Reserves 12 + min(maxlevel - 2, 6) bytes per lattice vertex
+ * of the set; used when the set's lattices hold fewer than 2^28 vertices in
+ * all (otherwise builds take the level form).  No counterpart in the
+ * reference (its build is host-driven, level by level). */
 int bt_grid_set_flow(bt_grid* g, int on);
 
 /* Diagnostic: the number of Jacobi passes of the T-vertex fix per level of

@@ -173,9 +173,12 @@ def test_member_misuse(bt, cuda):
 @pytest.mark.parametrize("prec", ["plain", "fast", "mixed"])
 def test_flow_builds_equal_level_builds(bt, cuda, prec):
     """The refinement levels run as one persistent launch (bt_batch_set_flow:
-    a block is checked as soon as its corners are traced) give the grids of
-    the level-by-level build, bit for bit: a set of poses (and one member
-    replayed from a CUDA graph), and the C2 grid L6 -> L10 alone."""
+    a block is checked as soon as its corners are traced, or refined as soon
+    as one traced diagonal decides it) give the grids of the level-by-level
+    build, bit for bit: a set of poses (and one member replayed from a CUDA
+    graph), the C2 grid L6 -> L10 alone, and L4 -> L12, whose eight levels are
+    more than early refinement's waiter bits hold (blocks then wait for all
+    four corners)."""
     cams, spins = cameras(bt, POSES)
     lvl = bt.GridSet(ML, SL, True, len(cams), opts=prec)
     lvl.build(cams, spins)
@@ -196,6 +199,12 @@ def test_flow_builds_equal_level_builds(bt, cuda, prec):
         b.build()
         assert b.info().flags == 0 and b.traced == a.traced
         assert_same(dense(b), dense(a), f"{prec} flow C2 L10, {bps} blocks per SM")
+    a = bt.Grid(12, 4, True, cam, opts=prec)
+    b = bt.Grid(12, 4, True, cam, opts=prec)
+    b.set_flow(True)
+    b.build()
+    assert b.info().flags == 0 and b.traced == a.traced
+    assert_same(dense(b), dense(a), f"{prec} flow C2 L4 -> L12")
 
 
 def test_flow_gives_up_when_a_ray_is_lost(bt, cuda):
