@@ -284,11 +284,13 @@ class Grid:
         launch per level (default) or a launch per pass."""
         L.check(L.lib().bt_grid_set_tfix_launch(self._h, 1 if cooperative else 0))
 
-    def export(self, out=None, pinned=True):
+    def export(self, out=None, pinned=True, stream=None):
         """The grid as key-ordered lists (CamToCel, steps, blockLevels).
 
         Returns dict of numpy arrays vi, vj, theta, phi, steps, bi, bj, level
-        (host copies).  `out` may pass preallocated arrays (reused)."""
+        (host copies).  `out` may pass preallocated arrays (reused).  `stream`
+        (default: the grid's) runs the export; it must follow the build (an
+        event), and the grid must not be built again before this returns."""
         torch = _torch()
         if out is None:
             inf = self.info()
@@ -303,8 +305,9 @@ class Grid:
             setattr(e, k, out[k].data_ptr())
         e.cap_vertices = out["vi"].numel()
         e.cap_blocks = out["bi"].numel()
-        L.check(L.lib().bt_grid_export(self._h, C.byref(e), _stream_ptr(self._stream)))
-        torch.cuda.current_stream().synchronize() if self._stream is None else self._stream.synchronize()
+        st = stream if stream is not None else self._stream
+        L.check(L.lib().bt_grid_export(self._h, C.byref(e), _stream_ptr(st)))
+        torch.cuda.current_stream().synchronize() if st is None else st.synchronize()
         nv, nb = int(e.n_vertices), int(e.n_blocks)
         res = {k: out[k][:nv] for k in ("vi", "vj", "theta", "phi", "steps")}
         res.update({k: out[k][:nb] for k in ("bi", "bj", "level")})
