@@ -779,9 +779,9 @@ void bt_server_destroy(bt_server* s);
  * the FP64 integrator's roofline is reported against. */
 int bt_probe_fp64_tflops(double* tflops, void* stream);
 
-/* The fast form's reciprocal (approximate reciprocal refined by two
- * Newton-Raphson steps) on n DEVICE values: for tests that check it against
- * 1/x.  No counterpart in the reference. */
+/* The fast form's reciprocal (approximate reciprocal refined by one
+ * Newton-Raphson step: relative error ~1e-12) on n DEVICE values: for tests
+ * that check it against 1/x.  No counterpart in the reference. */
 int bt_probe_fast_rcp(const double* x, double* out, size_t n, void* stream);
 
 /* Message for the last error on this thread ("" when none). */
