@@ -488,11 +488,80 @@ __device__ double2 read_vertex(const TfixArgs& A, const Edge& E, uint32_t ip,
   return L.thphi[id];
 }
 
-// checkAdjacentBlock (BT/Grid.h:132-177) as an explicit pre-order DFS.
-// Returns true if any written value differs from the previous pass.
-__device__ bool fix_edge(const TfixArgs& A, const Edge& E) {
+// One node of checkAdjacentBlock's walk (BT/Grid.h:132-177): the sub-edge
+// [fa, fb] of edge E.  When its midpoint exists, writes the midpoint's value
+// (hermite of the four values along the line, or the mean of the ends) to
+// Xcur, sets `changed` if it differs from the previous pass, and returns
+// true (the walk then visits both halves).
+__device__ bool fix_node(const TfixArgs& A, const Edge& E, uint32_t fa, uint32_t fb,
+                         bool& changed) {
   const LatticeView& L = A.L;
   const uint32_t M = L.M, N = L.N;
+  const uint32_t h = fb - fa;
+  const uint32_t ia = E.i0 + E.udlr * fa, ja = E.j0 + (1 - E.udlr) * fa;
+  uint32_t ib, jb;
+  if (fb == E.g) {
+    ib = E.i0 + E.udlr * E.g;
+    jb = (E.j0 + (1 - E.udlr) * E.g) % M;
+  } else {
+    ib = E.i0 + E.udlr * fb;
+    jb = E.j0 + (1 - E.udlr) * fb;
+  }
+  const uint32_t im = ia + E.udlr * h / 2, jm = ja + (1 - E.udlr) * h / 2;
+  if (!vexists(L, im, jm)) return false;
+  uint32_t jprev = (ja - (1 - E.udlr) * h + M) % M;
+  uint32_t jnext = (ja + (1 - E.udlr) * 2 * h) % M;
+  uint32_t iprev = ia - E.udlr * h;
+  uint32_t inext = ia + 2 * E.udlr * h;
+  bool half = false;
+  if (ia == 0) {
+    jprev = (ja + M / 2) % M;
+    iprev = h;
+  } else if (inext > N - 1) {
+    inext = ia;
+    if (L.eq) jnext = (ja + M / 2) % M;
+    else half = true;
+  }
+  double2 val;
+  bool succes = false;
+  const double2 va = read_vertex(A, E, ia, ja, fa, fb);
+  const double2 vb = read_vertex(A, E, ib, jb, fa, fb);
+  if (vexists(L, iprev, jprev) && vexists(L, inext, jnext)) {
+    const double2 vp = read_vertex(A, E, iprev, jprev, fa, fb);
+    const double2 vn = read_vertex(A, E, inext, jnext, fa, fb);
+    if (!(vp.x == -1 && vp.y == -1) && !(vn.x == -1 && vn.y == -1)) {
+      succes = true;
+      double ct[4] = {vp.x, va.x, vb.x, vn.x};
+      double cp[4] = {vp.y, va.y, vb.y, vn.y};
+      if (half) ct[3] = kPi - ct[3];
+      fix2pi(cp, 4);
+      val.x = hermite1(0.5, ct[0], ct[1], ct[2], ct[3]);
+      val.y = hermite1(0.5, cp[0], cp[1], cp[2], cp[3]);
+    }
+  }
+  if (!succes) {
+    double ct[2] = {va.x, vb.x};
+    double cp[2] = {va.y, vb.y};
+    fix2pi(cp, 2);
+    val.x = 1. / 2. * (ct[1] + ct[0]);
+    val.y = 1. / 2. * (cp[1] + cp[0]);
+  }
+  const size_t idm = (size_t)im * M + jm;
+  if (A.pass > 1) {
+    const double2 old = A.Xprev[idm];
+    if (__double_as_longlong(old.x) != __double_as_longlong(val.x) ||
+        __double_as_longlong(old.y) != __double_as_longlong(val.y))
+      changed = true;
+  }
+  A.Xcur[idm] = val;
+  return true;
+}
+
+// checkAdjacentBlock (BT/Grid.h:132-177) as an explicit pre-order DFS, one
+// thread per edge.  Returns true if any written value differs from the
+// previous pass.
+__device__ bool fix_edge(const TfixArgs& A, const Edge& E) {
+  const LatticeView& L = A.L;
   struct Frame { uint32_t a, b; int lv; };
   Frame stack[16];
   int sp = 0;
@@ -500,71 +569,94 @@ __device__ bool fix_edge(const TfixArgs& A, const Edge& E) {
   bool changed = false;
   while (sp > 0) {
     const Frame f = stack[--sp];
-    const uint32_t h = f.b - f.a;
-    const uint32_t ia = E.i0 + E.udlr * f.a, ja = E.j0 + (1 - E.udlr) * f.a;
-    uint32_t ib, jb;
-    if (f.b == E.g) {
-      ib = E.i0 + E.udlr * E.g;
-      jb = (E.j0 + (1 - E.udlr) * E.g) % M;
-    } else {
-      ib = E.i0 + E.udlr * f.b;
-      jb = E.j0 + (1 - E.udlr) * f.b;
-    }
-    const uint32_t im = ia + E.udlr * h / 2, jm = ja + (1 - E.udlr) * h / 2;
-    if (!vexists(L, im, jm)) continue;
-    uint32_t jprev = (ja - (1 - E.udlr) * h + M) % M;
-    uint32_t jnext = (ja + (1 - E.udlr) * 2 * h) % M;
-    uint32_t iprev = ia - E.udlr * h;
-    uint32_t inext = ia + 2 * E.udlr * h;
-    bool half = false;
-    if (ia == 0) {
-      jprev = (ja + M / 2) % M;
-      iprev = h;
-    } else if (inext > N - 1) {
-      inext = ia;
-      if (L.eq) jnext = (ja + M / 2) % M;
-      else half = true;
-    }
-    double2 val;
-    bool succes = false;
-    const double2 va = read_vertex(A, E, ia, ja, f.a, f.b);
-    const double2 vb = read_vertex(A, E, ib, jb, f.a, f.b);
-    if (vexists(L, iprev, jprev) && vexists(L, inext, jnext)) {
-      const double2 vp = read_vertex(A, E, iprev, jprev, f.a, f.b);
-      const double2 vn = read_vertex(A, E, inext, jnext, f.a, f.b);
-      if (!(vp.x == -1 && vp.y == -1) && !(vn.x == -1 && vn.y == -1)) {
-        succes = true;
-        double ct[4] = {vp.x, va.x, vb.x, vn.x};
-        double cp[4] = {vp.y, va.y, vb.y, vn.y};
-        if (half) ct[3] = kPi - ct[3];
-        fix2pi(cp, 4);
-        val.x = hermite1(0.5, ct[0], ct[1], ct[2], ct[3]);
-        val.y = hermite1(0.5, cp[0], cp[1], cp[2], cp[3]);
-      }
-    }
-    if (!succes) {
-      double ct[2] = {va.x, vb.x};
-      double cp[2] = {va.y, vb.y};
-      fix2pi(cp, 2);
-      val.x = 1. / 2. * (ct[1] + ct[0]);
-      val.y = 1. / 2. * (cp[1] + cp[0]);
-    }
-    const size_t idm = (size_t)im * M + jm;
-    if (A.pass > 1) {
-      const double2 old = A.Xprev[idm];
-      if (__double_as_longlong(old.x) != __double_as_longlong(val.x) ||
-          __double_as_longlong(old.y) != __double_as_longlong(val.y))
-        changed = true;
-    }
-    A.Xcur[idm] = val;
+    if (!fix_node(A, E, f.a, f.b, changed)) continue;
     if (f.lv + 1 == L.maxlevel) continue;
-    const uint32_t mo = f.a + h / 2;
+    const uint32_t mo = f.a + (f.b - f.a) / 2;
     if (sp + 2 <= 16) {
       stack[sp++] = {mo, f.b, f.lv + 1};  // right half after the left one
       stack[sp++] = {f.a, mo, f.lv + 1};
     } else {
       atomicOr(&A.ctr->err, 2u);
     }
+  }
+  return changed;
+}
+
+// The same walk by a team of T lanes (a power of two, T <= 16, teams aligned
+// in the warp; every lane of the warp calls, `valid` false for a team without
+// an edge), depth by depth: the sub-edges of one depth are independent, and
+// every value a node reads (its ends and the points one length beyond them)
+// sits at a multiple of its length, i.e. at a midpoint of an earlier depth,
+// so the values are the DFS's.  read_vertex keeps the DFS's view of which
+// points this pass has written.  g <= 64 (at most 32 sub-edges per depth).
+__device__ bool fix_edge_team(const TfixArgs& A, const Edge& E, bool valid, uint32_t g,
+                              unsigned T, unsigned t) {
+  const int depths = __ffs((int)g) - 1;  // log2 g
+  uint32_t vis = valid ? 1u : 0u;         // sub-edges of this depth the walk visits
+  bool changed = false;
+  for (int d = 0; d < depths; d++) {
+    const uint32_t nd = 1u << d, h = g >> d;
+    uint32_t wrote = 0;
+    for (uint32_t k = t; k < nd; k += T)
+      if (((vis >> k) & 1u) && fix_node(A, E, k * h, (k + 1) * h, changed)) wrote |= 1u << k;
+    __syncwarp();  // this depth's values before the next depth reads them
+    for (unsigned sft = 1; sft < T; sft <<= 1) wrote |= __shfl_xor_sync(0xffffffffu, wrote, sft);
+    vis = 0;
+    if (d + 1 < depths)
+      for (uint32_t k = 0; k < nd; k++)
+        if ((wrote >> k) & 1u) vis |= 3u << (2 * k);
+  }
+  return changed;
+}
+
+// One Jacobi pass of the fix over leaf edges [lo, hi) of grid A at side g, by
+// all threads of the launch's blockIdx.y row (warps whole).  A pass takes
+// about (rounds of edges over the threads) x (nodes walked one after another),
+// each node a few dependent loads: one thread per edge walks up to g - 1
+// nodes, a team of T = min(16, g / 2) lanes log2 g depths but takes T lanes
+// per edge.  Edges of 4 to 64 vertices go to teams when that estimate is the
+// smaller (a lone grid's coarse levels, whose long edges bound the pass);
+// otherwise one thread walks each edge (a set of many grids, whose edges
+// outnumber the threads).  Returns whether this thread wrote a changed value.
+__device__ bool tfix_sweep(const TfixArgs& A, uint32_t lo, uint32_t hi, uint32_t g) {
+  const LatticeView& L = A.L;
+  const uint32_t M = L.M;
+  const uint64_t n4 = 4ull * (hi - lo);
+  auto edge_of = [&](uint64_t u, Edge& E) -> bool {
+    const uint32_t key = A.leaves[lo + (uint32_t)(u >> 2)];
+    const int e = (int)(u & 3u);
+    const uint32_t i = key / M, j = key % M;
+    if (L.thphi[key].y < 0) return false;  // BT/Grid.h:107
+    const uint32_t k = i + g, l = (j + g) % M;
+    E = e == 0   ? Edge{i, j, 1, g, rank_of(i, j, 0)}
+        : e == 1 ? Edge{i, j, 0, g, rank_of(i, j, 1)}
+        : e == 2 ? Edge{i, l, 1, g, rank_of(i, j, 2)}
+                 : Edge{k, j, 0, g, rank_of(i, j, 3)};
+    return true;
+  };
+  bool changed = false;
+  const unsigned T = min(16u, g / 2);
+  const uint64_t lanes = (uint64_t)gridDim.x * blockDim.x;
+  const int depths = __ffs((int)g) - 1;
+  const uint64_t team_cost = (n4 * T + lanes - 1) / lanes * (uint64_t)depths;
+  const uint64_t walk_cost = (n4 + lanes - 1) / lanes * (uint64_t)(g - 1);
+  if (g < 4 || g > 64 || team_cost >= walk_cost) {
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n4;
+         u += (uint64_t)gridDim.x * blockDim.x) {
+      Edge E;
+      if (edge_of(u, E)) changed |= fix_edge(A, E);
+    }
+    return changed;
+  }
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned tpw = 32u / T, team = lane / T, t = lane % T;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t w0 = warp * tpw; w0 < n4; w0 += nwarps * tpw) {  // warp-uniform
+    const uint64_t u = w0 + team;
+    Edge E{0u, 0u, 0, g, 0ull};
+    const bool valid = u < n4 && edge_of(u, E);
+    changed |= fix_edge_team(A, E, valid, g, T, t);
   }
   return changed;
 }
@@ -591,25 +683,8 @@ __global__ void k_tfix_pass(const GridDesc* __restrict__ D, int level, int pass,
   if (A.pass > 1 && *(volatile uint32_t*)&ctr->tfix_flags[A.pass - 1] == 0)
     return;  // converged already
   const uint32_t lo = ctr->leaf_off[A.lo], hi = ctr->leaf_off[A.hi_slot];
-  const LatticeView& L = A.L;
-  const uint32_t M = L.M;
-  const uint32_t g = pow2u(L.maxlevel - A.level);
-  bool changed = false;
-  // one thread per (leaf, edge): an edge's T-vertices belong to it alone
-  const uint64_t n4 = 4ull * (hi - lo);
-  for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n4;
-       u += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t key = A.leaves[lo + (uint32_t)(u >> 2)];
-    const int e = (int)(u & 3u);
-    const uint32_t i = key / M, j = key % M;
-    if (L.thphi[key].y < 0) continue;  // BT/Grid.h:107
-    const uint32_t k = i + g, l = (j + g) % M;
-    const Edge E = e == 0   ? Edge{i, j, 1, g, rank_of(i, j, 0)}
-                   : e == 1 ? Edge{i, j, 0, g, rank_of(i, j, 1)}
-                   : e == 2 ? Edge{i, l, 1, g, rank_of(i, j, 2)}
-                            : Edge{k, j, 0, g, rank_of(i, j, 3)};
-    changed |= fix_edge(A, E);
-  }
+  // an edge's T-vertices belong to it alone
+  const bool changed = tfix_sweep(A, lo, hi, pow2u(A.L.maxlevel - A.level));
   if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0)
     atomicOr(&ctr->tfix_flags[A.pass], 1u);
 }
@@ -680,20 +755,7 @@ k_tfix_level(const GridDesc* __restrict__ D, int level, int lo_slot, int hi_slot
     // a grid that did not change in the previous pass is converged
     if (pass == 1 || *(volatile uint32_t*)&ctr->tfix_flags[pass - 1] != 0) {
       const TfixArgs A = tfix_args(d, level, pass, lo_slot, hi_slot);
-      bool changed = false;
-      for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n4;
-           u += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t key = A.leaves[lo + (uint32_t)(u >> 2)];
-        const int e = (int)(u & 3u);
-        const uint32_t i = key / M, j = key % M;
-        if (L.thphi[key].y < 0) continue;  // BT/Grid.h:107
-        const uint32_t k = i + g, l = (j + g) % M;
-        const Edge E = e == 0   ? Edge{i, j, 1, g, rank_of(i, j, 0)}
-                       : e == 1 ? Edge{i, j, 0, g, rank_of(i, j, 1)}
-                       : e == 2 ? Edge{i, l, 1, g, rank_of(i, j, 2)}
-                                : Edge{k, j, 0, g, rank_of(i, j, 3)};
-        changed |= fix_edge(A, E);
-      }
+      const bool changed = tfix_sweep(A, lo, hi, g);
       if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) {
         atomicOr(&ctr->tfix_flags[pass], 1u);
         atomicOr(&set_changed[pass], 1u);
