@@ -123,3 +123,28 @@ def test_ref_frame_rows_equal_whole_frame(oracle_mod):
                                        env_shape=bgr.shape[:2], lr=True, nthreads=4,
                                        area=ref["area"] * np.float32(1.5))
     assert not np.array_equal(r3["env"], r["env"])
+
+
+@pytest.mark.parametrize("name", sorted(CAMERAS))
+def test_early_refinement_rule_holds_on_test_grids(oracle_mod, name):
+    """The one-launch build refines a block as soon as one traced diagonal's
+    squared separation is above refineCheck's threshold (BT/Grid.h:410-445).
+    That equals the full rule, the larger of both diagonals by std::max,
+    unless the (0, 3) separation is NaN.  On the raw grids (before the
+    T-vertex fix) of the test cameras no vertex is NaN, and no leaf block has
+    a diagonal that would alone have refined it."""
+    cam, a = oracle_camera(oracle_mod, name)
+    maxlevel = 9
+    r = oracle_mod.grid_build(maxlevel, 6, True, cam, a, tfix=0)
+    th, ph, ex, bl = r["theta"], r["phi"], r["exists"] == 1, r["blevel"]
+    assert not np.isnan(th[ex]).any() and not np.isnan(ph[ex]).any()
+    M = r["M"]
+    ii, jj = np.nonzero((bl >= 0) & (bl < maxlevel))
+    assert ii.size > 0
+    lv = bl[ii, jj].astype(np.int64)
+    gap = 2 ** (maxlevel - lv)
+    kk, ll = ii + gap, (jj + gap) % M
+    d03 = (th[ii, jj] - th[kk, ll]) ** 2 + (ph[ii, jj] - ph[kk, ll]) ** 2
+    d12 = (th[kk, jj] - th[ii, ll]) ** 2 + (ph[kk, jj] - ph[ii, ll]) ** 2
+    thr = np.where(lv < 6, 1e-10, 0.015)
+    assert not (d03 > thr).any() and not (d12 > thr).any()
